@@ -1,0 +1,144 @@
+/* rmb_gpu.h -- C ABI of the B200 rmblastn search core (librmb_b200.so).
+ *
+ * The library replaces the search body that the reference runs per query under
+ * `--mt-mode` (rmblastn/src/main.rs:739-915 -> search_db_parallel, main.rs:1133-1236):
+ * lookup table, subject scan, exact word extension, diagonal dedup, ungapped X-drop,
+ * preliminary score-only gapped X-drop DP, interval-tree filters, traceback DP,
+ * complexity adjustment, endpoint purges, masklevel and the final hit order.
+ * Every DP, the scan and the extensions run as sm_100a kernels; there is no CPU path
+ * for them.  Plain pointers and sizes only; every call returns 0 on success or a
+ * nonzero status with a message in `err` (the alp_shim pattern of
+ * rmblast-stats/rmstats/csrc/alp_shim.cpp:44-110).  No C++ exception crosses the ABI.
+ * One context per host thread; calls on one context are not reentrant.
+ */
+#ifndef RMB_GPU_H
+#define RMB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RMB_OK 0
+#define RMB_EINVAL 1   /* bad argument */
+#define RMB_ECUDA 2    /* CUDA error (message carries cudaGetErrorString) */
+#define RMB_ENOMEM 3   /* device or host allocation failed */
+#define RMB_ESTATE 4   /* call out of order (e.g. search before rmb_db_load) */
+#define RMB_ELIMIT 5   /* input beyond a documented limit */
+
+/* Search options: rmblast-lib/src/options.rs:12-67 SearchParams.  mask_level < 0 or
+ * >= 100 disables masklevel (main.rs:560).  ungapped_cutoff < 0 derives it as the
+ * reference does per query (search/ka_cutoff.rs:126).  dust must be 0 (query DUST
+ * masking is not implemented in this library; the call fails with RMB_EINVAL). */
+typedef struct rmb_params {
+    int32_t gap_open, gap_extend, word_size;
+    int32_t xdrop_ungap, xdrop_gap, xdrop_gap_final;
+    int32_t min_raw_gapped_score;
+    int32_t complexity_adjust, dust, mask_level;
+    int32_t ungapped_cutoff;
+    int32_t device;       /* CUDA device ordinal */
+    int32_t schedule;     /* 0 = FIFO (only value accepted) */
+    int32_t reserved;
+} rmb_params;
+
+typedef struct rmb_ctx rmb_ctx;
+
+/* rmblast-lib/src/matrix.rs:62-214 ScoreMatrix: scores[q][s] in BLASTNA order
+ * (A C G T R Y M K W S B D H V N GAP), 16x16 row-major; freqs in BLASTNA order; lambda as
+ * the reference estimates it (matrix.rs:290).  matrix_name is the path or file name the
+ * user gave (used only for the Karlin-Altschul ungapped-cutoff table lookup). */
+int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const double freqs[16],
+                   double lambda, const char* matrix_name, rmb_ctx** out, char* err, size_t errlen);
+
+/* rmblast-lib/src/seq/mod.rs:155-291 SubjectDb::open + get_prepared: the library, one call.
+ * plus[i]: sentinel-wrapped BLASTNA (len[i] + 2 bytes) with ambiguity codes already resolved
+ * by NCBI CRandom (seq/fasta_db.rs:86-107); n_mask[i]: NULL or len[i] bytes holding the
+ * original code (4..14) at ambiguous positions, 0 elsewhere (fasta_db.rs:115-131);
+ * ids[i]: subject id.  The subject's oid is its index i. */
+int rmb_db_load(rmb_ctx* ctx, uint32_t n_subjects, const uint8_t* const* plus, const uint32_t* len,
+                const uint8_t* const* n_mask, const char* const* ids, char* err, size_t errlen);
+
+/* One reported HSP: rmblast-lib/src/output.rs:132-138 AlignResult (hits.rs:56-79 Hsp,
+ * stats.rs:25-44 AlignStats).  Coordinates 0-based half-open, subject on the plus strand. */
+typedef struct rmb_hsp {
+    int32_t score;
+    uint32_t q_start, q_end, q_len, s_start, s_end, s_len;
+    uint32_t subject_oid;
+    uint32_t strand;  /* 0 plus, 1 minus */
+    uint32_t matches, mismatches, query_gaps, subject_gaps, transitions, transversions, cpg_sites;
+    float perc_sub, perc_query_gap, perc_db_gap;
+    double kdiv, cpg_kdiv;
+    uint64_t ops_off;  /* into rmb_results.ops */
+    uint32_t ops_len;
+    uint32_t aln_len;  /* length of the aligned strings */
+    uint64_t seq_off;  /* into rmb_results.q_seq / s_seq (BLASTNA, gap = 15) */
+} rmb_hsp;
+
+/* Stage counters of one search call (the reference's diagnostics counters,
+ * search/engine.rs:28-37 and search/gapped.rs:25-36). */
+typedef struct rmb_counters {
+    uint64_t word_hits, seeds, ungapped, prelim_dp, prelims, tb_dp, finals;
+    uint64_t so_cells, tb_cells;
+    double ms_lookup, ms_scan, ms_ungapped, ms_dedup, ms_prelim_dp, ms_host_2a, ms_traceback, ms_host_2b;
+} rmb_counters;
+
+/* Results of rmb_search_batch, in the reference's output order per query
+ * (main.rs:1229-1234 then search/engine.rs:998-1017). */
+typedef struct rmb_results {
+    uint32_t n_queries;
+    uint64_t* query_off;  /* n_queries + 1 offsets into hsps */
+    uint64_t n_hsps;
+    rmb_hsp* hsps;
+    uint32_t* ops;        /* edit script: (op << 30) | count; op 0 Sub, 1 GapInQuery, 2 GapInSubject */
+    uint8_t* q_seq;
+    uint8_t* s_seq;
+    rmb_counters counters;
+} rmb_results;
+
+/* main.rs:1133-1236 search_db_parallel (single-chunk path) for n_queries queries.
+ * query[i]: sentinel-wrapped BLASTNA (qlen[i] + 2 bytes), not CRandom-resolved (queries keep
+ * N).  Queries of 1,999,800 bp or more take the reference's chunked path and are refused
+ * with RMB_ELIMIT. */
+int rmb_search_batch(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
+                     rmb_results** out, char* err, size_t errlen);
+
+/* output.rs:223-367 parse_outfmt + write_tabular: "6 <fields>" lines for every HSP, query by
+ * query; query_ids[i] names query i.  *text is NUL-terminated; free with rmb_text_free. */
+int rmb_format_tabular(const rmb_ctx* ctx, const rmb_results* res, const char* const* query_ids,
+                       const char* outfmt, char** text, size_t* text_len, char* err, size_t errlen);
+
+/* Stage taps, as search/engine.rs:796-832 search_with_query_lookup_seeds/_ungapped expose
+ * them: stage 0 = post-dedup seeds (strand, q, s per record: 3 uint32), stage 1 = sorted
+ * ungapped hits (strand, qs, qe, ss, se, score: 6 uint32), stage 2 = preliminary HSPs after the
+ * prelim endpoint purge (strand, qs, qe, ss, se, score, q_seed, s_seed: 8 uint32), for every
+ * (query, subject) pair in pair order.  *records is malloc'd; free with rmb_text_free. */
+int rmb_debug_stage(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
+                    int32_t stage, uint32_t** records, uint64_t* n_records, char* err, size_t errlen);
+
+/* Input preparation the reference does before the search (host side, no GPU needed).
+ * rmb_matrix_parse: rmblast-lib/src/matrix.rs:76-324 ScoreMatrix::from_reader (FREQS line,
+ * header, rows by position, -32768 for undefined codes, INT32_MIN/2 for the gap row/column,
+ * lambda by the reference's bisection).  Same refusals as the reference (bad FREQS, non-square
+ * matrix, non-negative expected score).
+ * rmb_encode_iupac: encoding.rs:125 encode_iupac (n ASCII bytes -> n + 2 BLASTNA bytes).
+ * rmb_resolve_subject: seq/fasta_db.rs:86-131 -- CRandom (seeded with the length) replaces each
+ * ambiguity code 4..14 by a base, and n_mask (n bytes) keeps the original codes; *has_mask is
+ * 0 when the subject has no ambiguity code (n_mask then stays all zero). */
+int rmb_matrix_parse(const char* text, int32_t scores[256], double freqs[16], double* lambda, char* err,
+                     size_t errlen);
+void rmb_encode_iupac(const char* ascii, size_t n, uint8_t* out);
+void rmb_resolve_subject(const uint8_t* raw, uint32_t n, uint8_t* plus, uint8_t* n_mask, int32_t* has_mask);
+
+void rmb_results_free(rmb_results* res);
+void rmb_text_free(void* p);
+void rmb_ctx_destroy(rmb_ctx* ctx);
+
+/* Library version string. */
+const char* rmb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RMB_GPU_H */

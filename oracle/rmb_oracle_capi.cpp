@@ -161,3 +161,52 @@ int rmbo_stage_file(const char* query_path, const char* db_path, const char* mat
 void rmbo_free(char* p) { free(p); }
 
 }  // extern "C"
+
+extern "C" {
+// Stage taps per (query, subject) pair in pair order, as uint32 records: stage 0 seeds
+// (strand, q, s), 1 sorted ungapped hits (strand, qs, qe, ss, se, score), 2 prelims after the
+// prelim purge (strand, qs, qe, ss, se, score, q_seed, s_seed).
+int rmbo_stage_text(const char* query_fasta, const char* db_fasta, const char* matrix_text, const char* matrix_name,
+                    const rmbo_params* cp, int stage, uint32_t** out, uint64_t* n_out, char* err, size_t errlen) {
+    try {
+        Matrix m = parse_matrix(matrix_text, matrix_name);
+        Params p = to_params(cp, matrix_name);
+        std::vector<Subject> db;
+        for (auto& r : read_fasta_text(db_fasta)) db.push_back(make_subject(r.id, r.seq));
+        auto qs = read_fasta_text(query_fasta);
+        uint64_t total = 0;
+        for (auto& s : db) total += s.len();
+        std::vector<uint32_t> rec;
+        for (auto& q : qs) {
+            Params pq = p;
+            pq.ungapped_cutoff = ungapped_cutoff(p.matrix_name, p.gap_open, p.gap_extend, p.min_raw_gapped_score,
+                                                 q.seq.size() - 2, db.empty() ? 0 : total / db.size());
+            QueryLookup ql = build_query_lookup(q.seq, pq);
+            for (auto& s : db) {
+                std::vector<SeedRecord> seeds;
+                std::vector<UngappedHit> ung;
+                std::vector<PrelimHsp> pre;
+                Taps t;
+                if (stage == 0) t.seeds = &seeds;
+                else if (stage == 1) t.ungapped = &ung;
+                else t.prelims = &pre;
+                search_pair(ql, q.seq, q.id, s, pq, m, t);
+                for (auto& x : seeds) rec.insert(rec.end(), {(uint32_t)x.strand, x.q_off, x.s_off});
+                for (auto& h : ung)
+                    rec.insert(rec.end(), {(uint32_t)h.strand, h.q_start, h.q_end, h.s_start, h.s_end, (uint32_t)h.score});
+                for (auto& h : pre)
+                    rec.insert(rec.end(), {(uint32_t)h.strand, h.q_start, h.q_end, h.s_start, h.s_end, (uint32_t)h.score,
+                                           h.q_seed, h.s_seed});
+            }
+        }
+        uint32_t* o = (uint32_t*)malloc(std::max<size_t>(rec.size(), 1) * 4);
+        if (!rec.empty()) memcpy(o, rec.data(), rec.size() * 4);
+        *out = o;
+        *n_out = rec.size() / (stage == 0 ? 3 : stage == 1 ? 6 : 8);
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return 1;
+    }
+}
+}

@@ -1,0 +1,297 @@
+"""Python host over the C ABI of include/rmb_gpu.h (librmb_b200.so).
+
+Mirrors the reference's library surface for the search path:
+  ScoreMatrix.from_text/from_file   rmblast-lib/src/matrix.rs:76-224
+  SearchParams                       rmblast-lib/src/options.rs:12-104
+  SubjectDb.from_fasta / from_records  rmblast-lib/src/seq/mod.rs:155-291 (CRandom decode)
+  Searcher.search                    rmblastn/src/main.rs:1133-1236 search_db_parallel, per query
+  Searcher.stage                     search/engine.rs:796-832 stage taps (seeds, ungapped, prelims)
+  Results.tabular                    rmblast-lib/src/output.rs:294-367 write_tabular
+
+There is no CPU path: every call goes to the CUDA library, and importing this module
+fails if librmb_b200.so was not built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "librmb_b200.so"
+
+
+class RmbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rmb error {code}: {msg}")
+        self.code = code
+
+
+class _Params(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "gap_open", "gap_extend", "word_size", "xdrop_ungap", "xdrop_gap", "xdrop_gap_final",
+        "min_raw_gapped_score", "complexity_adjust", "dust", "mask_level", "ungapped_cutoff",
+        "device", "schedule", "reserved")]
+
+
+class _Hsp(C.Structure):
+    _fields_ = [("score", C.c_int32)] + [(n, C.c_uint32) for n in (
+        "q_start", "q_end", "q_len", "s_start", "s_end", "s_len", "subject_oid", "strand", "matches",
+        "mismatches", "query_gaps", "subject_gaps", "transitions", "transversions", "cpg_sites")] + [
+        ("perc_sub", C.c_float), ("perc_query_gap", C.c_float), ("perc_db_gap", C.c_float),
+        ("kdiv", C.c_double), ("cpg_kdiv", C.c_double), ("ops_off", C.c_uint64), ("ops_len", C.c_uint32),
+        ("aln_len", C.c_uint32), ("seq_off", C.c_uint64)]
+
+
+class _Counters(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "word_hits", "seeds", "ungapped", "prelim_dp", "prelims", "tb_dp", "finals", "so_cells", "tb_cells")] + [
+        (n, C.c_double) for n in ("ms_lookup", "ms_scan", "ms_ungapped", "ms_dedup", "ms_prelim_dp", "ms_host_2a",
+                                  "ms_traceback", "ms_host_2b")]
+
+
+class _Results(C.Structure):
+    _fields_ = [("n_queries", C.c_uint32), ("query_off", C.POINTER(C.c_uint64)), ("n_hsps", C.c_uint64),
+                ("hsps", C.POINTER(_Hsp)), ("ops", C.POINTER(C.c_uint32)), ("q_seq", C.POINTER(C.c_uint8)),
+                ("s_seq", C.POINTER(C.c_uint8)), ("counters", _Counters)]
+
+
+def load_library(path: Path = LIB_PATH) -> C.CDLL:
+    if not path.exists():
+        raise ImportError(f"{path} is missing: build it with `python -m rmblast_b200.build`")
+    lib = C.CDLL(str(path))
+    u8p, u8pp = C.POINTER(C.c_uint8), C.POINTER(C.POINTER(C.c_uint8))
+    lib.rmb_ctx_create.argtypes = [C.POINTER(_Params), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_double,
+                                   C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]
+    lib.rmb_db_load.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32), u8pp,
+                                C.POINTER(C.c_char_p), C.c_char_p, C.c_size_t]
+    lib.rmb_search_batch.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32),
+                                     C.POINTER(C.POINTER(_Results)), C.c_char_p, C.c_size_t]
+    lib.rmb_format_tabular.argtypes = [C.c_void_p, C.POINTER(_Results), C.POINTER(C.c_char_p), C.c_char_p,
+                                       C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t]
+    lib.rmb_debug_stage.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32), C.c_int32,
+                                    C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
+    lib.rmb_matrix_parse.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.c_char_p, C.c_size_t]
+    lib.rmb_encode_iupac.argtypes = [C.c_char_p, C.c_size_t, u8p]
+    lib.rmb_encode_iupac.restype = None
+    lib.rmb_resolve_subject.argtypes = [u8p, C.c_uint32, u8p, u8p, C.POINTER(C.c_int32)]
+    lib.rmb_resolve_subject.restype = None
+    lib.rmb_results_free.argtypes = [C.POINTER(_Results)]
+    lib.rmb_results_free.restype = None
+    lib.rmb_text_free.argtypes = [C.c_void_p]
+    lib.rmb_text_free.restype = None
+    lib.rmb_ctx_destroy.argtypes = [C.c_void_p]
+    lib.rmb_ctx_destroy.restype = None
+    lib.rmb_version.restype = C.c_char_p
+    return lib
+
+
+_LIB: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = load_library()
+    return _LIB
+
+
+def _check(rc: int, err: C.Array) -> None:
+    if rc != 0:
+        raise RmbError(rc, err.value.decode(errors="replace"))
+
+
+def encode(ascii_seq: bytes | np.ndarray) -> np.ndarray:
+    """encoding.rs:125 encode_iupac: ASCII -> sentinel-wrapped BLASTNA."""
+    b = bytes(ascii_seq) if not isinstance(ascii_seq, np.ndarray) else ascii_seq.tobytes()
+    out = np.empty(len(b) + 2, dtype=np.uint8)
+    lib().rmb_encode_iupac(b, len(b), out.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return out
+
+
+def read_fasta(text: str) -> list[tuple[str, bytes]]:
+    """seq/fasta.rs:83 FastaReader: (id, sequence) per record."""
+    recs, name, buf = [], None, []
+    for line in text.splitlines():
+        if line.startswith(">"):
+            if name is not None:
+                recs.append((name, "".join(buf).encode()))
+            name = line[1:].split()[0]
+            buf = []
+        elif line.strip():
+            buf.append(line.strip())
+    if name is not None:
+        recs.append((name, "".join(buf).encode()))
+    return recs
+
+
+@dataclass
+class ScoreMatrix:
+    scores: np.ndarray  # int32 (16, 16), scores[q][s]
+    freqs: np.ndarray   # float64 (16,)
+    lambda_: float
+    name: str
+
+    @classmethod
+    def from_text(cls, text: str, name: str = "") -> "ScoreMatrix":
+        sc = (C.c_int32 * 256)()
+        fr = (C.c_double * 16)()
+        lam = C.c_double()
+        err = C.create_string_buffer(512)
+        _check(lib().rmb_matrix_parse(text.encode(), sc, fr, C.byref(lam), err, 512), err)
+        return cls(np.frombuffer(sc, dtype=np.int32).reshape(16, 16).copy(), np.frombuffer(fr).copy(),
+                   lam.value, name)
+
+    @classmethod
+    def from_file(cls, path: str) -> "ScoreMatrix":
+        return cls.from_text(Path(path).read_text(), path)
+
+
+@dataclass
+class SearchParams:
+    """options.rs:12-104 (with rmblastn's CLI defaults, main.rs:128-281)."""
+    gap_open: int = 20
+    gap_extend: int = 5
+    word_size: int = 11
+    xdrop_ungap: int = 20
+    xdrop_gap: int = 30
+    xdrop_gap_final: int = 100
+    min_raw_gapped_score: int = 0
+    complexity_adjust: bool = False
+    dust: bool = False
+    mask_level: int = -1
+    ungapped_cutoff: int = -1
+    device: int = 0
+
+    def _c(self) -> _Params:
+        return _Params(self.gap_open, self.gap_extend, self.word_size, self.xdrop_ungap, self.xdrop_gap,
+                       self.xdrop_gap_final, self.min_raw_gapped_score, int(self.complexity_adjust), int(self.dust),
+                       self.mask_level, self.ungapped_cutoff, self.device, 0, 0)
+
+
+class SubjectDb:
+    """seq/mod.rs:155-291: subjects decoded once, ambiguity codes CRandom-resolved."""
+
+    def __init__(self, ids: list[str], plus: list[np.ndarray], masks: list[np.ndarray | None]):
+        self.ids, self.plus, self.masks = ids, plus, masks
+
+    @classmethod
+    def from_records(cls, recs: list[tuple[str, bytes | np.ndarray]]) -> "SubjectDb":
+        ids, plus, masks = [], [], []
+        for name, seq in recs:
+            raw = encode(seq)
+            n = len(raw) - 2
+            p = np.empty_like(raw)
+            m = np.zeros(max(n, 1), dtype=np.uint8)
+            has = C.c_int32()
+            lib().rmb_resolve_subject(raw.ctypes.data_as(C.POINTER(C.c_uint8)), n,
+                                      p.ctypes.data_as(C.POINTER(C.c_uint8)), m.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                      C.byref(has))
+            ids.append(name)
+            plus.append(p)
+            masks.append(m[:n] if has.value else None)
+        return cls(ids, plus, masks)
+
+    @classmethod
+    def from_fasta(cls, text: str) -> "SubjectDb":
+        return cls.from_records(read_fasta(text))
+
+    def total_letters(self) -> int:
+        return sum(len(p) - 2 for p in self.plus)
+
+
+def _ptr_array(arrs: list[np.ndarray | None]):
+    t = (C.POINTER(C.c_uint8) * len(arrs))()
+    for i, a in enumerate(arrs):
+        t[i] = a.ctypes.data_as(C.POINTER(C.c_uint8)) if a is not None else C.POINTER(C.c_uint8)()
+    return t
+
+
+class Results:
+    """rmb_results: HSPs per query in the reference's output order."""
+
+    def __init__(self, searcher: "Searcher", ptr, query_ids: list[str]):
+        self._s, self._p, self.query_ids = searcher, ptr, query_ids
+        r = ptr.contents
+        self.n_hsps = int(r.n_hsps)
+        c = r.counters
+        self.counters = {f: getattr(c, f) for f, _ in _Counters._fields_}
+
+    def hsps(self) -> list[dict]:
+        r = self._p.contents
+        out = []
+        for q in range(r.n_queries):
+            for k in range(r.query_off[q], r.query_off[q + 1]):
+                h = r.hsps[k]
+                out.append({f: getattr(h, f) for f, _ in _Hsp._fields_} | {"query": q})
+        return out
+
+    def tabular(self, outfmt: str) -> str:
+        ids = (C.c_char_p * max(1, len(self.query_ids)))(*[i.encode() for i in self.query_ids])
+        txt = C.c_void_p()
+        n = C.c_size_t()
+        err = C.create_string_buffer(512)
+        _check(lib().rmb_format_tabular(self._s._ctx, self._p, ids, outfmt.encode(), C.byref(txt), C.byref(n), err,
+                                        512), err)
+        try:
+            return C.string_at(txt.value, n.value).decode()
+        finally:
+            lib().rmb_text_free(txt)
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            lib().rmb_results_free(self._p)
+            self._p = None
+
+
+class Searcher:
+    """One search context on one GPU: parameters, matrix and the resident library."""
+
+    def __init__(self, params: SearchParams, matrix: ScoreMatrix, db: SubjectDb):
+        self.params, self.matrix, self.db = params, matrix, db
+        ctx = C.c_void_p()
+        err = C.create_string_buffer(512)
+        sc = matrix.scores.astype(np.int32).ravel()
+        fr = matrix.freqs.astype(np.float64)
+        _check(lib().rmb_ctx_create(C.byref(params._c()), sc.ctypes.data_as(C.POINTER(C.c_int32)),
+                                    fr.ctypes.data_as(C.POINTER(C.c_double)), matrix.lambda_,
+                                    matrix.name.encode(), C.byref(ctx), err, 512), err)
+        self._ctx = ctx
+        n = len(db.ids)
+        lens = (C.c_uint32 * n)(*[len(p) - 2 for p in db.plus])
+        ids = (C.c_char_p * n)(*[i.encode() for i in db.ids])
+        _check(lib().rmb_db_load(ctx, n, _ptr_array(db.plus), lens, _ptr_array(db.masks), ids, err, 512), err)
+
+    def _queries(self, queries: list[np.ndarray]):
+        n = len(queries)
+        return n, _ptr_array(queries), (C.c_uint32 * max(n, 1))(*[len(q) - 2 for q in queries])
+
+    def search(self, queries: list[np.ndarray], query_ids: list[str] | None = None) -> Results:
+        n, qp, ql = self._queries(queries)
+        res = C.POINTER(_Results)()
+        err = C.create_string_buffer(1024)
+        _check(lib().rmb_search_batch(self._ctx, n, qp, ql, C.byref(res), err, 1024), err)
+        return Results(self, res, query_ids or [f"query{i}" for i in range(n)])
+
+    def stage(self, queries: list[np.ndarray], stage: int) -> np.ndarray:
+        n, qp, ql = self._queries(queries)
+        rec = C.POINTER(C.c_uint32)()
+        nrec = C.c_uint64()
+        err = C.create_string_buffer(1024)
+        _check(lib().rmb_debug_stage(self._ctx, n, qp, ql, stage, C.byref(rec), C.byref(nrec), err, 1024), err)
+        width = (3, 6, 8)[stage]
+        try:
+            a = np.ctypeslib.as_array(rec, shape=(int(nrec.value) * width,)).copy() if nrec.value else np.zeros(0, np.uint32)
+        finally:
+            lib().rmb_text_free(C.cast(rec, C.c_void_p))
+        return a.reshape(-1, width)
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            lib().rmb_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()

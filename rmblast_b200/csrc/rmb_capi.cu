@@ -1,0 +1,940 @@
+// rmb_capi.cu -- the C ABI of include/rmb_gpu.h: context, library upload, the batched search
+// pipeline (GPU stages + host order-dependent filters) and result packing.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <new>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/rmb_gpu.h"
+#include "rmb_device.cuh"
+#include "rmb_glue.hpp"
+#include "rmb_kernels.hpp"
+
+using namespace rmb;
+
+namespace {
+
+struct Fail : std::runtime_error {
+    int code;
+    Fail(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                          \
+    do {                                                                                               \
+        cudaError_t e_ = (x);                                                                          \
+        if (e_ != cudaSuccess)                                                                         \
+            throw Fail(e_ == cudaErrorMemoryAllocation ? RMB_ENOMEM : RMB_ECUDA,                        \
+                       std::string(#x) + ": " + cudaGetErrorString(e_));                                \
+    } while (0)
+
+struct DBuf {  // growable device buffer
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t nc = std::max<size_t>(n, 256);
+        CK(cudaMalloc(&p, nc));
+        cap = nc;
+    }
+    template <class T>
+    T* as() const { return (T*)p; }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+template <class T>
+void upload(DBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+const uint8_t COMPL[16] = {3, 2, 1, 0, 5, 4, 7, 6, 8, 9, 13, 12, 11, 10, 14, 15};
+
+void parallel_for(size_t n, const std::function<void(size_t)>& fn) {
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), n));
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> th;
+    std::exception_ptr err;
+    std::mutex mu;
+    for (size_t t = 0; t < nt; ++t)
+        th.emplace_back([&]() {
+            for (;;) {
+                size_t i = next.fetch_add(1);
+                if (i >= n) break;
+                try {
+                    fn(i);
+                } catch (...) {
+                    std::lock_guard<std::mutex> g(mu);
+                    if (!err) err = std::current_exception();
+                }
+            }
+        });
+    for (auto& x : th) x.join();
+    if (err) std::rethrow_exception(err);
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct rmb_ctx {
+    rmb_params p{};
+    GlueParams gp{};
+    std::string matrix_name;
+    int sms = 148;
+    cudaStream_t st = nullptr;
+    // library, host
+    std::vector<std::string> ids;
+    std::vector<uint32_t> slen;
+    std::vector<uint64_t> plus_off, packed_off;
+    std::vector<uint8_t> h_align, h_align_rc;
+    std::vector<uint8_t> h_mask, h_mask_rc;  // len bytes per subject that has a mask
+    std::vector<int64_t> mask_off;            // -1 = no mask
+    uint64_t total_letters = 0;
+    uint32_t max_slen = 0;
+    bool loaded = false;
+    // library, device
+    DBuf d_plus, d_rc, d_align, d_align_rc, d_packed, d_plus_off, d_packed_off, d_len, d_params;
+    // per-batch device buffers
+    DBuf q, qrc, qoff, qlen, pv, pv_off, cs, cs_off, cq, cq_off, lw;
+    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, n_wide, band, sel,
+        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
+    DevLib L{};
+};
+
+namespace {
+
+struct Lut {  // one query's table in the device layout (rmb_device.cuh DevQueries)
+    int lw = 0;
+    std::vector<uint32_t> pv, cell_start, cell_q;
+};
+
+// blast/nalookup.rs:128-335 and blast/mblookup.rs:106-235, as one CSR: every lw-mer of the
+// two-context buffer [fwd | N | rc] whose lw bases are all A/C/G/T, per cell in the order the
+// reference's table hands them out (ascending for lw <= 8, descending for the megablast table).
+void build_lut(const uint8_t* q, uint32_t n, int ws, Lut& L) {
+    const uint64_t approx = 2ull * n;
+    L.lw = choose_lut_width(ws, approx);
+    if (L.lw < 0) throw Fail(RMB_EINVAL, "word_size below 4");
+    const int lw = L.lw;
+    const uint32_t cells = 1u << (2 * lw);
+    std::vector<uint8_t> comb(2ull * n + 1);
+    for (uint32_t i = 0; i < n; ++i) comb[i] = q[1 + i];
+    comb[n] = 14;
+    for (uint32_t i = 0; i < n; ++i) comb[n + 1 + i] = COMPL[q[n - i] & 15];
+    std::vector<uint32_t> code(comb.size(), 0xffffffffu);
+    const uint32_t mask = cells - 1;
+    const int64_t locs[2][2] = {{0, (int64_t)n - 1}, {(int64_t)n + 1, 2 * (int64_t)n}};
+    for (auto& loc : locs) {
+        const int64_t from = loc[0], to = loc[1];
+        if (ws > to - from + 1) continue;
+        uint32_t e = 0;
+        int64_t valid_from = from + lw - 1;
+        for (int64_t rp = from; rp <= to; ++rp) {
+            const uint8_t b = comb[rp];
+            if (b & 0xFC) { e = 0; valid_from = rp + lw; continue; }
+            e = ((e << 2) & mask) | b;
+            if (rp < valid_from) continue;
+            code[rp + 1 - lw] = e;
+        }
+    }
+    L.cell_start.assign((size_t)cells + 1, 0);
+    for (uint32_t c : code)
+        if (c != 0xffffffffu) L.cell_start[c + 1]++;
+    for (uint32_t c = 0; c < cells; ++c) L.cell_start[c + 1] += L.cell_start[c];
+    L.cell_q.assign(L.cell_start[cells], 0);
+    std::vector<uint32_t> fill(L.cell_start.begin(), L.cell_start.end() - 1);
+    if (lw <= 8) {
+        for (size_t s = 0; s < code.size(); ++s)
+            if (code[s] != 0xffffffffu) L.cell_q[fill[code[s]]++] = (uint32_t)s;
+    } else {
+        for (size_t s = code.size(); s-- > 0;)
+            if (code[s] != 0xffffffffu) L.cell_q[fill[code[s]]++] = (uint32_t)s;
+    }
+    L.pv.assign(std::max<uint32_t>(cells / 32, 1), 0);
+    for (uint32_t c = 0; c < cells; ++c)
+        if (L.cell_start[c + 1] > L.cell_start[c]) L.pv[c >> 5] |= 1u << (c & 31);
+}
+
+std::vector<uint8_t> revcomp_full(const uint8_t* s, size_t n) {
+    std::vector<uint8_t> o(n);
+    for (size_t i = 0; i < n; ++i) o[i] = COMPL[s[n - 1 - i] & 15];
+    return o;
+}
+
+struct Taps {
+    std::vector<uint32_t>* seeds = nullptr;     // strand, q, s
+    std::vector<uint32_t>* ungapped = nullptr;  // strand, qs, qe, ss, se, score
+    std::vector<uint32_t>* prelims = nullptr;   // strand, qs, qe, ss, se, score, q_seed, s_seed
+};
+
+// One batch: returns per-query hits (reference order).
+void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen,
+                std::vector<std::vector<Hit>>& out_hits, rmb_counters& ctr, Taps* taps) {
+    const rmb_params& P = C.p;
+    const uint32_t ns = (uint32_t)C.ids.size();
+    out_hits.assign(nq, {});
+    std::vector<int32_t> ucut(nq);
+    for (uint32_t i = 0; i < nq; ++i) {
+        if (qlen[i] >= 1999800u) throw Fail(RMB_ELIMIT, "queries of 1,999,800 bp or more take the chunked path");
+        const uint64_t avg = ns ? C.total_letters / ns : 0;
+        ucut[i] = P.ungapped_cutoff >= 0 ? P.ungapped_cutoff
+                                          : ungapped_cutoff_for(C.matrix_name, P.gap_open, P.gap_extend,
+                                                                P.min_raw_gapped_score, qlen[i], avg);
+    }
+    // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table bytes.
+    uint32_t qb = 0;
+    while (qb < nq) {
+        uint64_t bytes = 0;
+        uint32_t qe = qb;
+        while (qe < nq && (qe == qb || (ucut[qe] == ucut[qb] && bytes < (1ull << 30)))) {
+            const int lw = choose_lut_width(P.word_size, 2ull * qlen[qe]);
+            bytes += (4ull << (2 * std::max(lw, 4))) + 8ull * qlen[qe];
+            ++qe;
+        }
+        const uint32_t nb = qe - qb;
+        auto t0 = std::chrono::steady_clock::now();
+        // ---- queries and lookup tables
+        std::vector<Lut> luts(nb);
+        parallel_for(nb, [&](size_t i) { build_lut(query[qb + i], qlen[qb + i], P.word_size, luts[i]); });
+        std::vector<uint8_t> hq, hqrc;
+        std::vector<uint64_t> hqoff(nb), hpvoff(nb), hcsoff(nb), hcqoff(nb);
+        std::vector<uint32_t> hqlen(nb);
+        std::vector<int32_t> hlw(nb);
+        uint64_t npv = 0, ncs = 0, ncq = 0;
+        for (uint32_t i = 0; i < nb; ++i) {
+            hqoff[i] = hq.size();
+            hqlen[i] = qlen[qb + i];
+            const uint8_t* s = query[qb + i];
+            hq.insert(hq.end(), s, s + qlen[qb + i] + 2);
+            auto rc = revcomp_full(s, qlen[qb + i] + 2);
+            hqrc.insert(hqrc.end(), rc.begin(), rc.end());
+            hpvoff[i] = npv;
+            hcsoff[i] = ncs;
+            hcqoff[i] = ncq;
+            npv += luts[i].pv.size();
+            ncs += luts[i].cell_start.size();
+            ncq += luts[i].cell_q.size();
+            hlw[i] = luts[i].lw;
+        }
+        std::vector<uint32_t> hpv(npv), hcs(ncs), hcq(std::max<uint64_t>(ncq, 1));
+        parallel_for(nb, [&](size_t i) {
+            std::copy(luts[i].pv.begin(), luts[i].pv.end(), hpv.begin() + hpvoff[i]);
+            std::copy(luts[i].cell_start.begin(), luts[i].cell_start.end(), hcs.begin() + hcsoff[i]);
+            std::copy(luts[i].cell_q.begin(), luts[i].cell_q.end(), hcq.begin() + hcqoff[i]);
+        });
+        luts.clear();
+        cudaStream_t st = C.st;
+        upload(C.q, hq, st);
+        upload(C.qrc, hqrc, st);
+        upload(C.qoff, hqoff, st);
+        upload(C.qlen, hqlen, st);
+        upload(C.pv, hpv, st);
+        upload(C.pv_off, hpvoff, st);
+        upload(C.cs, hcs, st);
+        upload(C.cs_off, hcsoff, st);
+        upload(C.cq, hcq, st);
+        upload(C.cq_off, hcqoff, st);
+        upload(C.lw, hlw, st);
+        DevQueries Q{C.q.as<uint8_t>(),      C.qrc.as<uint8_t>(),     C.q.as<uint8_t>(),  C.qoff.as<uint64_t>(),
+                     C.qlen.as<uint32_t>(),  C.pv.as<uint32_t>(),     C.pv_off.as<uint64_t>(),
+                     C.cs.as<uint32_t>(),    C.cs_off.as<uint64_t>(), C.cq.as<uint32_t>(),
+                     C.cq_off.as<uint64_t>(), C.lw.as<int32_t>(),     nb};
+        CK(cudaStreamSynchronize(st));
+        ctr.ms_lookup += ms_since(t0);
+
+        // ---- scan: count, offsets, write
+        t0 = std::chrono::steady_clock::now();
+        const uint64_t pair0 = (uint64_t)qb * ns;
+        // pair ids are relative to this sub-batch: query index qi - qb
+        const uint64_t npairs = (uint64_t)nb * ns;
+        C.counts.ensure((npairs + 1) * 4);
+        C.offs.ensure((npairs + 1) * 8);
+        CK(cudaMemsetAsync(C.counts.p, 0, (npairs + 1) * 4, st));
+        CK(launch_scan(false, C.L, Q, P.word_size, 0, npairs, C.counts.as<uint32_t>(), nullptr, nullptr, nullptr,
+                       C.sms, st));
+        size_t tb = 0;
+        CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), nullptr, tb, st));
+        C.temp.ensure(tb);
+        CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), C.temp.p, tb, st));
+        uint64_t nh = 0;
+        CK(cudaMemcpyAsync(&nh, C.offs.as<uint64_t>() + npairs, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (nh >= 0xffffffffull) throw Fail(RMB_ELIMIT, "more than 2^32 word hits in one batch");
+        ctr.word_hits += nh;
+        C.hits.ensure(nh * sizeof(SeedHit));
+        C.hit_pair.ensure(nh * 4);
+        CK(launch_scan(true, C.L, Q, P.word_size, 0, npairs, nullptr, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
+                       C.hit_pair.as<uint32_t>(), C.sms, st));
+        CK(cudaStreamSynchronize(st));
+        ctr.ms_scan += ms_since(t0);
+        (void)pair0;
+
+        // ---- ungapped extension of every hit, then the per-pair dedup
+        t0 = std::chrono::steady_clock::now();
+        C.ub.ensure(nh * sizeof(UngBox));
+        CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
+                           C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st));
+        CK(cudaStreamSynchronize(st));
+        ctr.ms_ungapped += ms_since(t0);
+        t0 = std::chrono::steady_clock::now();
+        C.flags.ensure(nh + 1);
+        C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
+        C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+        CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], 0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
+                        C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
+        C.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
+        C.n_sel.ensure(16);
+        tb = 0;
+        CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb,
+                            st));
+        C.temp.ensure(tb);
+        CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p,
+                            tb, st));
+        uint32_t nu = 0;
+        CK(cudaMemcpyAsync(&nu, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ctr.ms_dedup += ms_since(t0);
+        ctr.ungapped += nu;
+        if (taps && (taps->seeds || taps->ungapped)) {
+            std::vector<SeedHit> hh(nh);
+            std::vector<uint32_t> hp(nh);
+            std::vector<uint8_t> fl(nh);
+            std::vector<UngBox> uu(nh);
+            if (nh) {
+                CK(cudaMemcpy(hh.data(), C.hits.p, nh * sizeof(SeedHit), cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(hp.data(), C.hit_pair.p, nh * 4, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(fl.data(), C.flags.p, nh, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(uu.data(), C.ub.p, nh * sizeof(UngBox), cudaMemcpyDeviceToHost));
+            }
+            for (uint64_t i = 0; i < nh; ++i) {
+                if (!fl[i]) continue;
+                const uint32_t qi = hp[i] / ns, si = hp[i] % ns;
+                const uint32_t s_len = C.slen[si];
+                const bool minus = hh[i].qs >> 31;
+                const uint32_t qo = hh[i].qs & 0x7fffffffu, so = hh[i].s;
+                if (taps->seeds) {
+                    if (!minus) taps->seeds->insert(taps->seeds->end(), {0u, qo, so});
+                    else {
+                        const uint32_t en = (uint32_t)(P.word_size - hlw[qi]);
+                        const uint32_t sl = so + (uint32_t)hlw[qi];
+                        taps->seeds->insert(taps->seeds->end(), {1u, qo >= en ? qo - en : 0, s_len >= sl ? s_len - sl : 0});
+                    }
+                }
+            }
+            if (taps->ungapped) {
+                // per pair, in the reference's sort order (engine.rs:1280-1309)
+                std::vector<std::vector<UngSurvivor>> per(npairs);
+                for (uint64_t i = 0; i < nh; ++i) {
+                    if (fl[i] != 3) continue;
+                    UngSurvivor r{};
+                    r.q_seed = hh[i].qs & 0x7fffffffu;
+                    r.s_seed = hh[i].s;
+                    r.q_start = uu[i].q_start;
+                    r.q_end = uu[i].q_end;
+                    r.s_start = uu[i].s_start;
+                    r.s_end = uu[i].s_end;
+                    r.score = uu[i].score;
+                    r.strand = (uint8_t)(hh[i].qs >> 31);
+                    per[hp[i]].push_back(r);
+                }
+                for (uint64_t pr = 0; pr < npairs; ++pr) {
+                    auto& v = per[pr];
+                    if (v.empty()) continue;
+                    const uint32_t qa = hqlen[pr / ns], sa = C.slen[pr % ns];
+                    // sort exactly as phase2a_filter does, with every record kept
+                    for (auto& r : v) { r.p_score = INT32_MIN; }
+                    std::vector<UngSurvivor> w = v;
+                    auto ss = [&](const UngSurvivor& r) { return r.strand == 0 ? r.s_start : sa - r.s_end; };
+                    auto qk = [&](const UngSurvivor& r) -> uint64_t {
+                        return r.strand == 0 ? r.q_start : ((uint64_t)qa + 1) + ((uint64_t)qa >= r.q_end ? qa - r.q_end : 0);
+                    };
+                    auto sk = [&](const UngSurvivor& r) { return r.strand == 0 ? r.s_seed : sa - r.s_seed; };
+                    std::sort(w.begin(), w.end(), [&](const UngSurvivor& a, const UngSurvivor& b) {
+                        if (a.score != b.score) return a.score > b.score;
+                        if (ss(a) != ss(b)) return ss(a) < ss(b);
+                        const uint32_t la = a.s_end - a.s_start, lb = b.s_end - b.s_start;
+                        if (la != lb) return la > lb;
+                        if (qk(a) != qk(b)) return qk(a) < qk(b);
+                        return sk(a) < sk(b);
+                    });
+                    for (auto& r : w) {
+                        const uint32_t s0 = r.strand == 0 ? r.s_start : sa - r.s_end;
+                        const uint32_t s1 = r.strand == 0 ? r.s_end : sa - r.s_start;
+                        taps->ungapped->insert(taps->ungapped->end(),
+                                               {(uint32_t)r.strand, r.q_start, r.q_end, s0, s1, (uint32_t)r.score});
+                    }
+                }
+            }
+            if (!taps->prelims) { qb = qe; continue; }
+        }
+
+        // ---- preliminary gapped DP of every ungapped record
+        t0 = std::chrono::steady_clock::now();
+        C.po.ensure(std::max<uint64_t>(nu, 1) * sizeof(PrelimOut));
+        C.wide.ensure(std::max<uint64_t>(nu, 1) * 4);
+        C.n_wide.ensure(16);
+        C.cells.ensure(16);
+        C.fails.ensure(16);
+        CK(cudaMemsetAsync(C.n_wide.p, 0, 16, st));
+        CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
+        CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
+        CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
+                         C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(), C.wide.as<uint32_t>(),
+                         C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(), C.sms, st));
+        uint32_t nw = 0;
+        CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (nw) {
+            uint32_t qmax = 0;
+            for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
+            const uint64_t cap = (uint64_t)std::max(qmax, C.max_slen) + 2;
+            const uint32_t threads = std::min<uint32_t>(nw, (uint32_t)std::max<uint64_t>(128, (1ull << 31) / (cap * 8)));
+            C.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
+            CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(), C.ung_idx.as<uint32_t>(),
+                                  C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
+                                  C.po.as<PrelimOut>(), C.band.as<int2>(), cap, threads,
+                                  C.cells.as<unsigned long long>(), C.fails.as<unsigned int>(), st));
+        }
+        unsigned long long cells = 0;
+        unsigned int fails = 0;
+        CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&fails, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (fails) throw Fail(RMB_ECUDA, "prelim DP band exceeded its storage");
+        ctr.so_cells += cells;
+        ctr.prelim_dp += nu;
+        // survivors (score >= gapped cutoff) to the host
+        C.sel.ensure(std::max<uint64_t>(nu, 1) * 4);
+        tb = 0;
+        CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb, st));
+        C.temp.ensure(tb);
+        CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p, tb, st));
+        uint32_t nsv = 0;
+        CK(cudaMemcpyAsync(&nsv, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        C.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
+        CK(launch_gather_survivors(nsv, C.sel.as<uint32_t>(), C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
+                                   C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
+                                   C.surv.as<SurvivorRec>(), st));
+        std::vector<SurvivorRec> sv(nsv);
+        if (nsv) CK(cudaMemcpyAsync(sv.data(), C.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ctr.ms_prelim_dp += ms_since(t0);
+
+        // ---- host Phase 2a filter per pair
+        t0 = std::chrono::steady_clock::now();
+        std::vector<uint32_t> pair_ids;
+        std::vector<std::vector<UngSurvivor>> per_pair;
+        for (const SurvivorRec& r : sv) {
+            if (pair_ids.empty() || pair_ids.back() != r.pair) {
+                pair_ids.push_back(r.pair);
+                per_pair.emplace_back();
+            }
+            UngSurvivor u{};
+            u.q_seed = r.hit.qs & 0x7fffffffu;
+            u.s_seed = r.hit.s;
+            u.q_start = r.ub.q_start;
+            u.q_end = r.ub.q_end;
+            u.s_start = r.ub.s_start;
+            u.s_end = r.ub.s_end;
+            u.score = r.ub.score;
+            u.strand = (uint8_t)(r.hit.qs >> 31);
+            u.p_score = r.po.score;
+            u.p_qs = r.po.q_start;
+            u.p_qe = r.po.q_end;
+            u.p_ss = r.po.s_start;
+            u.p_se = r.po.s_end;
+            u.tb_q = r.po.tb_q;
+            u.tb_s = r.po.tb_s;
+            per_pair.back().push_back(u);
+        }
+        const size_t np = pair_ids.size();
+        std::vector<std::vector<Prelim>> prelims(np);
+        parallel_for(np, [&](size_t k) {
+            const uint32_t qa = hqlen[pair_ids[k] / ns], sa = C.slen[pair_ids[k] % ns];
+            prelims[k] = phase2a_filter(per_pair[k], qa, sa);
+            sort_prelims_for_traceback(prelims[k], qa, sa);
+        });
+        per_pair.clear();
+        uint64_t n_pre = 0;
+        for (auto& v : prelims) n_pre += v.size();
+        ctr.prelims += n_pre;
+        if (taps && taps->prelims) {
+            // in pipeline (purge) order: re-run the purge order is not kept after the traceback
+            // sort, so report them in traceback order per pair
+            for (size_t k = 0; k < np; ++k)
+                for (const Prelim& p : prelims[k])
+                    taps->prelims->insert(taps->prelims->end(), {(uint32_t)p.strand, p.q_start, p.q_end, p.s_start,
+                                                                 p.s_end, (uint32_t)p.score, p.q_seed, p.s_seed});
+            qb = qe;
+            continue;
+        }
+        ctr.ms_host_2a += ms_since(t0);
+
+        // ---- traceback DP of every prelim (GPU), with retries for scratch overflow
+        t0 = std::chrono::steady_clock::now();
+        std::vector<TbIn> tin;
+        tin.reserve(n_pre);
+        std::vector<uint64_t> pre_off(np + 1, 0);
+        for (size_t k = 0; k < np; ++k) {
+            pre_off[k + 1] = pre_off[k] + prelims[k].size();
+            for (const Prelim& p : prelims[k])
+                tin.push_back(TbIn{pair_ids[k], p.strand, p.q_seed, p.s_seed, p.q_start, p.q_end, p.s_start, p.s_end});
+        }
+        std::vector<TbResult> tres(tin.size());
+        if (!tin.empty()) {
+            uint32_t qmax = 0;
+            for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
+            std::vector<uint32_t> todo(tin.size());
+            for (uint32_t i = 0; i < todo.size(); ++i) todo[i] = i;
+            uint64_t trace_cap = 1ull << 20;
+            uint32_t ops_cap = 1024;
+            int rounds = 0;
+            while (!todo.empty()) {
+                if (++rounds > 12) throw Fail(RMB_ENOMEM, "traceback scratch kept overflowing");
+                std::vector<TbIn> chunk_in(todo.size());
+                for (size_t i = 0; i < todo.size(); ++i) chunk_in[i] = tin[todo[i]];
+                const uint64_t band_cells = (uint64_t)C.max_slen + 2;
+                const uint32_t rows_cap = qmax + 2;
+                const uint64_t per_thread = ((band_cells * 8 + (uint64_t)rows_cap * 8 + trace_cap) + 255) & ~255ull;
+                const uint64_t budget = 8ull << 30;
+                uint32_t threads = (uint32_t)std::min<uint64_t>(todo.size(), std::max<uint64_t>(32, budget / per_thread));
+                threads = (threads + 127) / 128 * 128;
+                upload(C.tb_in, chunk_in, st);
+                C.tb_out.ensure(todo.size() * sizeof(TbOut));
+                C.tb_ops.ensure(todo.size() * (uint64_t)ops_cap * 4);
+                C.tb_scratch.ensure((uint64_t)threads * per_thread);
+                CK(cudaMemsetAsync(C.cells.p, 0, 8, st));
+                CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), C.tb_in.as<TbIn>(),
+                                    C.tb_out.as<TbOut>(), C.tb_ops.as<uint32_t>(), ops_cap, C.tb_scratch.as<uint8_t>(),
+                                    per_thread, band_cells, rows_cap, threads, C.cells.as<unsigned long long>(), st));
+                std::vector<TbOut> to(todo.size());
+                std::vector<uint32_t> ops((uint64_t)todo.size() * ops_cap);
+                CK(cudaMemcpyAsync(to.data(), C.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(ops.data(), C.tb_ops.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                std::vector<uint32_t> again;
+                for (size_t i = 0; i < todo.size(); ++i) {
+                    const TbOut& o = to[i];
+                    if (o.status == 2) { again.push_back(todo[i]); continue; }
+                    if (o.status == 3) throw Fail(RMB_ECUDA, "traceback walk did not reach the origin");
+                    TbResult& r = tres[todo[i]];
+                    r.status = o.status;
+                    r.score = o.score;
+                    r.q0 = o.q0;
+                    r.q1 = o.q1;
+                    r.s0 = o.s0;
+                    r.s1 = o.s1;
+                    r.script.clear();
+                    for (uint32_t k = 0; k < o.n_ops; ++k) {
+                        const uint32_t v = ops[(uint64_t)i * ops_cap + k];
+                        r.script.push_back(RunOp{(uint8_t)(v >> 30), v & 0x3fffffffu});
+                    }
+                }
+                if (again.size() == todo.size()) {  // nothing finished: grow the caps
+                    trace_cap *= 4;
+                    ops_cap *= 4;
+                } else if (!again.empty()) {
+                    trace_cap *= 4;
+                    ops_cap *= 4;
+                }
+                ctr.tb_cells += cells;
+                todo.swap(again);
+            }
+        }
+        ctr.tb_dp += tin.size();
+        ctr.ms_traceback += ms_since(t0);
+
+        // ---- host Phase 2b per pair, then per query
+        t0 = std::chrono::steady_clock::now();
+        std::vector<std::vector<Hit>> pair_hits(np);
+        parallel_for(np, [&](size_t k) {
+            const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
+            const uint8_t* qs = query[qb + qi];
+            std::vector<uint8_t> qrc = revcomp_full(qs, hqlen[qi] + 2);
+            SubjectView v;
+            v.align = C.h_align.data() + C.plus_off[si];
+            v.align_rc = C.h_align_rc.data() + C.plus_off[si];
+            v.n_mask = C.mask_off[si] >= 0 ? C.h_mask.data() + C.mask_off[si] : nullptr;
+            v.n_mask_rc = C.mask_off[si] >= 0 ? C.h_mask_rc.data() + C.mask_off[si] : nullptr;
+            v.len = C.slen[si];
+            std::vector<TbResult> tr(tres.begin() + pre_off[k], tres.begin() + pre_off[k + 1]);
+            pair_hits[k] = phase2b_filter(prelims[k], tr, qs, qrc.data(), hqlen[qi], v, si, C.gp);
+        });
+        for (size_t k = 0; k < np; ++k) {
+            const uint32_t qi = pair_ids[k] / ns;
+            auto& dst = out_hits[qb + qi];
+            for (auto& h : pair_hits[k]) {
+                h.q_len = hqlen[qi];
+                dst.push_back(std::move(h));
+            }
+        }
+        parallel_for(nb, [&](size_t i) {
+            auto& v = out_hits[qb + i];
+            apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
+            sort_hit_list_order(v, C.ids);
+        });
+        for (uint32_t i = 0; i < nb; ++i) ctr.finals += out_hits[qb + i].size();
+        ctr.ms_host_2b += ms_since(t0);
+        qb = qe;
+    }
+}
+
+int fail_out(const std::exception& e, char* err, size_t errlen, int code) {
+    if (err && errlen) {
+        strncpy(err, e.what(), errlen - 1);
+        err[errlen - 1] = 0;
+    }
+    return code;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rmb_version(void) { return "rmblast-b200 0.1 (sm_100a)"; }
+
+int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const double freqs[16], double lambda,
+                   const char* matrix_name, rmb_ctx** out, char* err, size_t errlen) {
+    rmb_ctx* C = nullptr;
+    try {
+        if (!params || !scores || !freqs || !out) throw Fail(RMB_EINVAL, "null argument");
+        const rmb_params& p = *params;
+        if (p.word_size < 4) throw Fail(RMB_EINVAL, "word_size must be at least 4");
+        if (p.gap_open < 0 || p.gap_extend < 1) throw Fail(RMB_EINVAL, "gap costs out of range");
+        if (p.xdrop_ungap < 0 || p.xdrop_gap < 0 || p.xdrop_gap_final < 0 || p.min_raw_gapped_score < 0)
+            throw Fail(RMB_EINVAL, "negative X-drop or cutoff");
+        if (p.dust) throw Fail(RMB_EINVAL, "query DUST masking is not supported by this library (pass dust = 0)");
+        if (p.schedule != 0) throw Fail(RMB_EINVAL, "only the FIFO schedule (0) is supported");
+        C = new rmb_ctx();
+        C->p = p;
+        C->matrix_name = matrix_name ? matrix_name : "";
+        C->gp.gap_open = p.gap_open;
+        C->gp.gap_extend = p.gap_extend;
+        C->gp.gapped_cutoff = p.min_raw_gapped_score > 1 ? p.min_raw_gapped_score : 1;
+        C->gp.complexity_adjust = p.complexity_adjust != 0;
+        for (int i = 0; i < 16; ++i)
+            for (int j = 0; j < 16; ++j) C->gp.matrix[i][j] = scores[i * 16 + j];
+        for (int i = 0; i < 16; ++i) C->gp.freqs[i] = freqs[i];
+        C->gp.lambda = lambda;
+        int ndev = 0;
+        CK(cudaGetDeviceCount(&ndev));
+        if (p.device < 0 || p.device >= ndev) throw Fail(RMB_EINVAL, "no such CUDA device");
+        CK(cudaSetDevice(p.device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, p.device));
+        if (prop.major < 10) throw Fail(RMB_EINVAL, "this library is built for sm_100a (B200)");
+        C->sms = prop.multiProcessorCount;
+        CK(cudaStreamCreateWithFlags(&C->st, cudaStreamNonBlocking));
+        DevParams dp{};
+        dp.gap_open = p.gap_open;
+        dp.gap_extend = p.gap_extend;
+        dp.word_size = p.word_size;
+        dp.xdrop_ungap = p.xdrop_ungap;
+        dp.xdrop_gap = p.xdrop_gap;
+        dp.xdrop_gap_final = p.xdrop_gap_final;
+        dp.gapped_cutoff = C->gp.gapped_cutoff;
+        for (int i = 0; i < 256; ++i) dp.matrix[i] = scores[i];
+        C->d_params.ensure(sizeof(DevParams));
+        CK(cudaMemcpy(C->d_params.p, &dp, sizeof dp, cudaMemcpyHostToDevice));
+        *out = C;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        delete C;
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::exception& e) {
+        delete C;
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+int rmb_db_load(rmb_ctx* C, uint32_t n, const uint8_t* const* plus, const uint32_t* len, const uint8_t* const* n_mask,
+                const char* const* ids, char* err, size_t errlen) {
+    try {
+        if (!C || !plus || !len || !ids) throw Fail(RMB_EINVAL, "null argument");
+        if (n == 0) throw Fail(RMB_EINVAL, "the database contains no sequences");
+        CK(cudaSetDevice(C->p.device));
+        C->ids.assign(ids, ids + n);
+        C->slen.assign(len, len + n);
+        C->plus_off.resize(n);
+        C->packed_off.resize(n);
+        C->mask_off.assign(n, -1);
+        C->h_align.clear();
+        C->h_align_rc.clear();
+        C->h_mask.clear();
+        C->h_mask_rc.clear();
+        std::vector<uint8_t> hplus, hrc, packed;
+        C->total_letters = 0;
+        C->max_slen = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t L = len[i];
+            if (plus[i][0] != 15 || plus[i][L + 1] != 15) throw Fail(RMB_EINVAL, "subject is not sentinel-wrapped");
+            C->total_letters += L;
+            C->max_slen = std::max(C->max_slen, L);
+            C->plus_off[i] = hplus.size();
+            hplus.insert(hplus.end(), plus[i], plus[i] + L + 2);
+            auto rc = revcomp_full(plus[i], L + 2);
+            hrc.insert(hrc.end(), rc.begin(), rc.end());
+            std::vector<uint8_t> al(plus[i], plus[i] + L + 2);
+            if (n_mask && n_mask[i]) {
+                C->mask_off[i] = (int64_t)C->h_mask.size();
+                C->h_mask.insert(C->h_mask.end(), n_mask[i], n_mask[i] + L);
+                for (uint32_t k = 0; k < L; ++k) {
+                    const uint8_t c = n_mask[i][L - 1 - k];
+                    C->h_mask_rc.push_back(c ? COMPL[c & 15] : 0);
+                    if (n_mask[i][k]) al[k + 1] = n_mask[i][k];
+                }
+            }
+            C->h_align.insert(C->h_align.end(), al.begin(), al.end());
+            auto arc = revcomp_full(al.data(), al.size());
+            C->h_align_rc.insert(C->h_align_rc.end(), arc.begin(), arc.end());
+            // blast/util.rs:85-115: 3 pad bytes, 4 bases per byte (first base in bits 7:6), 3 pad bytes.
+            // The plus strand is CRandom-resolved, so every base is 0..3.
+            packed.insert(packed.end(), 3, 0);
+            C->packed_off[i] = packed.size();
+            for (uint32_t j = 0; j < L; j += 4) {
+                uint8_t byte = 0;
+                for (uint32_t k = 0; k < 4; ++k) {
+                    const uint8_t b = j + k < L ? plus[i][1 + j + k] : 0;
+                    if (j + k < L && b > 3) throw Fail(RMB_EINVAL, "subject bases must be CRandom-resolved (0..3)");
+                    byte = (uint8_t)((byte << 2) | (b & 3));
+                }
+                packed.push_back(byte);
+            }
+            packed.insert(packed.end(), 3, 0);
+        }
+        packed.insert(packed.end(), 4, 0);
+        cudaStream_t st = C->st;
+        upload(C->d_plus, hplus, st);
+        upload(C->d_rc, hrc, st);
+        upload(C->d_align, C->h_align, st);
+        upload(C->d_align_rc, C->h_align_rc, st);
+        upload(C->d_packed, packed, st);
+        upload(C->d_plus_off, C->plus_off, st);
+        upload(C->d_packed_off, C->packed_off, st);
+        upload(C->d_len, C->slen, st);
+        CK(cudaStreamSynchronize(st));
+        C->L = DevLib{C->d_plus.as<uint8_t>(),      C->d_rc.as<uint8_t>(),         C->d_align.as<uint8_t>(),
+                      C->d_align_rc.as<uint8_t>(),  C->d_packed.as<uint8_t>(),     C->d_plus_off.as<uint64_t>(),
+                      C->d_packed_off.as<uint64_t>(), C->d_len.as<uint32_t>(), n};
+        C->loaded = true;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+static void check_queries(uint32_t nq, const uint8_t* const* query, const uint32_t* qlen) {
+    if (nq && (!query || !qlen)) throw Fail(RMB_EINVAL, "null argument");
+    for (uint32_t i = 0; i < nq; ++i)
+        if (!query[i] || query[i][0] != 15 || query[i][qlen[i] + 1] != 15)
+            throw Fail(RMB_EINVAL, "query is not sentinel-wrapped BLASTNA");
+}
+
+int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, rmb_results** out,
+                     char* err, size_t errlen) {
+    try {
+        if (!C || !out) throw Fail(RMB_EINVAL, "null argument");
+        if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_search_batch");
+        check_queries(nq, query, qlen);
+        CK(cudaSetDevice(C->p.device));
+        std::vector<std::vector<Hit>> hits;
+        rmb_counters ctr{};
+        run_search(*C, nq, query, qlen, hits, ctr, nullptr);
+        uint64_t nh = 0, nops = 0, nseq = 0;
+        for (auto& v : hits)
+            for (auto& h : v) {
+                ++nh;
+                nops += h.script.size();
+                nseq += h.q_seq.size();
+            }
+        rmb_results* R = (rmb_results*)calloc(1, sizeof(rmb_results));
+        if (!R) throw std::bad_alloc();
+        R->n_queries = nq;
+        R->query_off = (uint64_t*)malloc((nq + 1) * sizeof(uint64_t));
+        R->hsps = (rmb_hsp*)malloc(std::max<uint64_t>(nh, 1) * sizeof(rmb_hsp));
+        R->ops = (uint32_t*)malloc(std::max<uint64_t>(nops, 1) * 4);
+        R->q_seq = (uint8_t*)malloc(std::max<uint64_t>(nseq, 1));
+        R->s_seq = (uint8_t*)malloc(std::max<uint64_t>(nseq, 1));
+        if (!R->query_off || !R->hsps || !R->ops || !R->q_seq || !R->s_seq) {
+            rmb_results_free(R);
+            throw std::bad_alloc();
+        }
+        R->n_hsps = nh;
+        uint64_t k = 0, o = 0, s = 0;
+        for (uint32_t qi = 0; qi < nq; ++qi) {
+            R->query_off[qi] = k;
+            for (auto& h : hits[qi]) {
+                rmb_hsp& x = R->hsps[k++];
+                x.score = h.score;
+                x.q_start = h.q_start; x.q_end = h.q_end; x.q_len = h.q_len;
+                x.s_start = h.s_start; x.s_end = h.s_end; x.s_len = h.s_len;
+                x.subject_oid = h.oid;
+                x.strand = h.strand;
+                x.matches = h.stats.matches; x.mismatches = h.stats.mismatches;
+                x.query_gaps = h.stats.query_gaps; x.subject_gaps = h.stats.subject_gaps;
+                x.transitions = h.stats.transitions; x.transversions = h.stats.transversions;
+                x.cpg_sites = h.stats.cpg_sites;
+                x.perc_sub = h.stats.perc_sub; x.perc_query_gap = h.stats.perc_query_gap;
+                x.perc_db_gap = h.stats.perc_db_gap;
+                x.kdiv = h.stats.kdiv; x.cpg_kdiv = h.stats.cpg_kdiv;
+                x.ops_off = o;
+                x.ops_len = (uint32_t)h.script.size();
+                for (auto& r : h.script) R->ops[o++] = ((uint32_t)r.op << 30) | r.n;
+                x.seq_off = s;
+                x.aln_len = (uint32_t)h.q_seq.size();
+                memcpy(R->q_seq + s, h.q_seq.data(), h.q_seq.size());
+                memcpy(R->s_seq + s, h.s_seq.data(), h.s_seq.size());
+                s += h.q_seq.size();
+            }
+        }
+        R->query_off[nq] = k;
+        R->counters = ctr;
+        *out = R;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, int32_t stage,
+                    uint32_t** records, uint64_t* n_records, char* err, size_t errlen) {
+    try {
+        if (!C || !records || !n_records) throw Fail(RMB_EINVAL, "null argument");
+        if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_debug_stage");
+        if (stage < 0 || stage > 2) throw Fail(RMB_EINVAL, "stage must be 0, 1 or 2");
+        check_queries(nq, query, qlen);
+        CK(cudaSetDevice(C->p.device));
+        std::vector<uint32_t> v;
+        Taps t;
+        if (stage == 0) t.seeds = &v;
+        else if (stage == 1) t.ungapped = &v;
+        else t.prelims = &v;
+        std::vector<std::vector<Hit>> hits;
+        rmb_counters ctr{};
+        run_search(*C, nq, query, qlen, hits, ctr, &t);
+        const uint64_t width = stage == 0 ? 3 : stage == 1 ? 6 : 8;
+        uint32_t* r = (uint32_t*)malloc(std::max<size_t>(v.size(), 1) * 4);
+        if (!r) throw std::bad_alloc();
+        if (!v.empty()) memcpy(r, v.data(), v.size() * 4);
+        *records = r;
+        *n_records = v.size() / width;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+int rmb_format_tabular(const rmb_ctx* C, const rmb_results* R, const char* const* query_ids, const char* outfmt,
+                       char** text, size_t* text_len, char* err, size_t errlen) {
+    try {
+        if (!C || !R || !outfmt || !text) throw Fail(RMB_EINVAL, "null argument");
+        std::istringstream is(outfmt);
+        std::string t;
+        std::vector<std::string> fields;
+        is >> t;
+        if (t != "6") throw Fail(RMB_EINVAL, "output format '" + t + "' is not supported; use 6 <fields>");
+        while (is >> t) fields.push_back(t);
+        if (fields.empty()) throw Fail(RMB_EINVAL, "-outfmt 6 needs a field list");
+        std::string out;
+        Hit h;
+        for (uint32_t qi = 0; qi < R->n_queries; ++qi) {
+            const std::string qid = query_ids ? query_ids[qi] : ("query" + std::to_string(qi));
+            for (uint64_t k = R->query_off[qi]; k < R->query_off[qi + 1]; ++k) {
+                const rmb_hsp& x = R->hsps[k];
+                h.score = x.score;
+                h.q_start = x.q_start; h.q_end = x.q_end; h.q_len = x.q_len;
+                h.s_start = x.s_start; h.s_end = x.s_end; h.s_len = x.s_len;
+                h.oid = x.subject_oid;
+                h.strand = (uint8_t)x.strand;
+                h.stats.matches = x.matches; h.stats.mismatches = x.mismatches;
+                h.stats.query_gaps = x.query_gaps; h.stats.subject_gaps = x.subject_gaps;
+                h.stats.transitions = x.transitions; h.stats.transversions = x.transversions;
+                h.stats.cpg_sites = x.cpg_sites;
+                h.stats.perc_sub = x.perc_sub; h.stats.perc_query_gap = x.perc_query_gap;
+                h.stats.perc_db_gap = x.perc_db_gap;
+                h.stats.kdiv = x.kdiv; h.stats.cpg_kdiv = x.cpg_kdiv;
+                h.q_seq.assign(R->q_seq + x.seq_off, R->q_seq + x.seq_off + x.aln_len);
+                h.s_seq.assign(R->s_seq + x.seq_off, R->s_seq + x.seq_off + x.aln_len);
+                if (!format_line(out, h, qid, C->ids.at(x.subject_oid), fields))
+                    throw Fail(RMB_EINVAL, "unknown -outfmt field");
+                out.push_back('\n');
+            }
+        }
+        char* o = (char*)malloc(out.size() + 1);
+        if (!o) throw std::bad_alloc();
+        memcpy(o, out.data(), out.size());
+        o[out.size()] = 0;
+        *text = o;
+        if (text_len) *text_len = out.size();
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+void rmb_results_free(rmb_results* R) {
+    if (!R) return;
+    free(R->query_off);
+    free(R->hsps);
+    free(R->ops);
+    free(R->q_seq);
+    free(R->s_seq);
+    free(R);
+}
+
+void rmb_text_free(void* p) { free(p); }
+
+void rmb_ctx_destroy(rmb_ctx* C) {
+    if (!C) return;
+    cudaSetDevice(C->p.device);
+    DBuf* all[] = {&C->d_plus, &C->d_rc, &C->d_align, &C->d_align_rc, &C->d_packed, &C->d_plus_off, &C->d_packed_off,
+                   &C->d_len, &C->d_params, &C->q, &C->qrc, &C->qoff, &C->qlen, &C->pv, &C->pv_off, &C->cs, &C->cs_off,
+                   &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
+                   &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->n_wide, &C->band,
+                   &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
+                   &C->tb_scratch};
+    for (DBuf* b : all) b->release();
+    if (C->st) cudaStreamDestroy(C->st);
+    delete C;
+}
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// rmb_glue.hpp -- host steps of the search core that are order-dependent per (query, subject)
+// pair and cost O(HSPs), not O(cells): the interval-tree filters, the endpoint purges, the
+// cut/re-evaluation of common-endpoint HSPs, complexity adjustment, alignment statistics,
+// masklevel and the output order.  The DP and scan work they consume comes from the GPU.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rmb {
+
+enum : uint8_t { OP_SUB = 0, OP_GAP_Q = 1, OP_GAP_S = 2 };  // hits.rs:21-31 EditOp
+struct RunOp { uint8_t op; uint32_t n; };
+using Script = std::vector<RunOp>;
+
+struct Stats {
+    uint32_t matches = 0, mismatches = 0, query_gaps = 0, subject_gaps = 0;
+    uint32_t transitions = 0, transversions = 0, cpg_sites = 0;
+    double kdiv = 0, cpg_kdiv = 0;
+    float perc_sub = 0, perc_query_gap = 0, perc_db_gap = 0;
+};
+
+struct Hit {  // output.rs:132 AlignResult
+    int32_t score = 0;
+    uint32_t q_start = 0, q_end = 0, q_len = 0, s_start = 0, s_end = 0, s_len = 0;
+    uint32_t oid = 0;
+    uint8_t strand = 0;  // 0 plus, 1 minus
+    Script script;
+    std::vector<uint8_t> q_seq, s_seq;
+    Stats stats;
+};
+
+// The host views of one subject the glue reads (sentinel-wrapped BLASTNA).
+struct SubjectView {
+    const uint8_t* align;     // IUB-restored plus strand
+    const uint8_t* align_rc;  // its reverse complement
+    const uint8_t* n_mask;    // nullptr or len bytes
+    const uint8_t* n_mask_rc; // nullptr or len bytes
+    uint32_t len;
+};
+
+struct GlueParams {
+    int32_t gap_open, gap_extend, gapped_cutoff;
+    bool complexity_adjust;
+    int32_t matrix[16][16];
+    double freqs[16];
+    double lambda;
+};
+
+// An ungapped record that passed the GPU prelim DP with a score >= the gapped cutoff.
+struct UngSurvivor {
+    uint32_t q_seed, s_seed, q_start, q_end, s_start, s_end;  // record frame
+    int32_t score;
+    uint8_t strand;
+    // prelim DP result (record frame) and traceback seed
+    int32_t p_score;
+    uint32_t p_qs, p_qe, p_ss, p_se, tb_q, tb_s;
+};
+struct Prelim {  // engine.rs:158-169 PrelimHsp
+    uint32_t q_seed, s_seed, q_start, q_end, s_start, s_end;
+    int32_t score;
+    uint8_t strand;
+};
+
+// engine.rs:1280-1411 + 1969-2083: sort, contain-filter and purge one pair's survivors.
+std::vector<Prelim> phase2a_filter(std::vector<UngSurvivor>& surv, uint32_t qa, uint32_t sa);
+
+// A traceback result from the GPU for one prelim (DP frame: query_rc for minus).
+struct TbResult {
+    int32_t status;
+    int32_t score;
+    uint32_t q0, q1, s0, s1;
+    Script script;
+};
+
+// engine.rs:1438-1762 on one pair: prelims (post purge, pipeline order) with their GPU
+// traceback results; returns the pair's final HSPs.
+std::vector<Hit> phase2b_filter(std::vector<Prelim>& prelims, std::vector<TbResult>& tbs, const uint8_t* query,
+                                const uint8_t* query_rc, uint32_t qa, const SubjectView& sv, uint32_t oid,
+                                const GlueParams& gp);
+
+// The stable order phase2b_filter processes prelims in (engine.rs:1471-1485); the caller
+// sorts before launching tracebacks so both sides agree.
+void sort_prelims_for_traceback(std::vector<Prelim>& p, uint32_t qa, uint32_t sa);
+
+// engine.rs:863-974 (cross-subject mode) and main.rs:1230-1234 + engine.rs:998-1017.
+void apply_mask_level(std::vector<Hit>& hits, uint32_t mask_level);
+void sort_hit_list_order(std::vector<Hit>& hits, const std::vector<std::string>& subject_ids);
+
+// output.rs:294-367 one tabular line (no newline); returns false on an unknown field.
+bool format_line(std::string& out, const Hit& h, const std::string& qid, const std::string& sid,
+                 const std::vector<std::string>& fields);
+
+int choose_lut_width(int word_size, uint64_t approx_entries);
+int ungapped_cutoff_for(const std::string& matrix_name, int go, int ge, int min_raw, uint64_t qlen, uint64_t avg);
+Stats align_stats(const std::vector<uint8_t>& q, const std::vector<uint8_t>& s);
+
+}  // namespace rmb

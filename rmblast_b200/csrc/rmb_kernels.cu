@@ -1,0 +1,1046 @@
+// rmb_kernels.cu -- sm_100a kernels of the search core.
+//
+//   k_scan        lookup-table scan of the packed library + exact word extension
+//                 (blast/nascan.rs, blast/mblookup.rs:247-343, engine.rs:1118-1218); a warp per
+//                 (query, subject) pair, lanes on consecutive scan offsets, two passes (count,
+//                 then write at the pair's prefix offset) so every pair's hits keep scan order.
+//   k_ungapped    ungapped X-drop extension of every word hit (search/ungapped.rs:38-121),
+//                 one thread per hit, computed for all hits ahead of the dedup.
+//   k_dedup       the order-dependent diagonal hash (search/diag_hash.rs) replayed per pair in
+//                 scan order on the precomputed extensions, one thread per pair.
+//   k_prelim      preliminary score-only X-drop DP (search/gapped.rs:124-418) of every ungapped
+//                 record, one thread per record, the DP band in a shared-memory ring;
+//                 k_prelim_wide reruns the records whose band outgrew the ring with the band in
+//                 global memory.
+//   k_traceback   improve_seed + traceback X-drop DP + trace walk (engine.rs:383-572,
+//                 engine.rs:2953-3039, search/gapped.rs:450-757), one thread per prelim HSP.
+//
+// All scores are int32; the arithmetic and the order of every comparison follow the cited
+// reference functions so results are bit-identical.
+#include <cstdint>
+#include <cstdio>
+
+#include "rmb_device.cuh"
+#include "rmb_kernels.hpp"
+
+namespace rmb {
+
+// ---------------------------------------------------------------------------------------
+// scan
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t kmer_at(const uint8_t* pk, uint32_t p, int lw) {
+    const uint8_t* b = pk + (p >> 2);
+    uint32_t raw = ((uint32_t)b[0] << 24) | ((uint32_t)b[1] << 16) | ((uint32_t)b[2] << 8) | (uint32_t)b[3];
+    uint32_t sh = 2u * (16u - (p & 3u) - (uint32_t)lw);
+    return (raw >> sh) & ((1u << (2 * lw)) - 1u);
+}
+
+struct PairView {
+    const uint8_t* qmask;  // sentinel-wrapped
+    const uint8_t* splus;  // sentinel-wrapped
+    const uint8_t* src;    // sentinel-wrapped
+    int64_t qlen, slen;
+    int lw, ext_needed;
+};
+
+// engine.rs:1118-1149 (plus) and 1187-1218 (minus): exact extension to word_size on the
+// masked query; returns false if the word hit is dropped.
+__device__ __forceinline__ bool exact_extend(const PairView& v, uint32_t q0c, uint32_t p, uint32_t& qs, uint32_t& so) {
+    const int64_t c1 = v.qlen + 1;
+    const int64_t lw = v.lw, need = v.ext_needed;
+    if ((int64_t)q0c < c1) {
+        int64_t el = 0, er = 0;
+        if (need > 0) {
+            while (el < need) {
+                int64_t qi = (int64_t)q0c - el - 1, si = (int64_t)p - el - 1;
+                if (qi < 0 || si < 0) break;
+                uint8_t qb = v.qmask[1 + qi], sb = v.splus[1 + si];
+                if (qb >= 4 || sb >= 4 || qb != sb) break;
+                ++el;
+            }
+            while (el + er < need) {
+                int64_t qi = (int64_t)q0c + lw + er, si = (int64_t)p + lw + er;
+                if (qi >= v.qlen || si >= v.slen) break;
+                uint8_t qb = v.qmask[1 + qi], sb = v.splus[1 + si];
+                if (qb >= 4 || sb >= 4 || qb != sb) break;
+                ++er;
+            }
+            if (el + er < need) return false;
+        }
+        qs = (uint32_t)((int64_t)q0c - el);
+        so = (uint32_t)((int64_t)p - el);
+        return true;
+    }
+    const int64_t rcq = (int64_t)q0c - c1;
+    const int64_t q0 = v.qlen - rcq - lw, s0 = v.slen - (int64_t)p - lw;
+    if (q0 < 0 || s0 < 0) return false;
+    int64_t el = 0, er = 0;
+    if (need > 0) {
+        while (er < need) {
+            int64_t qi = q0 + lw + er, si = s0 + lw + er;
+            if (qi >= v.qlen || si >= v.slen) break;
+            uint8_t qb = v.qmask[1 + qi], sb = v.src[1 + si];
+            if (qb >= 4 || sb >= 4 || qb != sb) break;
+            ++er;
+        }
+        while (el + er < need) {
+            int64_t qi = q0 - el - 1, si = s0 - el - 1;
+            if (qi < 0 || si < 0) break;
+            uint8_t qb = v.qmask[1 + qi], sb = v.src[1 + si];
+            if (qb >= 4 || sb >= 4 || qb != sb) break;
+            ++el;
+        }
+        if (el + er < need) return false;
+    }
+    qs = (uint32_t)(q0 + er) | 0x80000000u;
+    so = (uint32_t)(s0 + er);
+    return true;
+}
+
+template <bool WRITE>
+__global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
+                                               uint32_t* counts, const uint64_t* offs, SeedHit* hits,
+                                               uint32_t* hit_pair) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t w = warp; w < n_pairs; w += nwarps) {
+        const uint64_t pair = pair0 + w;
+        const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
+        const uint32_t qlen = Q.len[qi], slen = L.len[si];
+        uint64_t out = WRITE ? offs[w] : 0;
+        uint32_t total = 0;
+        if (qlen >= (uint32_t)ws && slen >= (uint32_t)ws) {
+            PairView v;
+            v.qmask = Q.qmask + Q.off[qi];
+            v.splus = L.plus + L.plus_off[si];
+            v.src = L.rc + L.plus_off[si];
+            v.qlen = qlen;
+            v.slen = slen;
+            v.lw = Q.lw[qi];
+            v.ext_needed = ws - v.lw;
+            const uint32_t step = (uint32_t)(ws - v.lw + 1);
+            const uint32_t npos = (slen - (uint32_t)v.lw) / step + 1;
+            const uint8_t* pk = L.packed + L.packed_off[si];
+            const uint32_t* pv = Q.pv + Q.pv_off[qi];
+            const uint32_t* cs = Q.cell_start + Q.cs_off[qi];
+            const uint32_t* cq = Q.cell_q + Q.cq_off[qi];
+            for (uint32_t k0 = 0; k0 < npos; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                uint32_t c = 0, b = 0, e = 0, p = 0;
+                if (k < npos) {
+                    p = k * step;
+                    const uint32_t idx = kmer_at(pk, p, v.lw);
+                    if (__ldg(pv + (idx >> 5)) & (1u << (idx & 31))) {
+                        b = __ldg(cs + idx);
+                        e = __ldg(cs + idx + 1);
+                        for (uint32_t j = b; j < e; ++j) {
+                            uint32_t qs, so;
+                            if (exact_extend(v, __ldg(cq + j), p, qs, so)) ++c;
+                        }
+                    }
+                }
+                uint32_t incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const uint32_t wsum = __shfl_sync(0xffffffffu, incl, 31);
+                if (WRITE && c) {
+                    uint64_t o = out + total + (incl - c);
+                    for (uint32_t j = b; j < e; ++j) {
+                        uint32_t qs, so;
+                        if (exact_extend(v, __ldg(cq + j), p, qs, so)) {
+                            hits[o] = SeedHit{qs, so};
+                            hit_pair[o] = (uint32_t)pair;
+                            ++o;
+                        }
+                    }
+                }
+                total += wsum;
+            }
+        }
+        if (!WRITE && lane == 0) counts[w] = total;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// ungapped extension: search/ungapped.rs:38-121
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void extend_ungapped(const uint8_t* query, int64_t q_real, const uint8_t* subject,
+                                                int64_t s_real, uint32_t q_off, uint32_t s_off, const int32_t* mat,
+                                                int32_t xdrop, int32_t& score_out, uint32_t& qs_out, uint32_t& qe_out,
+                                                uint32_t& ss_out, uint32_t& se_out) {
+    const int32_t x = -xdrop;
+    const int64_t qo = q_off, so = s_off;
+    int32_t score = 0, sum = 0;
+    int64_t q_beg = qo;
+    {
+        int64_t q = qo - 1, s = so - 1;
+        while (q >= 0 && s >= 0) {
+            const uint8_t qb = query[1 + q], sb = subject[1 + s];
+            if (qb == 15 || sb == 15) break;
+            sum += mat[((qb & 15) << 4) | (sb & 15)];
+            if (sum > 0) {
+                q_beg = q;
+                score += sum;
+                sum = 0;
+            } else if (sum < x) {
+                break;
+            }
+            --q;
+            --s;
+        }
+    }
+    int64_t q_end = qo;
+    int32_t xc = x;
+    sum = 0;
+    {
+        int64_t q = qo, s = so;
+        while (q < q_real && s < s_real) {
+            const uint8_t qb = query[1 + q], sb = subject[1 + s];
+            if (qb == 15 || sb == 15) break;
+            sum += mat[((qb & 15) << 4) | (sb & 15)];
+            if (sum > 0) {
+                q_end = q + 1;
+                score += sum;
+                xc = (-score > x) ? -score : x;
+                sum = 0;
+            } else if (sum < xc) {
+                break;
+            }
+            ++q;
+            ++s;
+        }
+    }
+    score_out = score;
+    qs_out = (uint32_t)q_beg;
+    qe_out = (uint32_t)q_end;
+    ss_out = (uint32_t)(so - (qo - q_beg));
+    se_out = (uint32_t)(so + (q_end - qo));
+}
+
+// engine.rs:1165-1170 (plus) and 1244-1261 (minus): the extension in NCBI's frame, its box in
+// the record frame, and the value the diagonal hash stores for the seed.
+__global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                   int32_t ucut, uint64_t n, const SeedHit* __restrict__ hits,
+                                                   const uint32_t* __restrict__ hit_pair, UngBox* __restrict__ out) {
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    const int32_t ws = P->word_size, xd = P->xdrop_ungap;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const SeedHit h = hits[i];
+        const uint32_t pair = hit_pair[i];
+        const uint32_t qi = pair / L.n, si = pair % L.n;
+        const uint32_t qlen = Q.len[qi], slen = L.len[si];
+        const uint8_t* sp = L.plus + L.plus_off[si];
+        const uint32_t qo = h.qs & 0x7fffffffu, so = h.s;
+        UngBox u;
+        int32_t sc;
+        uint32_t a, b, c, d;
+        if (!(h.qs >> 31)) {
+            extend_ungapped(Q.q + Q.off[qi], qlen, sp, slen, qo, so, mat, xd, sc, a, b, c, d);
+            u.score = sc;
+            u.q_start = a;
+            u.q_end = b;
+            u.s_start = c;
+            u.s_end = d;
+            u.store = sc >= ucut ? d : so + (uint32_t)ws;
+        } else {
+            const uint32_t qn = qlen - 1 - qo, sn = slen - 1 - so;
+            extend_ungapped(Q.qrc + Q.off[qi], qlen, sp, slen, qn, sn, mat, xd, sc, a, b, c, d);
+            u.score = sc;
+            u.q_start = qlen - b;
+            u.q_end = qlen - a;
+            u.s_start = slen - d;
+            u.s_end = slen - c;
+            const uint32_t key = slen - so - (uint32_t)Q.lw[qi];
+            u.store = sc >= ucut ? d : key + (uint32_t)ws;
+        }
+        out[i] = u;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// diagonal dedup: search/diag_hash.rs:24-111 replayed in scan order (engine.rs:1151-1170,
+// 1220-1261).  flags[i]: 0 = dropped by the hash, 1 = seed, 3 = seed kept as an ungapped hit.
+// ---------------------------------------------------------------------------------------
+struct DiagCell { int32_t diag; uint32_t level, next; };
+
+__device__ __forceinline__ uint32_t diag_bucket(int32_t d) { return ((uint32_t)d * 0x9E370001u) % 512u; }
+
+__device__ void dedup_pair(uint32_t tag, uint64_t b, uint64_t e, int32_t ws, int32_t lw, uint32_t qlen, uint32_t slen,
+                           int32_t ucut, const SeedHit* __restrict__ hits, const UngBox* __restrict__ ub,
+                           uint8_t* __restrict__ flags, uint32_t* bb, uint32_t* bt, DiagCell* cells) {
+    const int32_t window = 1 - ws;
+    uint32_t occ = 1;  // cells are 1-based, cells[k - 1] holds cell k
+    for (uint64_t i = b; i < e; ++i) {
+        const SeedHit h = hits[i];
+        const uint32_t qo = h.qs & 0x7fffffffu, so = h.s;
+        int32_t diag;
+        uint32_t key;
+        if (!(h.qs >> 31)) {
+            diag = (int32_t)(so - qo);
+            key = so;
+        } else {
+            diag = (int32_t)(slen - 2u * qlen - 1u + (qo - so));
+            key = slen - so - (uint32_t)lw;
+        }
+        const uint32_t bk = diag_bucket(diag);
+        const uint32_t head = bt[bk] == tag ? bb[bk] : 0u;
+        uint32_t last = 0;
+        for (uint32_t c = head; c; c = cells[c - 1].next)
+            if (cells[c - 1].diag == diag) { last = cells[c - 1].level; break; }
+        if (key < last) { flags[i] = 0; continue; }
+        const UngBox u = ub[i];
+        flags[i] = u.score >= ucut ? 3 : 1;
+        bool done = false;
+        for (uint32_t c = head; c; c = cells[c - 1].next) {
+            DiagCell& cl = cells[c - 1];
+            if (cl.diag == diag) { cl.level = u.store; done = true; break; }
+            if ((int32_t)(key - cl.level) > window) { cl.diag = diag; cl.level = u.store; done = true; break; }
+        }
+        if (!done) {
+            cells[occ - 1] = DiagCell{diag, u.store, head};
+            bb[bk] = occ;
+            bt[bk] = tag;
+            ++occ;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_dedup(DevLib L, DevQueries Q, int32_t ws, int32_t ucut, uint64_t pair0,
+                                                uint64_t n_pairs, const uint64_t* __restrict__ offs,
+                                                const SeedHit* __restrict__ hits, const UngBox* __restrict__ ub,
+                                                uint8_t* __restrict__ flags, uint32_t* __restrict__ scratch,
+                                                DiagCell* __restrict__ cells) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t* bb = scratch + tid * 1024;
+    uint32_t* bt = bb + 512;
+    for (int k = 0; k < 512; ++k) bt[k] = 0;
+    for (uint64_t w = tid; w < n_pairs; w += nth) {
+        const uint64_t b = offs[w], e = offs[w + 1];
+        if (b == e) continue;
+        const uint64_t pair = pair0 + w;
+        const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
+        dedup_pair((uint32_t)w + 1u, b, e, ws, Q.lw[qi], Q.len[qi], L.len[si], ucut, hits, ub, flags, bb, bt, cells + b);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// score-only X-drop DP: search/gapped.rs:124-337 (outer sequence a, inner sequence b)
+// ---------------------------------------------------------------------------------------
+struct RingBand {  // band cells b live at ring[b & (W-1)]; valid while the band is < W wide
+    int2* ring;
+    uint32_t mask;
+    __device__ __forceinline__ int2 get(uint32_t b) const { return ring[b & mask]; }
+    __device__ __forceinline__ void set(uint32_t b, int2 v) { ring[b & mask] = v; }
+    __device__ __forceinline__ void set_best(uint32_t b, int32_t v) { ring[b & mask].x = v; }
+    __device__ __forceinline__ bool fits(uint32_t b, uint32_t first_b) const { return b - first_b <= mask; }
+};
+struct FlatBand {  // band cells at absolute index b; capacity >= n + 2
+    int2* cell;
+    __device__ __forceinline__ int2 get(uint32_t b) const { return cell[b]; }
+    __device__ __forceinline__ void set(uint32_t b, int2 v) { cell[b] = v; }
+    __device__ __forceinline__ void set_best(uint32_t b, int32_t v) { cell[b].x = v; }
+    __device__ __forceinline__ bool fits(uint32_t, uint32_t) const { return true; }
+};
+
+struct DpResult { int32_t score; uint32_t a_len, b_len; };
+
+// Returns false if the band outgrew the storage.  b bytes are BLASTNA codes (0..15).
+template <bool REVERSE, class Band>
+__device__ bool so_dp(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint32_t m, uint32_t n, int32_t go,
+                      int32_t ge, int32_t x_dropoff, const int32_t* __restrict__ mat, Band band, DpResult& res,
+                      uint64_t& cells) {
+    res = DpResult{0, 0, 0};
+    if (m == 0 || n == 0) return true;
+    const int32_t goe = go + ge;
+    const int32_t xdrop = x_dropoff > goe ? x_dropoff : goe;
+    band.set(0, make_int2(0, -goe));
+    int32_t score = -goe;
+    uint32_t b_size = 1;
+    for (uint32_t j = 1; j <= n; ++j) {
+        if (score < -xdrop) break;
+        if (!band.fits(j, 0)) return false;
+        band.set(j, make_int2(score, score - goe));
+        score -= ge;
+        b_size = j + 1;
+    }
+    int32_t best = 0;
+    uint32_t best_a = 0, best_b = 0, first_b = 0;
+    for (uint32_t ai = 0; ai < m; ++ai) {
+        const uint32_t ap = REVERSE ? m - 1 - ai : ai;
+        const int32_t* row = mat + ((a[ap] & 15) << 4);
+        int32_t sc = MININT, gap_row = MININT;
+        uint32_t last_b = first_b;
+        const int32_t prev_best = best;
+        cells += b_size - first_b;
+        for (uint32_t bi = first_b; bi < b_size; ++bi) {
+            const int2 c = band.get(bi);
+            int32_t next_score = 0;
+            if (bi < n) next_score = c.x + row[b[REVERSE ? n - 1 - bi : bi]];
+            int32_t cell = sc;
+            if (c.y > cell) cell = c.y;
+            if (gap_row > cell) cell = gap_row;
+            if (best - cell > xdrop) {
+                if (bi == first_b) ++first_b;
+                else band.set_best(bi, MININT);
+            } else {
+                last_b = bi;
+                if (cell > best) { best_b = bi; best = cell; }
+                gap_row -= ge;
+                const int32_t open = cell - goe;
+                const int32_t col_ext = c.y - ge;
+                band.set(bi, make_int2(cell, col_ext > open ? col_ext : open));
+                if (open > gap_row) gap_row = open;
+            }
+            sc = next_score;
+        }
+        if (best > prev_best) best_a = ai + 1;
+        if (first_b >= b_size) break;
+        if (last_b + 1 < b_size) {
+            b_size = last_b + 1;
+        } else {
+            while (gap_row >= best - xdrop && b_size <= n) {
+                if (!band.fits(b_size, first_b)) return false;
+                band.set(b_size, make_int2(gap_row, gap_row - goe));
+                gap_row -= ge;
+                ++b_size;
+            }
+        }
+        if (b_size <= n) {
+            if (!band.fits(b_size, first_b)) return false;
+            band.set(b_size, make_int2(MININT, MININT));
+            ++b_size;
+        }
+    }
+    res = DpResult{best, best_a, best_b};
+    return true;
+}
+
+// engine.rs:1850-1895 prelim_pivot: (pivot_q, pivot_s, tb_q, tb_s)
+__device__ __forceinline__ void prelim_pivot(bool plus, uint32_t q_seed, uint32_t s_seed, uint32_t s_start,
+                                             uint32_t s_end, uint32_t qa, uint32_t sa, uint32_t lw, uint32_t o[4]) {
+    if (plus) {
+        uint32_t tq = q_seed, ts = s_seed;
+        if (s_end >= s_seed + 8) { tq += 3; ts += 3; }
+        const uint32_t oa = 4 - (ts % 4);
+        uint32_t ps = ts + oa, pq = tq + oa;
+        if (ps >= sa || pq >= qa) { ps -= 4; pq -= 4; }
+        o[0] = pq; o[1] = ps; o[2] = tq; o[3] = ts;
+    } else {
+        const uint32_t saved = sa - s_seed - lw;
+        const uint32_t s_end_fwd = sa - s_start;
+        const bool ext = s_end_fwd >= saved + 8;
+        uint32_t tq = q_seed, ts = s_seed;
+        if (ext) { tq = q_seed + lw - 4; ts = s_seed + lw - 4; }
+        const uint32_t shift = ext ? 3 : 0;
+        const uint32_t qn = (qa - q_seed - lw) + shift, sn = (sa - s_seed - lw) + shift;
+        const uint32_t oa = 4 - (sn % 4);
+        uint32_t ql = qn + oa, sl = sn + oa;
+        if (ql > qa || sl > sa) { ql -= 4; sl -= 4; }
+        o[0] = ql; o[1] = sl; o[2] = tq; o[3] = ts;
+    }
+}
+
+// One record of engine.rs:1350-1397: pivot, X = min(xdrop_gap, ungapped score), the two
+// score-only extensions (gapped.rs:360-418), frame conversion and the gapped cutoff.
+template <class BandL, class BandR>
+__device__ bool prelim_one(const DevLib& L, const DevQueries& Q, const DevParams* P, const int32_t* mat,
+                           uint32_t pair, const SeedHit h, const UngBox u, BandL bl, BandR br, PrelimOut& out,
+                           uint64_t& cells) {
+    const uint32_t qi = pair / L.n, si = pair % L.n;
+    const uint32_t qa = Q.len[qi], sa = L.len[si];
+    const bool plus = !(h.qs >> 31);
+    uint32_t piv[4];
+    prelim_pivot(plus, h.qs & 0x7fffffffu, h.s, u.s_start, u.s_end, qa, sa, (uint32_t)Q.lw[qi], piv);
+    const int32_t xd = P->xdrop_gap < u.score ? P->xdrop_gap : u.score;
+    const uint8_t* qseq = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
+    const uint8_t* sseq = L.plus + L.plus_off[si] + 1;
+    const uint32_t qp = piv[0], sp = piv[1];
+    DpResult l, r{0, 0, 0};
+    if (!so_dp<true>(sseq, qseq, sp, qp, P->gap_open, P->gap_extend, xd, mat, bl, l, cells)) return false;
+    const uint32_t rm = sa > sp ? sa - sp : 0, rn = qa > qp ? qa - qp : 0;
+    if (rm > 0 && rn > 0)
+        if (!so_dp<false>(sseq + sp, qseq + qp, rm, rn, P->gap_open, P->gap_extend, xd, mat, br, r, cells)) return false;
+    const int32_t total = l.score + r.score;
+    out.score = INT32_MIN;
+    if (total < 0) return true;
+    uint32_t q0 = qp - l.b_len, s0 = sp - l.a_len, q1 = qp + r.b_len, s1 = sp + r.a_len;
+    if (!plus) {
+        const uint32_t t0 = qa - q1, t1 = qa - q0, t2 = sa - s1, t3 = sa - s0;
+        q0 = t0; q1 = t1; s0 = t2; s1 = t3;
+    }
+    if (total < P->gapped_cutoff) return true;
+    out = PrelimOut{total, q0, q1, s0, s1, piv[2], piv[3]};
+    return true;
+}
+
+template <int W>
+__global__ void __launch_bounds__(128) k_prelim(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint64_t n,
+                                                 const uint32_t* __restrict__ idx, const SeedHit* __restrict__ hits,
+                                                 const uint32_t* __restrict__ hit_pair, const UngBox* __restrict__ ub,
+                                                 PrelimOut* __restrict__ out, uint32_t* __restrict__ wide,
+                                                 unsigned int* __restrict__ n_wide,
+                                                 unsigned long long* __restrict__ cells_total) {
+    extern __shared__ int2 smem_ring[];
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    RingBand band{smem_ring + threadIdx.x * W, W - 1};
+    uint64_t cells = 0;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = idx[t];
+        PrelimOut o{INT32_MIN, 0, 0, 0, 0, 0, 0};
+        uint64_t c = 0;
+        if (prelim_one(L, Q, P, mat, hit_pair[i], hits[i], ub[i], band, band, o, c)) {
+            out[t] = o;
+            cells += c;
+        } else {
+            const unsigned int k = atomicAdd(n_wide, 1u);
+            wide[k] = (uint32_t)t;
+        }
+    }
+    for (int o = 16; o; o >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o);
+    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// The records whose band outgrew the ring, with the band at absolute indices in global memory
+// (`band_cap` cells per thread, at least the longest inner sequence + 2).
+__global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                      uint32_t n_wide, const uint32_t* __restrict__ wide,
+                                                      const uint32_t* __restrict__ idx, const SeedHit* __restrict__ hits,
+                                                      const uint32_t* __restrict__ hit_pair,
+                                                      const UngBox* __restrict__ ub, PrelimOut* __restrict__ out,
+                                                      int2* __restrict__ band_mem, uint64_t band_cap,
+                                                      unsigned long long* __restrict__ cells_total,
+                                                      unsigned int* __restrict__ failures) {
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    FlatBand band{band_mem + tid * band_cap};
+    uint64_t cells = 0;
+    for (uint64_t k = tid; k < n_wide; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = wide[k];
+        const uint32_t i = idx[t];
+        PrelimOut o{INT32_MIN, 0, 0, 0, 0, 0, 0};
+        uint64_t c = 0;
+        if (!prelim_one(L, Q, P, mat, hit_pair[i], hits[i], ub[i], band, band, o, c)) atomicAdd(failures, 1u);
+        out[t] = o;
+        cells += c;
+    }
+    if (cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// ---------------------------------------------------------------------------------------
+// traceback: engine.rs:383-572 improve_seed, search/gapped.rs:450-757 align_ex +
+// traceback_flat, engine.rs:2953-3039 gapped_extend_bidirectional
+// ---------------------------------------------------------------------------------------
+constexpr uint8_t T_GAP_A = 0, T_SUB = 3, T_GAP_B = 6, T_MASK = 7, T_EXT_A = 0x10, T_EXT_B = 0x40;
+
+__device__ __forceinline__ uint32_t satsub(uint32_t a, uint32_t b) { return a > b ? a - b : 0; }
+
+__device__ void improve_seed(const uint8_t* query, uint32_t qlen, const uint8_t* subject, uint32_t slen, uint32_t q_seed,
+                             uint32_t s_seed, uint32_t pqs, uint32_t pqe, uint32_t pss, uint32_t pse, bool minus,
+                             uint32_t& oq, uint32_t& os) {
+    const int32_t RUN = 10;
+    const int32_t hmax = 15;  // (int)(10 * 1.5)
+    oq = q_seed;
+    os = s_seed;
+    if (!minus) {
+        int32_t score = -1;
+        uint32_t qf = q_seed, sf = s_seed;
+        while (qf < pqe && qf < qlen && sf < slen && query[qf] == subject[sf]) {
+            if (++score > RUN) return;
+            ++qf;
+            ++sf;
+        }
+        uint32_t qb = q_seed, sb = s_seed;
+        for (;;) {
+            if (query[qb] != subject[sb]) break;
+            if (++score > RUN) return;
+            if (qb == 0 || sb == 0) break;
+            --qb;
+            --sb;
+        }
+        const uint32_t offset = min(satsub(q_seed, pqs), satsub(s_seed, pss));
+        const uint32_t sqs = q_seed - offset, sss = s_seed - offset;
+        const uint32_t qn = min(satsub(pse, sss), satsub(pqe, sqs));
+        int32_t max_score = 0, sc = 0;
+        uint32_t max_off = sqs;
+        bool is_match = false, prev = false;
+        for (uint32_t i = 0; i < qn; ++i) {
+            const uint32_t qi = sqs + i, si = sss + i;
+            if (qi >= qlen || si >= slen) break;
+            is_match = query[qi] == subject[si];
+            if (is_match != prev) {
+                prev = is_match;
+                if (is_match) sc = 1;
+                else if (sc > max_score) { max_score = sc; max_off = qi - (uint32_t)(sc / 2); }
+            } else if (is_match) {
+                if (++sc > hmax) {
+                    const uint32_t nq = qi - (uint32_t)(hmax / 2);
+                    oq = nq;
+                    os = sss + (nq - sqs);
+                    return;
+                }
+            }
+        }
+        if (is_match && sc > max_score) {
+            max_score = sc;
+            max_off = sqs + qn - (uint32_t)(sc / 2);
+        }
+        if (max_score > 0) {
+            oq = max_off;
+            os = sss + (max_off - sqs);
+        }
+        return;
+    }
+    int32_t score = -1;
+    uint32_t qf = q_seed, sf = s_seed;
+    while (qf < qlen && sf < slen && query[qf] == subject[sf]) {
+        if (++score > RUN) return;
+        ++qf;
+        ++sf;
+    }
+    uint32_t qb = q_seed, sb = s_seed;
+    for (;;) {
+        if (query[qb] != subject[sb]) break;
+        if (++score > RUN) return;
+        if (qb <= pqs || sb == 0) break;
+        --qb;
+        --sb;
+    }
+    const uint32_t offset = min(satsub(satsub(pqe, 1), q_seed), satsub(satsub(pse, 1), s_seed));
+    const uint32_t top_q = q_seed + offset, top_s = s_seed + offset;
+    const uint32_t qn = min(satsub(top_q, pqs) + 1, satsub(top_s, pss) + 1);
+    int32_t max_score = 0, sc = 0;
+    int64_t max_off = q_seed;
+    bool is_match = false, prev = false;
+    for (uint32_t i = 0; i < qn; ++i) {
+        const uint32_t qi = top_q - i, si = top_s - i;
+        if (qi >= qlen || si >= slen) continue;
+        is_match = query[qi] == subject[si];
+        if (is_match != prev) {
+            prev = is_match;
+            if (is_match) sc = 1;
+            else if (sc > max_score) { max_score = sc; max_off = (int64_t)qi + sc / 2; }
+        } else if (is_match) {
+            if (++sc > hmax) {
+                const uint32_t nq = qi + (uint32_t)(hmax / 2);
+                oq = nq;
+                os = top_s - (top_q - nq);
+                return;
+            }
+        }
+    }
+    if (is_match && sc > max_score) {
+        max_score = sc;
+        max_off = (int64_t)top_q - (int64_t)qn + sc / 2;
+    }
+    if (max_score > 0) {
+        if (max_off < 0) return;
+        const int64_t delta = (int64_t)top_q - max_off;
+        int64_t ns = (int64_t)top_s - delta;
+        if (ns < 0) ns = 0;
+        oq = (uint32_t)max_off;
+        os = (uint32_t)ns;
+    }
+}
+
+// Per-thread traceback scratch: the band (absolute indices), the row table and the trace
+// bytes.  Any write past a capacity sets `overflow` and the DP stops.
+struct TbScratch {
+    int2* band;
+    uint2* rows;     // (byte offset of the row, first_b of the row)
+    uint32_t rows_cap;
+    uint8_t* trace;
+    uint64_t trace_cap;
+};
+
+// search/gapped.rs:450-689 align_ex (a = query outer, b = subject inner) and 692-757
+// traceback_flat.  Writes the script in reverse order (last op first) into ops_rev.
+// Returns 0 ok, 2 overflow (need = trace bytes wanted).
+template <bool REVERSE>
+__device__ int align_ex_tb(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint32_t m, uint32_t n,
+                           int32_t go, int32_t ge, int32_t x_dropoff, const int32_t* __restrict__ mat, TbScratch& S,
+                           int32_t& score_out, uint32_t& a_len, uint32_t& b_len, uint32_t* ops_rev, uint32_t ops_cap,
+                           uint32_t& n_ops, uint64_t& cells, uint64_t& need) {
+    score_out = 0;
+    a_len = b_len = 0;
+    n_ops = 0;
+    if (m == 0 || n == 0) return 0;
+    const int32_t goe = go + ge;
+    const int32_t xdrop = x_dropoff > goe ? x_dropoff : goe;
+    uint64_t flen = 0;
+    uint32_t nrows = 0;
+#define TB_PUT(v)                                   \
+    do {                                            \
+        if (flen >= S.trace_cap) { need = flen * 2 + 4096; return 2; } \
+        S.trace[flen++] = (v);                      \
+    } while (0)
+    S.band[0] = make_int2(0, -goe);
+    if (nrows >= S.rows_cap) { need = 0; return 2; }
+    S.rows[nrows++] = make_uint2(0, 0);
+    TB_PUT(T_GAP_B);
+    int32_t score = -goe;
+    uint32_t b_size = 1;
+    for (uint32_t j = 1; j <= n; ++j) {
+        if (score < -xdrop) break;
+        S.band[j] = make_int2(score, score - goe);
+        TB_PUT(T_GAP_A);
+        score -= ge;
+        b_size = j + 1;
+    }
+    int32_t best = 0;
+    uint32_t best_a = 0, best_b = 0, first_b = 0;
+    for (uint32_t ai = 0; ai < m; ++ai) {
+        const uint32_t ap = REVERSE ? m - 1 - ai : ai;
+        const int32_t* row = mat + ((a[ap] & 15) << 4);
+        if (nrows >= S.rows_cap) { need = 0; return 2; }
+        S.rows[nrows++] = make_uint2((uint32_t)flen, first_b);
+        int32_t sc = MININT, gap_row = MININT;
+        uint32_t last_b = first_b;
+        cells += b_size - first_b;
+        for (uint32_t bi = first_b; bi < b_size; ++bi) {
+            uint32_t bb = 0;
+            if (bi < n) bb = b[REVERSE ? n - 1 - bi : bi] & 15;
+            int2 c = S.band[bi];
+            const int32_t next_score = c.x + row[bb];
+            uint8_t op = T_SUB;
+            int32_t cell = sc;
+            if (c.y > cell) { cell = c.y; op = T_GAP_B; }
+            if (gap_row > cell) { cell = gap_row; op = T_GAP_A; }
+            if (best - cell > xdrop) {
+                if (bi == first_b) ++first_b;
+                else S.band[bi].x = MININT;
+            } else {
+                last_b = bi;
+                if (cell > best) { best = cell; best_a = ai + 1; best_b = bi; }
+                gap_row -= ge;
+                const int32_t gcol = c.y - ge;
+                const int32_t open = cell - goe;
+                int32_t bg;
+                if (gcol < open) bg = open;
+                else { bg = gcol; op |= T_EXT_B; }
+                S.band[bi] = make_int2(cell, bg);
+                if (gap_row < open) gap_row = open;
+                else op |= T_EXT_A;
+            }
+            sc = next_score;
+            TB_PUT(op);
+        }
+        if (first_b >= b_size) break;
+        if (last_b + 1 < b_size) {
+            b_size = last_b + 1;
+        } else {
+            while (gap_row >= best - xdrop && b_size <= n) {
+                S.band[b_size] = make_int2(gap_row, gap_row - goe);
+                gap_row -= ge;
+                TB_PUT(T_GAP_A);
+                ++b_size;
+            }
+        }
+        if (b_size <= n) {
+            S.band[b_size] = make_int2(MININT, MININT);
+            ++b_size;
+        }
+    }
+#undef TB_PUT
+    score_out = best;
+    a_len = best_a;
+    b_len = best_b;
+    // traceback_flat: walk from (best_a, best_b) to (0, 0)
+    if (best_a == 0 && best_b == 0) return 0;
+    uint32_t aa = best_a, bq = best_b;
+    uint8_t prev = T_SUB;
+    uint32_t cur_op = 0xffffffffu, cur_n = 0;
+    const uint64_t steps = (uint64_t)best_a + best_b;
+    for (uint64_t st = 0; st < steps; ++st) {
+        const uint2 ri = S.rows[aa];
+        const uint64_t row_end = aa + 1 < nrows ? S.rows[aa + 1].x : flen;
+        uint8_t raw = T_GAP_A;
+        if (bq >= ri.y) {
+            const uint64_t k = (uint64_t)ri.x + (bq - ri.y);
+            raw = k < row_end ? S.trace[k] : T_GAP_A;
+        }
+        uint8_t op;
+        if ((prev & T_MASK) == T_GAP_A) op = (raw & T_EXT_A) ? T_GAP_A : (raw & T_MASK);
+        else if ((prev & T_MASK) == T_GAP_B) op = (raw & T_EXT_B) ? T_GAP_B : (raw & T_MASK);
+        else op = raw & T_MASK;
+        prev = op;
+        uint32_t eop;
+        if (op == T_GAP_A) { eop = 1; bq = bq ? bq - 1 : 0; }
+        else if (op == T_GAP_B) { eop = 2; aa = aa ? aa - 1 : 0; }
+        else { eop = 0; aa = aa ? aa - 1 : 0; bq = bq ? bq - 1 : 0; }
+        if (eop == cur_op) ++cur_n;
+        else {
+            if (cur_n) {
+                if (n_ops >= ops_cap) { need = 0; return 2; }
+                ops_rev[n_ops++] = (cur_op << 30) | cur_n;
+            }
+            cur_op = eop;
+            cur_n = 1;
+        }
+        if (aa == 0 && bq == 0) break;
+    }
+    if (cur_n) {
+        if (n_ops >= ops_cap) { need = 0; return 2; }
+        ops_rev[n_ops++] = (cur_op << 30) | cur_n;
+    }
+    if (aa != 0 || bq != 0) return 3;  // the walk did not reach the origin
+    return 0;
+}
+
+__global__ void __launch_bounds__(128) k_traceback(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                    uint32_t n, const TbIn* __restrict__ in, TbOut* __restrict__ out,
+                                                    uint32_t* __restrict__ ops_out, uint32_t ops_cap,
+                                                    uint8_t* __restrict__ scratch, uint64_t scratch_per_thread,
+                                                    uint64_t band_cells, uint32_t rows_cap,
+                                                    unsigned long long* __restrict__ cells_total) {
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint8_t* base = scratch + tid * scratch_per_thread;
+    TbScratch S;
+    S.band = (int2*)base;
+    S.rows = (uint2*)(base + band_cells * sizeof(int2));
+    S.rows_cap = rows_cap;
+    S.trace = base + band_cells * sizeof(int2) + (uint64_t)rows_cap * sizeof(uint2);
+    S.trace_cap = scratch_per_thread - band_cells * sizeof(int2) - (uint64_t)rows_cap * sizeof(uint2);
+    uint64_t cells = 0;
+    for (uint64_t t = tid; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const TbIn h = in[t];
+        const uint32_t qi = h.pair / L.n, si = h.pair % L.n;
+        const uint32_t qa = Q.len[qi], sa = L.len[si];
+        const bool plus = h.strand == 0;
+        const uint8_t* qfwd = Q.q + Q.off[qi] + 1;
+        const uint8_t* sfs = (plus ? L.align : L.align_rc) + L.plus_off[si] + 1;
+        uint32_t nq, ns;
+        improve_seed(qfwd, qa, sfs, sa, h.q_seed, h.s_seed, h.q_start, h.q_end, h.s_start, h.s_end, !plus, nq, ns);
+        const uint32_t tq = plus ? nq : qa - 1 - nq, ts = plus ? ns : sa - 1 - ns;
+        const uint8_t* qa_ = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
+        const uint8_t* sa_ = L.align + L.plus_off[si] + 1;
+        uint32_t* ops = ops_out + t * (uint64_t)ops_cap;
+        TbOut o{0, 0, 0, 0, 0, 0, 0, 0};
+        uint64_t need = 0;
+        int32_t ls, rs = 0;
+        uint32_t la, lb, ra = 0, rb = 0, nl = 0, nr = 0;
+        int st = align_ex_tb<true>(qa_, sa_, tq + 1, ts + 1, P->gap_open, P->gap_extend, P->xdrop_gap_final, mat, S, ls, la,
+                                   lb, ops, ops_cap, nl, cells, need);
+        // left script is written last-op-first of the reversed DP, i.e. already in forward order
+        if (st == 0) {
+            const uint32_t rq = tq + 1, rsd = ts + 1;
+            const uint32_t rm = qa > rq ? qa - rq : 0, rn = sa > rsd ? sa - rsd : 0;
+            if (rm > 0 && rn > 0)
+                st = align_ex_tb<false>(qa_ + rq, sa_ + rsd, rm, rn, P->gap_open, P->gap_extend, P->xdrop_gap_final,
+                                        mat, S, rs, ra, rb, ops + nl, ops_cap - nl, nr, cells, need);
+        }
+        if (st != 0) {
+            o.status = st == 3 ? 3 : 2;
+            o.need = (uint32_t)min(need, (uint64_t)0xffffffffu);
+            out[t] = o;
+            continue;
+        }
+        // right script: reverse it in place to forward order, then merge at the junction
+        for (uint32_t i = 0, j = nr ? nr - 1 : 0; i < j; ++i, --j) {
+            uint32_t tmp = ops[nl + i];
+            ops[nl + i] = ops[nl + j];
+            ops[nl + j] = tmp;
+        }
+        uint32_t nops = nl;
+        for (uint32_t i = 0; i < nr; ++i) {
+            const uint32_t v = ops[nl + i];
+            if (nops > 0 && (ops[nops - 1] >> 30) == (v >> 30)) ops[nops - 1] += v & 0x3fffffffu;
+            else ops[nops++] = v;
+        }
+        int32_t total = ls + rs;
+        uint32_t q_start = tq + 1 - la, s_start = ts + 1 - lb;
+        uint32_t q_end = tq + 1 + ra, s_end = ts + 1 + rb;
+        uint32_t first = 0;
+        while (first < nops && (ops[first] >> 30) != 0) {
+            const uint32_t op = ops[first] >> 30, cnt = ops[first] & 0x3fffffffu;
+            total += P->gap_open + (int32_t)cnt * P->gap_extend;
+            if (op == 1) s_start += cnt;
+            else q_start += cnt;
+            ++first;
+        }
+        while (nops > first && (ops[nops - 1] >> 30) != 0) {
+            const uint32_t op = ops[nops - 1] >> 30, cnt = ops[nops - 1] & 0x3fffffffu;
+            total += P->gap_open + (int32_t)cnt * P->gap_extend;
+            if (op == 1) s_end -= cnt;
+            else q_end -= cnt;
+            --nops;
+        }
+        if (first) {
+            for (uint32_t i = first; i < nops; ++i) ops[i - first] = ops[i];
+            nops -= first;
+        }
+        if (total < 0) {
+            o.status = 1;
+            out[t] = o;
+            continue;
+        }
+        o.status = 0;
+        o.score = total;
+        o.q0 = q_start;
+        o.q1 = q_end;
+        o.s0 = s_start;
+        o.s1 = s_end;
+        o.n_ops = nops;
+        out[t] = o;
+    }
+    for (int o2 = 16; o2; o2 >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o2);
+    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// ---------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------
+static int grid_for(uint64_t work, int block, int per_sm_blocks, int sms) {
+    uint64_t g = (work + block - 1) / block;
+    uint64_t cap = (uint64_t)sms * per_sm_blocks;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+cudaError_t launch_scan(bool write, const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
+                        uint32_t* counts, const uint64_t* offs, SeedHit* hits, uint32_t* hit_pair, int sms,
+                        cudaStream_t st) {
+    const int block = 256;
+    const int grid = grid_for(n_pairs * 32, block, 8, sms);
+    if (write) k_scan<true><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair);
+    else k_scan<false><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut, uint64_t n,
+                            const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    const int block = 256;
+    k_ungapped<<<grid_for(n, block, 8, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out);
+    return cudaGetLastError();
+}
+
+uint64_t dedup_threads(int sms) { return (uint64_t)sms * 8 * 128; }
+
+cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32_t ucut, uint64_t pair0,
+                         uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits, const UngBox* ub, uint8_t* flags,
+                         uint32_t* scratch, void* cells, int sms, cudaStream_t st) {
+    const int block = 128;
+    const uint64_t want = (n_pairs + block - 1) / block;
+    const uint64_t cap = dedup_threads(sms) / block;
+    const int grid = (int)(want < cap ? (want ? want : 1) : cap);
+    k_dedup<<<grid, block, 0, st>>>(L, Q, ws, ucut, pair0, n_pairs, offs, hits, ub, flags, scratch, (DiagCell*)cells);
+    return cudaGetLastError();
+}
+
+size_t diag_cell_bytes() { return sizeof(DiagCell); }
+
+constexpr int PRELIM_W = 64;
+
+cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n, const uint32_t* idx,
+                          const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub, PrelimOut* out,
+                          uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    const int block = 128;
+    const size_t smem = (size_t)block * PRELIM_W * sizeof(int2);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_prelim<PRELIM_W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_prelim<PRELIM_W><<<grid_for(n, block, 3, sms), block, smem, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide,
+                                                                      n_wide, cells);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_wide,
+                               const uint32_t* wide, const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair,
+                               const UngBox* ub, PrelimOut* out, int2* band_mem, uint64_t band_cap, uint32_t threads,
+                               unsigned long long* cells, unsigned int* failures, cudaStream_t st) {
+    if (!n_wide) return cudaSuccess;
+    const int block = 128;
+    const int grid = (int)((threads + block - 1) / block);
+    k_prelim_wide<<<grid, block, 0, st>>>(L, Q, P, n_wide, wide, idx, hits, hit_pair, ub, out, band_mem, band_cap, cells,
+                                          failures);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n, const TbIn* in,
+                             TbOut* out, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch, uint64_t per_thread,
+                             uint64_t band_cells, uint32_t rows_cap, uint32_t threads, unsigned long long* cells,
+                             cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    const int block = 128;
+    const int grid = (int)((threads + block - 1) / block);
+    k_traceback<<<grid, block, 0, st>>>(L, Q, P, n, in, out, ops, ops_cap, scratch, per_thread, band_cells, rows_cap,
+                                        cells);
+    return cudaGetLastError();
+}
+
+}  // namespace rmb
+
+// ---------------------------------------------------------------------------------------
+// compaction helpers (CUB device-wide scan / select)
+// ---------------------------------------------------------------------------------------
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+namespace rmb {
+
+__global__ void k_gather_survivors(uint32_t n, const uint32_t* __restrict__ sel, const uint32_t* __restrict__ idx,
+                                   const SeedHit* __restrict__ hits, const uint32_t* __restrict__ hit_pair,
+                                   const UngBox* __restrict__ ub, const PrelimOut* __restrict__ po,
+                                   SurvivorRec* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t t = sel[k];
+    const uint32_t i = idx[t];
+    out[k] = SurvivorRec{hit_pair[i], hits[i], ub[i], po[t]};
+}
+
+cudaError_t launch_gather_survivors(uint32_t n, const uint32_t* sel, const uint32_t* idx, const SeedHit* hits,
+                                    const uint32_t* hit_pair, const UngBox* ub, const PrelimOut* po,
+                                    SurvivorRec* out, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    k_gather_survivors<<<(n + 255) / 256, 256, 0, st>>>(n, sel, idx, hits, hit_pair, ub, po, out);
+    return cudaGetLastError();
+}
+
+struct FlagEq {
+    const uint8_t* f;
+    uint8_t want;
+    __host__ __device__ bool operator()(const uint32_t& i) const { return f[i] == want; }
+};
+struct PrelimPass {
+    const PrelimOut* p;
+    __host__ __device__ bool operator()(const uint32_t& i) const { return p[i].score != INT32_MIN; }
+};
+
+cudaError_t launch_select_eq(const uint8_t* flags, uint64_t n, uint8_t want, uint32_t* out, uint32_t* n_out,
+                             void* temp, size_t& temp_bytes, cudaStream_t st) {
+    thrust::counting_iterator<uint32_t> it(0);
+    return cub::DeviceSelect::If(temp, temp_bytes, it, out, n_out, (int64_t)n, FlagEq{flags, want}, st);
+}
+
+cudaError_t launch_select_prelim(const PrelimOut* po, uint64_t n, uint32_t* out, uint32_t* n_out, void* temp,
+                                 size_t& temp_bytes, cudaStream_t st) {
+    thrust::counting_iterator<uint32_t> it(0);
+    return cub::DeviceSelect::If(temp, temp_bytes, it, out, n_out, (int64_t)n, PrelimPass{po}, st);
+}
+
+cudaError_t launch_offsets(const uint32_t* counts, uint64_t n, uint64_t* offs, void* temp, size_t& temp_bytes,
+                           cudaStream_t st) {
+    return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offs, (int64_t)n, st);
+}
+
+}  // namespace rmb

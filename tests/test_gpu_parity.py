@@ -1,0 +1,148 @@
+"""Parity of the CUDA search core with the oracle and the reference's NCBI goldens.
+
+Every comparison is exact (byte-identical outfmt-6 text, identical stage records): the path is
+integer arithmetic plus the reference's own f64/f32 formulas on the host, so there is no
+tolerance.  Inputs are the reference's fixtures and seeded synthetic genome/library workloads.
+"""
+import numpy as np
+import pytest
+
+import oracle_ref as O
+from rmblast_b200 import api, build, synth
+
+pytestmark = pytest.mark.gpu
+G = O.GOLDEN
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+
+
+def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str):
+    m = api.ScoreMatrix.from_text(matrix_text, matrix_name)
+    sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
+                          xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
+                          min_raw_gapped_score=p["min_raw_gapped_score"],
+                          complexity_adjust=bool(p.get("complexity_adjust", 0)), dust=False,
+                          mask_level=p.get("mask_level", -1))
+    return api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
+
+
+def gpu_text(p, matrix_text, matrix_name, db_fasta, query_fasta, outfmt):
+    s = searcher(p, matrix_text, matrix_name, db_fasta)
+    recs = api.read_fasta(query_fasta)
+    res = s.search([api.encode(seq) for _, seq in recs], [n for n, _ in recs])
+    return res.tabular(outfmt), res
+
+
+def test_golden_nomask_nodust_through_c_abi():
+    p = dict(O.RM_PARAMS, mask_level=101)
+    txt, _ = gpu_text(p, (G / "comparison.matrix").read_text(), "comparison.matrix", (G / "db.fa").read_text(),
+                      (G / "query.fa").read_text(), O.RM_FIELDS)
+    assert txt == (G / "expected_nomask_nodust.ncbi-2.17.1.tsv").read_text()
+
+
+def test_golden_db_dash_subjects_nomask():
+    # '-' in subjects is N: CRandom-resolved for the scan, restored for the traceback
+    p = dict(O.RM_PARAMS, mask_level=101)
+    mt = (G / "comparison.matrix").read_text()
+    db = (G / "db_dash.fa").read_text()
+    q = (G / "query.fa").read_text()
+    txt, _ = gpu_text(p, mt, "comparison.matrix", db, q, O.RM_FIELDS)
+    want, _, _ = O.search_text(q, db, mt, "comparison.matrix", p, O.RM_FIELDS)
+    assert txt == want
+
+
+def test_identity_matrix_default_cutoff_matches_oracle():
+    p = dict(gap_open=20, gap_extend=5, word_size=14, xdrop_ungap=20, xdrop_gap=30, xdrop_gap_final=100,
+             min_raw_gapped_score=0)
+    mt = (G / "identity.matrix").read_text()
+    db, q = (G / "db.fa").read_text(), (G / "query.fa").read_text()
+    txt, _ = gpu_text(p, mt, "identity.matrix", db, q, "6 score qstart qend sstart send sseqid perc_sub")
+    want, _, _ = O.search_text(q, db, mt, "identity.matrix", p, "6 score qstart qend sstart send sseqid perc_sub")
+    assert txt.count("\n") > 300
+    assert txt == want
+
+
+def synthetic(name, scale, flags):
+    qs, db, prm = synth.workload(name, scale=scale)
+    p = dict(prm)
+    p.update(flags)
+    qf = synth.to_fasta([n for n, _ in qs], [s for _, s in qs])
+    dbf = synth.to_fasta([n for n, _ in db], [s for _, s in db])
+    return qf, dbf, p
+
+
+FIELDS = "6 score perc_sub perc_query_gap perc_db_gap qseqid qstart qend sseqid sstart send kdiv cpg_kdiv qseq sseq"
+
+
+@pytest.mark.parametrize("flags", ["rm", "default"])
+def test_synthetic_small_matches_oracle(flags):
+    qf, dbf, p = synthetic("small", 0.25, synth.RM_FLAGS if flags == "rm" else synth.DEFAULT_FLAGS)
+    txt, res = gpu_text(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, qf, FIELDS)
+    want, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert txt.count("\n") > 10
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"]
+    assert res.counters["so_cells"] == ctr["so_cells"]
+
+
+def test_synthetic_plain_matches_oracle():
+    qf, dbf, p = synthetic("plain", 0.003, synth.RM_FLAGS)
+    txt, res = gpu_text(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, qf, FIELDS)
+    want, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert txt.count("\n") > 20
+    assert txt == want
+    for k in ("word_hits", "ungapped", "prelim_dp", "so_cells"):
+        if k == "word_hits":
+            continue  # the oracle counts scanner hits before the exact extension, the GPU after it
+        assert res.counters[k] == ctr[k], k
+
+
+@pytest.mark.parametrize("ws", [4, 5, 6, 7, 8, 9, 10, 11, 12, 14, 16, 24])
+def test_word_sizes_stage_taps_and_output(ws):
+    qf, dbf, p = synthetic("small", 0.04, synth.RM_FLAGS)
+    p["word_size"] = ws
+    s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf)
+    recs = api.read_fasta(qf)
+    qs = [api.encode(seq) for _, seq in recs]
+    for stage in (0, 1):
+        got = s.stage(qs, stage)
+        want = O.stage_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, stage)
+        assert got.shape == want.shape, (stage, got.shape, want.shape)
+        assert np.array_equal(got, want), stage
+    got = s.stage(qs, 2)
+    want = O.stage_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, 2)
+    assert sorted(map(tuple, got.tolist())) == sorted(map(tuple, want.tolist()))
+    res = s.search(qs, [n for n, _ in recs])
+    want_txt, _, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert res.tabular(FIELDS) == want_txt
+
+
+def test_golden_stage_taps_match_oracle():
+    p = dict(O.RM_PARAMS, mask_level=101)
+    mt, db, q = (G / "comparison.matrix").read_text(), (G / "db.fa").read_text(), (G / "query.fa").read_text()
+    s = searcher(p, mt, "comparison.matrix", db)
+    qs = [api.encode(seq) for _, seq in api.read_fasta(q)]
+    for stage in (0, 1):
+        assert np.array_equal(s.stage(qs, stage), O.stage_text(q, db, mt, "comparison.matrix", p, stage))
+
+
+def test_edge_cases():
+    p = dict(O.RM_PARAMS, mask_level=101)
+    mt, db = (G / "comparison.matrix").read_text(), (G / "db.fa").read_text()
+    s = searcher(p, mt, "comparison.matrix", db)
+    # shorter than the word size, exactly the word size, all N, empty batch
+    qs = [api.encode(b"ACGT"), api.encode(b"A" * 14), api.encode(b"N" * 5000)]
+    res = s.search(qs)
+    assert res.n_hsps == 0
+    assert s.search([]).n_hsps == 0
+    # the chunked path is refused, not silently truncated
+    with pytest.raises(api.RmbError) as e:
+        s.search([api.encode(b"A" * 1_999_800)])
+    assert e.value.code == 5
+    # dust needs the query masker, which this library refuses rather than skipping
+    m = api.ScoreMatrix.from_text(mt, "comparison.matrix")
+    with pytest.raises(api.RmbError):
+        api.Searcher(api.SearchParams(dust=True), m, api.SubjectDb.from_fasta(db))

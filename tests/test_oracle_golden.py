@@ -1,0 +1,70 @@
+"""Pins the CPU oracle to the reference's NCBI-2.17.1 golden outputs.
+
+The CLI goldens are the reference's rmblastn/tests/data fixtures (copied into tests/golden by
+tests/golden/make_fixtures.py) with the command lines of rmblastn/tests/cli.rs:11-35, 144-290.
+The chr22 stage goldens (rmblast-lib/tests/*_regression.rs, 247,629 records each) are read from
+the reference tree when it is present.
+"""
+from pathlib import Path
+
+import pytest
+
+import oracle_ref as O
+
+G = O.GOLDEN
+RM = ["--gapopen", "20", "--gapextend", "5", "--word-size", "14", "--xdrop-ungap", "400",
+      "--xdrop-gap-final", "200", "--xdrop-gap", "100", "--min-raw-gapped-score", "200", "--outfmt", O.RM_FIELDS]
+REF = Path("/root/reference")
+
+
+def _run(db, q, m, extra):
+    return O.run_cli(["--db", str(G / db), "--query", str(G / q), "--matrix", str(G / m), *extra])
+
+
+CASES = [
+    ("nomask_nodust", "db.fa", "query.fa", "comparison.matrix", RM + ["--mask-level", "101", "--dust", "no", "--num-threads", "4"]),
+    ("rm_defaults", "db.fa", "query.fa", "comparison.matrix", RM + ["--mask-level", "80", "--complexity-adjust", "--dust", "yes"]),
+    ("query_dash", "db.fa", "query_dash.fa", "comparison.matrix", RM + ["--mask-level", "80", "--complexity-adjust", "--dust", "yes"]),
+    ("db_dash", "db_dash.fa", "query.fa", "comparison.matrix", RM + ["--mask-level", "80", "--complexity-adjust", "--dust", "yes"]),
+    ("asym_freqs", "db.fa", "query.fa", "asym_freqs.matrix", RM + ["--mask-level", "101", "--complexity-adjust", "--dust", "yes"]),
+    ("defaults", "db.fa", "query.fa", "comparison.matrix", ["--gapopen", "20", "--gapextend", "5", "--outfmt", O.RM_FIELDS]),
+]
+
+
+@pytest.mark.parametrize("name,db,q,m,extra", CASES, ids=[c[0] for c in CASES])
+def test_oracle_matches_ncbi_golden(name, db, q, m, extra):
+    got = _run(db, q, m, extra)
+    want = (G / f"expected_{name}.ncbi-2.17.1.tsv").read_text()
+    assert got == want
+
+
+def test_identity_matrix_has_no_score_zero_hits():
+    # rmblastn/tests/cli.rs:210-226
+    out = _run("db.fa", "query.fa", "identity.matrix",
+               ["--gapopen", "20", "--gapextend", "5", "--word-size", "14", "--dust", "no", "--outfmt", "6 score qstart qend"])
+    lines = out.splitlines()
+    assert len(lines) > 300
+    for ln in lines:
+        s, a, b = map(int, ln.split("\t"))
+        assert s >= 1 and b >= a
+
+
+@pytest.mark.skipif(not (REF / "tests/data/chr22.fa").exists(), reason="reference tree not mounted")
+@pytest.mark.parametrize("stage,gold", [(0, "chr22_dedup_seeds.txt"), (1, "chr22_ungapped_hits.txt")])
+def test_oracle_matches_chr22_stage_goldens(stage, gold):
+    import ctypes as C
+    lib = O.lib()
+    lib.rmbo_stage_file.argtypes = [C.c_char_p] * 3 + [C.POINTER(O.OParams), C.c_int, C.POINTER(C.c_void_p),
+                                                       C.c_char_p, C.c_size_t]
+    p = O.oparams(dict(O.RM_PARAMS, complexity_adjust=1, dust=0, mask_level=80))
+    out = C.c_void_p()
+    err = C.create_string_buffer(512)
+    rc = lib.rmbo_stage_file(str(REF / "tests/data/chr22.fa").encode(), str(REF / "tests/data/alu.2bit").encode(),
+                             str(REF / "rmblast-lib/tests/data/comparison.matrix").encode(), C.byref(p), stage,
+                             C.byref(out), err, 512)
+    assert rc == 0, err.value
+    got = C.string_at(out.value).decode()
+    lib.rmbo_free(out)
+    want = (REF / "rmblast-lib/tests/data" / gold).read_text()
+    assert got.count("\n") == 247629
+    assert got == want
