@@ -82,6 +82,10 @@ typedef struct rmb_counters {
     uint64_t word_hits, seeds, ungapped, prelim_dp, prelims, tb_dp, finals;
     uint64_t so_cells, tb_cells;
     double ms_lookup, ms_scan, ms_ungapped, ms_dedup, ms_prelim_dp, ms_host_2a, ms_traceback, ms_host_2b;
+    /* device time of the kernels (CUDA events on the library's stream) and the number of
+     * this library's own kernel launches (CUB scans/sorts/selects not counted) */
+    double gpu_ms_scan, gpu_ms_ungapped, gpu_ms_dedup, gpu_ms_prelim, gpu_ms_traceback, gpu_ms_lookup;
+    uint64_t launches;
 } rmb_counters;
 
 /* Results of rmb_search_batch, in the reference's output order per query
@@ -103,6 +107,16 @@ typedef struct rmb_results {
  * with RMB_ELIMIT. */
 int rmb_search_batch(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
                      rmb_results** out, char* err, size_t errlen);
+
+/* The same search split at the host/device boundary: rmb_queries_upload copies the queries
+ * into device memory once (the reference's per-query BLASTNA buffers, main.rs:740-746), and
+ * rmb_search_resident runs search_db_parallel on them; rmb_search_batch is upload + search +
+ * free.  A query set belongs to the device of the context that uploaded it. */
+typedef struct rmb_queries rmb_queries;
+int rmb_queries_upload(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
+                       rmb_queries** out, char* err, size_t errlen);
+int rmb_search_resident(rmb_ctx* ctx, rmb_queries* queries, rmb_results** out, char* err, size_t errlen);
+void rmb_queries_free(rmb_queries* queries);
 
 /* output.rs:223-367 parse_outfmt + write_tabular: "6 <fields>" lines for every HSP, query by
  * query; query_ids[i] names query i.  *text is NUL-terminated; free with rmb_text_free. */
@@ -134,6 +148,10 @@ void rmb_resolve_subject(const uint8_t* raw, uint32_t n, uint8_t* plus, uint8_t*
 void rmb_results_free(rmb_results* res);
 void rmb_text_free(void* p);
 void rmb_ctx_destroy(rmb_ctx* ctx);
+
+/* Measurement helper: sustained int32 add/max throughput of the device in Tops/s (the
+ * roofline denominator for the integer DP kernels). */
+int rmb_probe_int32_peak(int32_t device, double* tops, char* err, size_t errlen);
 
 /* Library version string. */
 const char* rmb_version(void);

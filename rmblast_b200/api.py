@@ -48,7 +48,8 @@ class _Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "word_hits", "seeds", "ungapped", "prelim_dp", "prelims", "tb_dp", "finals", "so_cells", "tb_cells")] + [
         (n, C.c_double) for n in ("ms_lookup", "ms_scan", "ms_ungapped", "ms_dedup", "ms_prelim_dp", "ms_host_2a",
-                                  "ms_traceback", "ms_host_2b")]
+                                  "ms_traceback", "ms_host_2b", "gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
+                                  "gpu_ms_prelim", "gpu_ms_traceback", "gpu_ms_lookup")] + [("launches", C.c_uint64)]
 
 
 class _Results(C.Structure):
@@ -85,7 +86,22 @@ def load_library(path: Path = LIB_PATH) -> C.CDLL:
     lib.rmb_ctx_destroy.argtypes = [C.c_void_p]
     lib.rmb_ctx_destroy.restype = None
     lib.rmb_version.restype = C.c_char_p
+    lib.rmb_queries_upload.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32), C.POINTER(C.c_void_p),
+                                       C.c_char_p, C.c_size_t]
+    lib.rmb_search_resident.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.POINTER(_Results)), C.c_char_p,
+                                        C.c_size_t]
+    lib.rmb_queries_free.argtypes = [C.c_void_p]
+    lib.rmb_queries_free.restype = None
+    lib.rmb_probe_int32_peak.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_char_p, C.c_size_t]
     return lib
+
+
+def int32_peak_tops(device: int = 0) -> float:
+    """Sustained int32 add/max throughput of the device (Tops/s), measured by the library."""
+    v = C.c_double()
+    err = C.create_string_buffer(256)
+    _check(lib().rmb_probe_int32_peak(device, C.byref(v), err, 256), err)
+    return v.value
 
 
 _LIB: C.CDLL | None = None
@@ -246,6 +262,19 @@ class Results:
             self._p = None
 
 
+class ResidentQueries:
+    def __init__(self, h: C.c_void_p, n: int):
+        self._h, self.n = h, n
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().rmb_queries_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.free()
+
+
 class Searcher:
     """One search context on one GPU: parameters, matrix and the resident library."""
 
@@ -274,6 +303,20 @@ class Searcher:
         err = C.create_string_buffer(1024)
         _check(lib().rmb_search_batch(self._ctx, n, qp, ql, C.byref(res), err, 1024), err)
         return Results(self, res, query_ids or [f"query{i}" for i in range(n)])
+
+    def upload(self, queries: list[np.ndarray]) -> "ResidentQueries":
+        """rmb_queries_upload: the queries copied into device memory once."""
+        n, qp, ql = self._queries(queries)
+        h = C.c_void_p()
+        err = C.create_string_buffer(1024)
+        _check(lib().rmb_queries_upload(self._ctx, n, qp, ql, C.byref(h), err, 1024), err)
+        return ResidentQueries(h, n)
+
+    def search_resident(self, rq: "ResidentQueries", query_ids: list[str] | None = None) -> Results:
+        res = C.POINTER(_Results)()
+        err = C.create_string_buffer(1024)
+        _check(lib().rmb_search_resident(self._ctx, rq._h, C.byref(res), err, 1024), err)
+        return Results(self, res, query_ids or [f"query{i}" for i in range(rq.n)])
 
     def stage(self, queries: list[np.ndarray], stage: int) -> np.ndarray:
         n, qp, ql = self._queries(queries)

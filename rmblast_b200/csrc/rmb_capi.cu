@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <sstream>
@@ -93,6 +94,26 @@ void parallel_for(size_t n, const std::function<void(size_t)>& fn) {
     if (err) std::rethrow_exception(err);
 }
 
+struct EvTimer {  // device time between two events on one stream
+    cudaEvent_t a = nullptr, b = nullptr;
+    EvTimer() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~EvTimer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    void start(cudaStream_t st) { cudaEventRecord(a, st); }
+    void stop(cudaStream_t st) { cudaEventRecord(b, st); }
+    double ms() {
+        float m = 0;
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&m, a, b);
+        return m;
+    }
+};
+
 double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -118,65 +139,29 @@ struct rmb_ctx {
     // library, device
     DBuf d_plus, d_rc, d_align, d_align_rc, d_packed, d_plus_off, d_packed_off, d_len, d_params;
     // per-batch device buffers
-    DBuf q, qrc, qoff, qlen, pv, pv_off, cs, cs_off, cq, cq_off, lw;
+    DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, n_wide, band, sel,
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
     DevLib L{};
 };
 
-namespace {
-
-struct Lut {  // one query's table in the device layout (rmb_device.cuh DevQueries)
-    int lw = 0;
-    std::vector<uint32_t> pv, cell_start, cell_q;
+// Queries resident on the device (rmb_queries_upload); the host copy feeds the host steps.
+struct rmb_queries {
+    uint32_t n = 0;
+    int device = 0;
+    std::vector<uint8_t> host;     // concatenated sentinel-wrapped queries
+    std::vector<uint64_t> off;     // offset of query i in host / d_q / d_qrc
+    std::vector<uint32_t> len;
+    DBuf d_q, d_qrc, d_off, d_len;
+    void release() {
+        d_q.release();
+        d_qrc.release();
+        d_off.release();
+        d_len.release();
+    }
 };
 
-// blast/nalookup.rs:128-335 and blast/mblookup.rs:106-235, as one CSR: every lw-mer of the
-// two-context buffer [fwd | N | rc] whose lw bases are all A/C/G/T, per cell in the order the
-// reference's table hands them out (ascending for lw <= 8, descending for the megablast table).
-void build_lut(const uint8_t* q, uint32_t n, int ws, Lut& L) {
-    const uint64_t approx = 2ull * n;
-    L.lw = choose_lut_width(ws, approx);
-    if (L.lw < 0) throw Fail(RMB_EINVAL, "word_size below 4");
-    const int lw = L.lw;
-    const uint32_t cells = 1u << (2 * lw);
-    std::vector<uint8_t> comb(2ull * n + 1);
-    for (uint32_t i = 0; i < n; ++i) comb[i] = q[1 + i];
-    comb[n] = 14;
-    for (uint32_t i = 0; i < n; ++i) comb[n + 1 + i] = COMPL[q[n - i] & 15];
-    std::vector<uint32_t> code(comb.size(), 0xffffffffu);
-    const uint32_t mask = cells - 1;
-    const int64_t locs[2][2] = {{0, (int64_t)n - 1}, {(int64_t)n + 1, 2 * (int64_t)n}};
-    for (auto& loc : locs) {
-        const int64_t from = loc[0], to = loc[1];
-        if (ws > to - from + 1) continue;
-        uint32_t e = 0;
-        int64_t valid_from = from + lw - 1;
-        for (int64_t rp = from; rp <= to; ++rp) {
-            const uint8_t b = comb[rp];
-            if (b & 0xFC) { e = 0; valid_from = rp + lw; continue; }
-            e = ((e << 2) & mask) | b;
-            if (rp < valid_from) continue;
-            code[rp + 1 - lw] = e;
-        }
-    }
-    L.cell_start.assign((size_t)cells + 1, 0);
-    for (uint32_t c : code)
-        if (c != 0xffffffffu) L.cell_start[c + 1]++;
-    for (uint32_t c = 0; c < cells; ++c) L.cell_start[c + 1] += L.cell_start[c];
-    L.cell_q.assign(L.cell_start[cells], 0);
-    std::vector<uint32_t> fill(L.cell_start.begin(), L.cell_start.end() - 1);
-    if (lw <= 8) {
-        for (size_t s = 0; s < code.size(); ++s)
-            if (code[s] != 0xffffffffu) L.cell_q[fill[code[s]]++] = (uint32_t)s;
-    } else {
-        for (size_t s = code.size(); s-- > 0;)
-            if (code[s] != 0xffffffffu) L.cell_q[fill[code[s]]++] = (uint32_t)s;
-    }
-    L.pv.assign(std::max<uint32_t>(cells / 32, 1), 0);
-    for (uint32_t c = 0; c < cells; ++c)
-        if (L.cell_start[c + 1] > L.cell_start[c]) L.pv[c >> 5] |= 1u << (c & 31);
-}
+namespace {
 
 std::vector<uint8_t> revcomp_full(const uint8_t* s, size_t n) {
     std::vector<uint8_t> o(n);
@@ -190,121 +175,146 @@ struct Taps {
     std::vector<uint32_t>* prelims = nullptr;   // strand, qs, qe, ss, se, score, q_seed, s_seed
 };
 
-// One batch: returns per-query hits (reference order).
-void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen,
-                std::vector<std::vector<Hit>>& out_hits, rmb_counters& ctr, Taps* taps) {
+// One search over resident queries: per-query hits in the reference's order.
+void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hits, rmb_counters& ctr,
+                Taps* taps) {
     const rmb_params& P = C.p;
     const uint32_t ns = (uint32_t)C.ids.size();
+    const uint32_t nq = QH.n;
+    const uint32_t* qlen = QH.len.data();
     out_hits.assign(nq, {});
-    std::vector<int32_t> ucut(nq);
+    std::vector<int32_t> ucut(nq), lw_all(nq);
     for (uint32_t i = 0; i < nq; ++i) {
         if (qlen[i] >= 1999800u) throw Fail(RMB_ELIMIT, "queries of 1,999,800 bp or more take the chunked path");
         const uint64_t avg = ns ? C.total_letters / ns : 0;
         ucut[i] = P.ungapped_cutoff >= 0 ? P.ungapped_cutoff
                                           : ungapped_cutoff_for(C.matrix_name, P.gap_open, P.gap_extend,
                                                                 P.min_raw_gapped_score, qlen[i], avg);
+        lw_all[i] = choose_lut_width(P.word_size, 2ull * qlen[i]);
     }
-    // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table bytes.
+    cudaStream_t st = C.st;
+    upload(C.lw, lw_all, st);
+    // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table size.
     uint32_t qb = 0;
     while (qb < nq) {
-        uint64_t bytes = 0;
+        uint64_t cells_b = 0, pos_b = 0;
         uint32_t qe = qb;
-        while (qe < nq && (qe == qb || (ucut[qe] == ucut[qb] && bytes < (1ull << 30)))) {
-            const int lw = choose_lut_width(P.word_size, 2ull * qlen[qe]);
-            bytes += (4ull << (2 * std::max(lw, 4))) + 8ull * qlen[qe];
+        while (qe < nq) {
+            const uint64_t c = (1ull << (2 * lw_all[qe])) + 1, p2 = 2ull * qlen[qe] + 1;
+            if (qe > qb && (ucut[qe] != ucut[qb] || cells_b + c > (1ull << 30) || pos_b + p2 > (1ull << 30))) break;
+            cells_b += c;
+            pos_b += p2;
             ++qe;
         }
         const uint32_t nb = qe - qb;
         auto t0 = std::chrono::steady_clock::now();
-        // ---- queries and lookup tables
-        std::vector<Lut> luts(nb);
-        parallel_for(nb, [&](size_t i) { build_lut(query[qb + i], qlen[qb + i], P.word_size, luts[i]); });
-        std::vector<uint8_t> hq, hqrc;
-        std::vector<uint64_t> hqoff(nb), hpvoff(nb), hcsoff(nb), hcqoff(nb);
-        std::vector<uint32_t> hqlen(nb);
-        std::vector<int32_t> hlw(nb);
-        uint64_t npv = 0, ncs = 0, ncq = 0;
+        // ---- lookup tables of the sub-batch, built on the device
+        std::vector<uint64_t> hpvoff(nb), hcsoff(nb), hposoff(nb), hzero(nb, 0);
+        std::vector<uint32_t> hqlen(qlen + qb, qlen + qe);
+        std::vector<int32_t> hlw(lw_all.begin() + qb, lw_all.begin() + qe);
+        uint64_t npv = 0, ncs = 0, npos = 0;
         for (uint32_t i = 0; i < nb; ++i) {
-            hqoff[i] = hq.size();
-            hqlen[i] = qlen[qb + i];
-            const uint8_t* s = query[qb + i];
-            hq.insert(hq.end(), s, s + qlen[qb + i] + 2);
-            auto rc = revcomp_full(s, qlen[qb + i] + 2);
-            hqrc.insert(hqrc.end(), rc.begin(), rc.end());
             hpvoff[i] = npv;
             hcsoff[i] = ncs;
-            hcqoff[i] = ncq;
-            npv += luts[i].pv.size();
-            ncs += luts[i].cell_start.size();
-            ncq += luts[i].cell_q.size();
-            hlw[i] = luts[i].lw;
+            hposoff[i] = npos;
+            npv += std::max<uint64_t>((1ull << (2 * hlw[i])) / 32, 1);
+            ncs += (1ull << (2 * hlw[i])) + 1;
+            npos += 2ull * hqlen[i] + 1;
         }
-        std::vector<uint32_t> hpv(npv), hcs(ncs), hcq(std::max<uint64_t>(ncq, 1));
-        parallel_for(nb, [&](size_t i) {
-            std::copy(luts[i].pv.begin(), luts[i].pv.end(), hpv.begin() + hpvoff[i]);
-            std::copy(luts[i].cell_start.begin(), luts[i].cell_start.end(), hcs.begin() + hcsoff[i]);
-            std::copy(luts[i].cell_q.begin(), luts[i].cell_q.end(), hcq.begin() + hcqoff[i]);
-        });
-        luts.clear();
-        cudaStream_t st = C.st;
-        upload(C.q, hq, st);
-        upload(C.qrc, hqrc, st);
-        upload(C.qoff, hqoff, st);
-        upload(C.qlen, hqlen, st);
-        upload(C.pv, hpv, st);
         upload(C.pv_off, hpvoff, st);
-        upload(C.cs, hcs, st);
         upload(C.cs_off, hcsoff, st);
-        upload(C.cq, hcq, st);
-        upload(C.cq_off, hcqoff, st);
-        upload(C.lw, hlw, st);
-        DevQueries Q{C.q.as<uint8_t>(),      C.qrc.as<uint8_t>(),     C.q.as<uint8_t>(),  C.qoff.as<uint64_t>(),
-                     C.qlen.as<uint32_t>(),  C.pv.as<uint32_t>(),     C.pv_off.as<uint64_t>(),
-                     C.cs.as<uint32_t>(),    C.cs_off.as<uint64_t>(), C.cq.as<uint32_t>(),
-                     C.cq_off.as<uint64_t>(), C.lw.as<int32_t>(),     nb};
+        upload(C.cq_off, hzero, st);
+        upload(C.pos_off, hposoff, st);
+        C.pv.ensure(npv * 4);
+        C.cs.ensure((ncs + 1) * 4);
+        C.lut_counts.ensure((ncs + 1) * 4);
+        C.cq.ensure(npos * 4);
+        C.lut_keys.ensure(npos * 4);
+        C.lut_vals.ensure(npos * 4);
+        C.lut_keys2.ensure(npos * 4);
+        C.lut_vals2.ensure(npos * 4);
+        DevQueries Q{QH.d_q.as<uint8_t>(),       QH.d_qrc.as<uint8_t>(),  QH.d_q.as<uint8_t>(),
+                     QH.d_off.as<uint64_t>() + qb, QH.d_len.as<uint32_t>() + qb, C.pv.as<uint32_t>(),
+                     C.pv_off.as<uint64_t>(),    C.cs.as<uint32_t>(),     C.cs_off.as<uint64_t>(),
+                     C.cq.as<uint32_t>(),        C.cq_off.as<uint64_t>(), C.lw.as<int32_t>() + qb, nb};
+        EvTimer ev;
+        ev.start(st);
+        {
+            size_t tb = C.temp.cap;
+            uint64_t nvalid = 0;
+            cudaError_t e = launch_lut_build(Q, P.word_size, nb, C.pos_off.as<uint64_t>(), npos, ncs, npv,
+                                             C.lut_keys.as<uint32_t>(), C.lut_vals.as<uint32_t>(),
+                                             C.lut_keys2.as<uint32_t>(), C.lut_vals2.as<uint32_t>(),
+                                             C.lut_counts.as<uint32_t>(), C.cs.as<uint32_t>(), C.cq.as<uint32_t>(),
+                                             C.pv.as<uint32_t>(), C.temp.p, tb, nvalid, st);
+            if (e == cudaErrorNotReady) {
+                C.temp.ensure(tb);
+                tb = C.temp.cap;
+                e = launch_lut_build(Q, P.word_size, nb, C.pos_off.as<uint64_t>(), npos, ncs, npv,
+                                     C.lut_keys.as<uint32_t>(), C.lut_vals.as<uint32_t>(), C.lut_keys2.as<uint32_t>(),
+                                     C.lut_vals2.as<uint32_t>(), C.lut_counts.as<uint32_t>(), C.cs.as<uint32_t>(),
+                                     C.cq.as<uint32_t>(), C.pv.as<uint32_t>(), C.temp.p, tb, nvalid, st);
+            }
+            CK(e);
+        }
+        ev.stop(st);
         CK(cudaStreamSynchronize(st));
+        ctr.gpu_ms_lookup += ev.ms();
+        ctr.launches += 3;  // codes, place, pv
         ctr.ms_lookup += ms_since(t0);
+        auto qhost = [&](uint32_t local) { return QH.host.data() + QH.off[qb + local]; };
 
-        // ---- scan: count, offsets, write
+        // ---- scan: count, offsets, write (pair ids are local to the sub-batch)
         t0 = std::chrono::steady_clock::now();
-        const uint64_t pair0 = (uint64_t)qb * ns;
-        // pair ids are relative to this sub-batch: query index qi - qb
         const uint64_t npairs = (uint64_t)nb * ns;
         C.counts.ensure((npairs + 1) * 4);
         C.offs.ensure((npairs + 1) * 8);
         CK(cudaMemsetAsync(C.counts.p, 0, (npairs + 1) * 4, st));
+        ev.start(st);
         CK(launch_scan(false, C.L, Q, P.word_size, 0, npairs, C.counts.as<uint32_t>(), nullptr, nullptr, nullptr,
                        C.sms, st));
         size_t tb = 0;
         CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), nullptr, tb, st));
         C.temp.ensure(tb);
         CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), C.temp.p, tb, st));
+        ev.stop(st);
         uint64_t nh = 0;
         CK(cudaMemcpyAsync(&nh, C.offs.as<uint64_t>() + npairs, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        ctr.gpu_ms_scan += ev.ms();
         if (nh >= 0xffffffffull) throw Fail(RMB_ELIMIT, "more than 2^32 word hits in one batch");
         ctr.word_hits += nh;
         C.hits.ensure(nh * sizeof(SeedHit));
         C.hit_pair.ensure(nh * 4);
+        ev.start(st);
         CK(launch_scan(true, C.L, Q, P.word_size, 0, npairs, nullptr, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
                        C.hit_pair.as<uint32_t>(), C.sms, st));
+        ev.stop(st);
         CK(cudaStreamSynchronize(st));
+        ctr.gpu_ms_scan += ev.ms();
+        ctr.launches += 2;
         ctr.ms_scan += ms_since(t0);
-        (void)pair0;
 
         // ---- ungapped extension of every hit, then the per-pair dedup
         t0 = std::chrono::steady_clock::now();
         C.ub.ensure(nh * sizeof(UngBox));
+        ev.start(st);
         CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
                            C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st));
+        ev.stop(st);
         CK(cudaStreamSynchronize(st));
+        ctr.gpu_ms_ungapped += ev.ms();
+        ctr.launches += nh ? 1 : 0;
         ctr.ms_ungapped += ms_since(t0);
         t0 = std::chrono::steady_clock::now();
         C.flags.ensure(nh + 1);
         C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
         C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+        ev.start(st);
         CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], 0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
                         C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
+        ev.stop(st);
+        ctr.launches += 1;
         C.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
         C.n_sel.ensure(16);
         tb = 0;
@@ -316,6 +326,7 @@ void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint
         uint32_t nu = 0;
         CK(cudaMemcpyAsync(&nu, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        ctr.gpu_ms_dedup += ev.ms();
         ctr.ms_dedup += ms_since(t0);
         ctr.ungapped += nu;
         if (taps && (taps->seeds || taps->ungapped)) {
@@ -401,22 +412,31 @@ void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint
         CK(cudaMemsetAsync(C.n_wide.p, 0, 16, st));
         CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
         CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
+        ev.start(st);
         CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
                          C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(), C.wide.as<uint32_t>(),
                          C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(), C.sms, st));
+        ev.stop(st);
+        ctr.launches += nu ? 1 : 0;
         uint32_t nw = 0;
         CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        ctr.gpu_ms_prelim += ev.ms();
         if (nw) {
             uint32_t qmax = 0;
             for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
             const uint64_t cap = (uint64_t)std::max(qmax, C.max_slen) + 2;
             const uint32_t threads = std::min<uint32_t>(nw, (uint32_t)std::max<uint64_t>(128, (1ull << 31) / (cap * 8)));
             C.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
+            EvTimer ew;
+            ew.start(st);
+            ctr.launches += 1;
             CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(), C.ung_idx.as<uint32_t>(),
                                   C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
                                   C.po.as<PrelimOut>(), C.band.as<int2>(), cap, threads,
                                   C.cells.as<unsigned long long>(), C.fails.as<unsigned int>(), st));
+            ew.stop(st);
+            ctr.gpu_ms_prelim += ew.ms();
         }
         unsigned long long cells = 0;
         unsigned int fails = 0;
@@ -436,6 +456,7 @@ void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint
         CK(cudaMemcpyAsync(&nsv, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         C.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
+        ctr.launches += nsv ? 1 : 0;
         CK(launch_gather_survivors(nsv, C.sel.as<uint32_t>(), C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
                                    C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
                                    C.surv.as<SurvivorRec>(), st));
@@ -528,15 +549,20 @@ void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint
                 C.tb_ops.ensure(todo.size() * (uint64_t)ops_cap * 4);
                 C.tb_scratch.ensure((uint64_t)threads * per_thread);
                 CK(cudaMemsetAsync(C.cells.p, 0, 8, st));
+                EvTimer et;
+                et.start(st);
+                ctr.launches += 1;
                 CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), C.tb_in.as<TbIn>(),
                                     C.tb_out.as<TbOut>(), C.tb_ops.as<uint32_t>(), ops_cap, C.tb_scratch.as<uint8_t>(),
                                     per_thread, band_cells, rows_cap, threads, C.cells.as<unsigned long long>(), st));
+                et.stop(st);
                 std::vector<TbOut> to(todo.size());
                 std::vector<uint32_t> ops((uint64_t)todo.size() * ops_cap);
                 CK(cudaMemcpyAsync(to.data(), C.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(ops.data(), C.tb_ops.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                ctr.gpu_ms_traceback += et.ms();
                 std::vector<uint32_t> again;
                 for (size_t i = 0; i < todo.size(); ++i) {
                     const TbOut& o = to[i];
@@ -574,7 +600,7 @@ void run_search(rmb_ctx& C, uint32_t nq, const uint8_t* const* query, const uint
         std::vector<std::vector<Hit>> pair_hits(np);
         parallel_for(np, [&](size_t k) {
             const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
-            const uint8_t* qs = query[qb + qi];
+            const uint8_t* qs = qhost(qi);
             std::vector<uint8_t> qrc = revcomp_full(qs, hqlen[qi] + 2);
             SubjectView v;
             v.align = C.h_align.data() + C.plus_off[si];
@@ -759,66 +785,98 @@ static void check_queries(uint32_t nq, const uint8_t* const* query, const uint32
             throw Fail(RMB_EINVAL, "query is not sentinel-wrapped BLASTNA");
 }
 
-int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, rmb_results** out,
-                     char* err, size_t errlen) {
+static rmb_queries* make_queries(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen) {
+    check_queries(nq, query, qlen);
+    rmb_queries* H = new rmb_queries();
+    try {
+        H->n = nq;
+        H->device = C->p.device;
+        H->len.assign(qlen, qlen + nq);
+        H->off.resize(nq);
+        uint64_t tot = 0;
+        for (uint32_t i = 0; i < nq; ++i) {
+            H->off[i] = tot;
+            tot += (uint64_t)qlen[i] + 2;
+        }
+        H->host.resize(std::max<uint64_t>(tot, 1));
+        for (uint32_t i = 0; i < nq; ++i) memcpy(H->host.data() + H->off[i], query[i], (size_t)qlen[i] + 2);
+        cudaStream_t st = C->st;
+        H->d_q.ensure(H->host.size());
+        H->d_qrc.ensure(H->host.size());
+        CK(cudaMemcpyAsync(H->d_q.p, H->host.data(), tot, cudaMemcpyHostToDevice, st));
+        upload(H->d_off, H->off, st);
+        upload(H->d_len, H->len, st);
+        CK(launch_revcomp(H->d_q.as<uint8_t>(), H->d_off.as<uint64_t>(), H->d_len.as<uint32_t>(), nq,
+                          H->d_qrc.as<uint8_t>(), st));
+        CK(cudaStreamSynchronize(st));
+        return H;
+    } catch (...) {
+        H->release();
+        delete H;
+        throw;
+    }
+}
+
+static rmb_results* pack_results(const std::vector<std::vector<Hit>>& hits, const rmb_counters& ctr) {
+    const uint32_t nq = (uint32_t)hits.size();
+    uint64_t nh = 0, nops = 0, nseq = 0;
+    for (auto& v : hits)
+        for (auto& h : v) {
+            ++nh;
+            nops += h.script.size();
+            nseq += h.q_seq.size();
+        }
+    rmb_results* R = (rmb_results*)calloc(1, sizeof(rmb_results));
+    if (!R) throw std::bad_alloc();
+    R->n_queries = nq;
+    R->query_off = (uint64_t*)malloc((nq + 1) * sizeof(uint64_t));
+    R->hsps = (rmb_hsp*)malloc(std::max<uint64_t>(nh, 1) * sizeof(rmb_hsp));
+    R->ops = (uint32_t*)malloc(std::max<uint64_t>(nops, 1) * 4);
+    R->q_seq = (uint8_t*)malloc(std::max<uint64_t>(nseq, 1));
+    R->s_seq = (uint8_t*)malloc(std::max<uint64_t>(nseq, 1));
+    if (!R->query_off || !R->hsps || !R->ops || !R->q_seq || !R->s_seq) {
+        rmb_results_free(R);
+        throw std::bad_alloc();
+    }
+    R->n_hsps = nh;
+    uint64_t k = 0, o = 0, s = 0;
+    for (uint32_t qi = 0; qi < nq; ++qi) {
+        R->query_off[qi] = k;
+        for (auto& h : hits[qi]) {
+            rmb_hsp& x = R->hsps[k++];
+            x.score = h.score;
+            x.q_start = h.q_start; x.q_end = h.q_end; x.q_len = h.q_len;
+            x.s_start = h.s_start; x.s_end = h.s_end; x.s_len = h.s_len;
+            x.subject_oid = h.oid;
+            x.strand = h.strand;
+            x.matches = h.stats.matches; x.mismatches = h.stats.mismatches;
+            x.query_gaps = h.stats.query_gaps; x.subject_gaps = h.stats.subject_gaps;
+            x.transitions = h.stats.transitions; x.transversions = h.stats.transversions;
+            x.cpg_sites = h.stats.cpg_sites;
+            x.perc_sub = h.stats.perc_sub; x.perc_query_gap = h.stats.perc_query_gap;
+            x.perc_db_gap = h.stats.perc_db_gap;
+            x.kdiv = h.stats.kdiv; x.cpg_kdiv = h.stats.cpg_kdiv;
+            x.ops_off = o;
+            x.ops_len = (uint32_t)h.script.size();
+            for (auto& r : h.script) R->ops[o++] = ((uint32_t)r.op << 30) | r.n;
+            x.seq_off = s;
+            x.aln_len = (uint32_t)h.q_seq.size();
+            memcpy(R->q_seq + s, h.q_seq.data(), h.q_seq.size());
+            memcpy(R->s_seq + s, h.s_seq.data(), h.s_seq.size());
+            s += h.q_seq.size();
+        }
+    }
+    R->query_off[nq] = k;
+    R->counters = ctr;
+    return R;
+}
+
+int rmb_queries_upload(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen,
+                       rmb_queries** out, char* err, size_t errlen) {
     try {
         if (!C || !out) throw Fail(RMB_EINVAL, "null argument");
-        if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_search_batch");
-        check_queries(nq, query, qlen);
         CK(cudaSetDevice(C->p.device));
-        std::vector<std::vector<Hit>> hits;
-        rmb_counters ctr{};
-        run_search(*C, nq, query, qlen, hits, ctr, nullptr);
-        uint64_t nh = 0, nops = 0, nseq = 0;
-        for (auto& v : hits)
-            for (auto& h : v) {
-                ++nh;
-                nops += h.script.size();
-                nseq += h.q_seq.size();
-            }
-        rmb_results* R = (rmb_results*)calloc(1, sizeof(rmb_results));
-        if (!R) throw std::bad_alloc();
-        R->n_queries = nq;
-        R->query_off = (uint64_t*)malloc((nq + 1) * sizeof(uint64_t));
-        R->hsps = (rmb_hsp*)malloc(std::max<uint64_t>(nh, 1) * sizeof(rmb_hsp));
-        R->ops = (uint32_t*)malloc(std::max<uint64_t>(nops, 1) * 4);
-        R->q_seq = (uint8_t*)malloc(std::max<uint64_t>(nseq, 1));
-        R->s_seq = (uint8_t*)malloc(std::max<uint64_t>(nseq, 1));
-        if (!R->query_off || !R->hsps || !R->ops || !R->q_seq || !R->s_seq) {
-            rmb_results_free(R);
-            throw std::bad_alloc();
-        }
-        R->n_hsps = nh;
-        uint64_t k = 0, o = 0, s = 0;
-        for (uint32_t qi = 0; qi < nq; ++qi) {
-            R->query_off[qi] = k;
-            for (auto& h : hits[qi]) {
-                rmb_hsp& x = R->hsps[k++];
-                x.score = h.score;
-                x.q_start = h.q_start; x.q_end = h.q_end; x.q_len = h.q_len;
-                x.s_start = h.s_start; x.s_end = h.s_end; x.s_len = h.s_len;
-                x.subject_oid = h.oid;
-                x.strand = h.strand;
-                x.matches = h.stats.matches; x.mismatches = h.stats.mismatches;
-                x.query_gaps = h.stats.query_gaps; x.subject_gaps = h.stats.subject_gaps;
-                x.transitions = h.stats.transitions; x.transversions = h.stats.transversions;
-                x.cpg_sites = h.stats.cpg_sites;
-                x.perc_sub = h.stats.perc_sub; x.perc_query_gap = h.stats.perc_query_gap;
-                x.perc_db_gap = h.stats.perc_db_gap;
-                x.kdiv = h.stats.kdiv; x.cpg_kdiv = h.stats.cpg_kdiv;
-                x.ops_off = o;
-                x.ops_len = (uint32_t)h.script.size();
-                for (auto& r : h.script) R->ops[o++] = ((uint32_t)r.op << 30) | r.n;
-                x.seq_off = s;
-                x.aln_len = (uint32_t)h.q_seq.size();
-                memcpy(R->q_seq + s, h.q_seq.data(), h.q_seq.size());
-                memcpy(R->s_seq + s, h.s_seq.data(), h.s_seq.size());
-                s += h.q_seq.size();
-            }
-        }
-        R->query_off[nq] = k;
-        R->counters = ctr;
-        *out = R;
+        *out = make_queries(C, nq, query, qlen);
         return RMB_OK;
     } catch (const Fail& e) {
         return fail_out(e, err, errlen, e.code);
@@ -829,14 +887,51 @@ int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const
     }
 }
 
+int rmb_search_resident(rmb_ctx* C, rmb_queries* H, rmb_results** out, char* err, size_t errlen) {
+    try {
+        if (!C || !H || !out) throw Fail(RMB_EINVAL, "null argument");
+        if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before the search");
+        if (H->device != C->p.device) throw Fail(RMB_EINVAL, "queries were uploaded to another device");
+        CK(cudaSetDevice(C->p.device));
+        std::vector<std::vector<Hit>> hits;
+        rmb_counters ctr{};
+        run_search(*C, *H, hits, ctr, nullptr);
+        *out = pack_results(hits, ctr);
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+void rmb_queries_free(rmb_queries* H) {
+    if (!H) return;
+    cudaSetDevice(H->device);
+    H->release();
+    delete H;
+}
+
+int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, rmb_results** out,
+                     char* err, size_t errlen) {
+    rmb_queries* H = nullptr;
+    int rc = rmb_queries_upload(C, nq, query, qlen, &H, err, errlen);
+    if (rc != RMB_OK) return rc;
+    rc = rmb_search_resident(C, H, out, err, errlen);
+    rmb_queries_free(H);
+    return rc;
+}
+
 int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, int32_t stage,
                     uint32_t** records, uint64_t* n_records, char* err, size_t errlen) {
     try {
         if (!C || !records || !n_records) throw Fail(RMB_EINVAL, "null argument");
         if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_debug_stage");
         if (stage < 0 || stage > 2) throw Fail(RMB_EINVAL, "stage must be 0, 1 or 2");
-        check_queries(nq, query, qlen);
         CK(cudaSetDevice(C->p.device));
+        std::unique_ptr<rmb_queries, void (*)(rmb_queries*)> H(make_queries(C, nq, query, qlen), rmb_queries_free);
         std::vector<uint32_t> v;
         Taps t;
         if (stage == 0) t.seeds = &v;
@@ -844,7 +939,7 @@ int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const 
         else t.prelims = &v;
         std::vector<std::vector<Hit>> hits;
         rmb_counters ctr{};
-        run_search(*C, nq, query, qlen, hits, ctr, &t);
+        run_search(*C, *H, hits, ctr, &t);
         const uint64_t width = stage == 0 ? 3 : stage == 1 ? 6 : 8;
         uint32_t* r = (uint32_t*)malloc(std::max<size_t>(v.size(), 1) * 4);
         if (!r) throw std::bad_alloc();
@@ -927,7 +1022,8 @@ void rmb_ctx_destroy(rmb_ctx* C) {
     if (!C) return;
     cudaSetDevice(C->p.device);
     DBuf* all[] = {&C->d_plus, &C->d_rc, &C->d_align, &C->d_align_rc, &C->d_packed, &C->d_plus_off, &C->d_packed_off,
-                   &C->d_len, &C->d_params, &C->q, &C->qrc, &C->qoff, &C->qlen, &C->pv, &C->pv_off, &C->cs, &C->cs_off,
+                   &C->d_len, &C->d_params, &C->pv, &C->pv_off, &C->cs, &C->cs_off, &C->pos_off, &C->lut_keys,
+                   &C->lut_vals, &C->lut_keys2, &C->lut_vals2, &C->lut_counts,
                    &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
                    &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,

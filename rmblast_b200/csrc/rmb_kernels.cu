@@ -1044,3 +1044,155 @@ cudaError_t launch_offsets(const uint32_t* counts, uint64_t n, uint64_t* offs, v
 }
 
 }  // namespace rmb
+
+// ---------------------------------------------------------------------------------------
+// lookup tables on the device: blast/nalookup.rs:128-335 and blast/mblookup.rs:106-235 as one
+// CSR per query.  Every lw-mer of [fwd | N | rc] whose bases are all A/C/G/T, inside a context
+// at least word_size long, goes to cell `code`; a stable radix sort by (query, code) keeps the
+// positions ascending, and the megablast tables (lw > 8) are reversed per cell, which is the
+// order their hash chains return (mblookup.rs:80-95).
+// ---------------------------------------------------------------------------------------
+#include <cub/device/device_radix_sort.cuh>
+
+namespace rmb {
+
+constexpr uint32_t NO_CODE = 0xffffffffu;
+
+__global__ void k_lut_codes(DevQueries Q, int32_t ws, const uint64_t* __restrict__ pos_off,
+                            uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t* __restrict__ counts) {
+    const uint32_t qi = blockIdx.x;
+    const uint32_t n = Q.len[qi];
+    const int lw = Q.lw[qi];
+    const uint8_t* q = Q.q + Q.off[qi];      // sentinel-wrapped forward query
+    const uint8_t* r = Q.qrc + Q.off[qi];    // sentinel-wrapped reverse complement
+    const uint64_t base = pos_off[qi];
+    const uint64_t cbase = Q.cs_off[qi];
+    const uint32_t total = 2 * n + 1;
+    const bool ok = (int64_t)ws <= (int64_t)n;  // each context is n bases long
+    for (uint32_t s = threadIdx.x; s < total; s += blockDim.x) {
+        uint32_t code = NO_CODE;
+        if (ok && s != n) {
+            // context 0 = [0, n-1], context 1 = [n+1, 2n]
+            const uint32_t ctx_end = s < n ? n - 1 : 2 * n;
+            if (s + (uint32_t)lw - 1 <= ctx_end) {
+                uint32_t c = 0;
+                bool valid = true;
+                for (int k = 0; k < lw; ++k) {
+                    const uint32_t t = s + k;
+                    const uint8_t b = t < n ? q[1 + t] : r[1 + (t - n - 1)];
+                    if (b & 0xFC) { valid = false; break; }
+                    c = (c << 2) | b;
+                }
+                if (valid) code = c;
+            }
+        }
+        keys[base + s] = code == NO_CODE ? NO_CODE : (uint32_t)(cbase + code);
+        vals[base + s] = s;
+        if (code != NO_CODE) atomicAdd(counts + cbase + code, 1u);
+    }
+}
+
+__global__ void k_lut_place(uint64_t n_valid, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                            const uint32_t* __restrict__ cs, const uint64_t* __restrict__ cs_off, const int32_t* lw,
+                            uint32_t nq, uint32_t* __restrict__ cell_q) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_valid;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t key = keys[k];
+        // query of this key: last cs_off <= key
+        uint32_t lo = 0, hi = nq;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (cs_off[mid] <= key) lo = mid;
+            else hi = mid;
+        }
+        uint64_t dst = k;
+        if (lw[lo] > 8) dst = (uint64_t)cs[key] + cs[key + 1] - 1 - (k - cs[key]);
+        cell_q[dst] = vals[k];
+    }
+}
+
+__global__ void k_lut_pv(uint64_t n_words_total, const uint64_t* __restrict__ pv_off, const uint64_t* __restrict__ cs_off,
+                         const int32_t* __restrict__ lw, uint32_t nq, const uint32_t* __restrict__ counts,
+                         uint32_t* __restrict__ pv) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n_words_total;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nq;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (pv_off[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        const uint64_t cells = 1ull << (2 * lw[lo]);
+        const uint64_t c0 = (w - pv_off[lo]) * 32;
+        uint32_t bits = 0;
+        for (uint32_t b = 0; b < 32 && c0 + b < cells; ++b)
+            if (counts[cs_off[lo] + c0 + b]) bits |= 1u << b;
+        pv[w] = bits;
+    }
+}
+
+cudaError_t launch_lut_build(const DevQueries& Q, int32_t ws, uint32_t nq, const uint64_t* pos_off, uint64_t n_pos,
+                             uint64_t n_cells, uint64_t n_pv, uint32_t* keys, uint32_t* vals, uint32_t* keys2,
+                             uint32_t* vals2, uint32_t* counts, uint32_t* cs, uint32_t* cell_q, uint32_t* pv,
+                             void* temp, size_t& temp_bytes, uint64_t& n_valid, cudaStream_t st) {
+    // temp sizing pass
+    size_t t_scan = 0, t_sort = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, t_scan, counts, cs, (int64_t)n_cells + 1, st);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceRadixSort::SortPairs(nullptr, t_sort, keys, keys2, vals, vals2, (int64_t)n_pos, 0, 32, st);
+    if (e != cudaSuccess) return e;
+    const size_t need = t_scan > t_sort ? t_scan : t_sort;
+    if (!temp || temp_bytes < need) {
+        temp_bytes = need;
+        return cudaErrorNotReady;  // caller grows temp and calls again
+    }
+    e = cudaMemsetAsync(counts, 0, (n_cells + 1) * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_lut_codes<<<nq, 512, 0, st>>>(Q, ws, pos_off, keys, vals, counts);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    size_t tb = temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(temp, tb, counts, cs, (int64_t)n_cells + 1, st);
+    if (e != cudaSuccess) return e;
+    tb = temp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, (int64_t)n_pos, 0, 32, st);
+    if (e != cudaSuccess) return e;
+    uint32_t nv = 0;
+    e = cudaMemcpyAsync(&nv, cs + n_cells, 4, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    n_valid = nv;
+    if (nv) {
+        const int blocks = (int)((nv + 255) / 256 < 65536 ? (nv + 255) / 256 : 65536);
+        k_lut_place<<<blocks, 256, 0, st>>>(nv, keys2, vals2, cs, Q.cs_off, Q.lw, nq, cell_q);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    const int pb = (int)((n_pv + 255) / 256 < 65536 ? (n_pv + 255) / 256 : 65536);
+    k_lut_pv<<<pb, 256, 0, st>>>(n_pv, Q.pv_off, Q.cs_off, Q.lw, nq, counts, pv);
+    return cudaGetLastError();
+}
+
+}  // namespace rmb
+
+namespace rmb {
+// reverse complement of every sentinel-wrapped query (encoding.rs:136 revcomp_blastna)
+__global__ void k_revcomp(const uint8_t* __restrict__ q, const uint64_t* __restrict__ off,
+                          const uint32_t* __restrict__ len, uint8_t* __restrict__ rc) {
+    __shared__ uint8_t comp[16];
+    if (threadIdx.x < 16) {
+        const uint8_t c[16] = {3, 2, 1, 0, 5, 4, 7, 6, 8, 9, 13, 12, 11, 10, 14, 15};
+        comp[threadIdx.x] = c[threadIdx.x];
+    }
+    __syncthreads();
+    const uint64_t o = off[blockIdx.x];
+    const uint32_t n = len[blockIdx.x] + 2;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) rc[o + i] = comp[q[o + n - 1 - i] & 15];
+}
+
+cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* rc,
+                           cudaStream_t st) {
+    if (!nq) return cudaSuccess;
+    k_revcomp<<<nq, 256, 0, st>>>(q, off, len, rc);
+    return cudaGetLastError();
+}
+}  // namespace rmb

@@ -53,3 +53,20 @@ cudaError_t launch_select_prelim(const PrelimOut* po, uint64_t n, uint32_t* out,
 cudaError_t launch_offsets(const uint32_t* counts, uint64_t n, uint64_t* offs, void* temp, size_t& temp_bytes,
                            cudaStream_t st);
 }  // namespace rmb
+
+namespace rmb {
+// Builds the lookup tables of nq queries on the device (Q.q/qrc/off/len/lw/cs_off/pv_off set;
+// cell_start values are global offsets into cell_q, so Q.cq_off must be all zero).
+// pos_off[i] = sum over earlier queries of (2 len + 1); n_pos the total; n_cells the sum of
+// (4^lw + 1); n_pv the pv words.  Returns cudaErrorNotReady with temp_bytes set when temp is
+// too small.  n_valid = table entries.
+cudaError_t launch_lut_build(const DevQueries& Q, int32_t ws, uint32_t nq, const uint64_t* pos_off, uint64_t n_pos,
+                             uint64_t n_cells, uint64_t n_pv, uint32_t* keys, uint32_t* vals, uint32_t* keys2,
+                             uint32_t* vals2, uint32_t* counts, uint32_t* cs, uint32_t* cell_q, uint32_t* pv,
+                             void* temp, size_t& temp_bytes, uint64_t& n_valid, cudaStream_t st);
+}  // namespace rmb
+
+namespace rmb {
+cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* rc,
+                           cudaStream_t st);
+}  // namespace rmb
