@@ -127,7 +127,9 @@ int rmb_format_tabular(const rmb_ctx* ctx, const rmb_results* res, const char* c
  * them: stage 0 = post-dedup seeds (strand, q, s per record: 3 uint32), stage 1 = sorted
  * ungapped hits (strand, qs, qe, ss, se, score: 6 uint32), stage 2 = preliminary HSPs after the
  * prelim endpoint purge (strand, qs, qe, ss, se, score, q_seed, s_seed: 8 uint32), for every
- * (query, subject) pair in pair order.  *records is malloc'd; free with rmb_text_free. */
+ * (query, subject) pair in pair order; stage 3 = the query lookup tables (query, cell, position:
+ * 3 uint32 per entry in retrieval order; position 0xffffffff flags a cell whose presence bit
+ * disagrees with its entries) -- blast/nalookup.rs:301 / blast/mblookup.rs:190.  *records is malloc'd; free with rmb_text_free. */
 int rmb_debug_stage(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
                     int32_t stage, uint32_t** records, uint64_t* n_records, char* err, size_t errlen);
 

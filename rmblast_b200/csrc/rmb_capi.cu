@@ -173,6 +173,7 @@ struct Taps {
     std::vector<uint32_t>* seeds = nullptr;     // strand, q, s
     std::vector<uint32_t>* ungapped = nullptr;  // strand, qs, qe, ss, se, score
     std::vector<uint32_t>* prelims = nullptr;   // strand, qs, qe, ss, se, score, q_seed, s_seed
+    std::vector<uint32_t>* lookup = nullptr;    // query, cell, position (retrieval order)
 };
 
 // One search over resident queries: per-query hits in the reference's order.
@@ -261,6 +262,23 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         CK(cudaStreamSynchronize(st));
         ctr.gpu_ms_lookup += ev.ms();
         ctr.launches += 3;  // codes, place, pv
+        if (taps && taps->lookup) {
+            std::vector<uint32_t> hcs(ncs + 1), hcq(npos), hpv(npv);
+            CK(cudaMemcpy(hcs.data(), C.cs.p, (ncs + 1) * 4, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(hcq.data(), C.cq.p, npos * 4, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(hpv.data(), C.pv.p, npv * 4, cudaMemcpyDeviceToHost));
+            for (uint32_t i = 0; i < nb; ++i) {
+                const uint64_t cells = 1ull << (2 * hlw[i]);
+                for (uint64_t c = 0; c < cells; ++c) {
+                    const uint32_t b = hcs[hcsoff[i] + c], e = hcs[hcsoff[i] + c + 1];
+                    const bool present = (hpv[hpvoff[i] + (c >> 5)] >> (c & 31)) & 1u;
+                    if (present != (e > b)) taps->lookup->insert(taps->lookup->end(), {qb + i, (uint32_t)c, 0xffffffffu});
+                    for (uint32_t j = b; j < e; ++j) taps->lookup->insert(taps->lookup->end(), {qb + i, (uint32_t)c, hcq[j]});
+                }
+            }
+            qb = qe;
+            continue;
+        }
         ctr.ms_lookup += ms_since(t0);
         auto qhost = [&](uint32_t local) { return QH.host.data() + QH.off[qb + local]; };
 
@@ -929,18 +947,19 @@ int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const 
     try {
         if (!C || !records || !n_records) throw Fail(RMB_EINVAL, "null argument");
         if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_debug_stage");
-        if (stage < 0 || stage > 2) throw Fail(RMB_EINVAL, "stage must be 0, 1 or 2");
+        if (stage < 0 || stage > 3) throw Fail(RMB_EINVAL, "stage must be 0..3");
         CK(cudaSetDevice(C->p.device));
         std::unique_ptr<rmb_queries, void (*)(rmb_queries*)> H(make_queries(C, nq, query, qlen), rmb_queries_free);
         std::vector<uint32_t> v;
         Taps t;
         if (stage == 0) t.seeds = &v;
         else if (stage == 1) t.ungapped = &v;
-        else t.prelims = &v;
+        else if (stage == 2) t.prelims = &v;
+        else t.lookup = &v;
         std::vector<std::vector<Hit>> hits;
         rmb_counters ctr{};
         run_search(*C, *H, hits, ctr, &t);
-        const uint64_t width = stage == 0 ? 3 : stage == 1 ? 6 : 8;
+        const uint64_t width = stage == 0 ? 3 : stage == 1 ? 6 : stage == 2 ? 8 : 3;
         uint32_t* r = (uint32_t*)malloc(std::max<size_t>(v.size(), 1) * 4);
         if (!r) throw std::bad_alloc();
         if (!v.empty()) memcpy(r, v.data(), v.size() * 4);

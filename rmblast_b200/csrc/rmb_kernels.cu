@@ -1106,7 +1106,7 @@ __global__ void k_lut_place(uint64_t n_valid, const uint32_t* __restrict__ keys,
             else hi = mid;
         }
         uint64_t dst = k;
-        if (lw[lo] > 8) dst = (uint64_t)cs[key] + cs[key + 1] - 1 - (k - cs[key]);
+        if (lw[lo] > 8) dst = (uint64_t)cs[key + 1] - 1 - (k - cs[key]);  // reverse within the cell
         cell_q[dst] = vals[k];
     }
 }

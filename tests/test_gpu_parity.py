@@ -146,3 +146,33 @@ def test_edge_cases():
     m = api.ScoreMatrix.from_text(mt, "comparison.matrix")
     with pytest.raises(api.RmbError):
         api.Searcher(api.SearchParams(dust=True), m, api.SubjectDb.from_fasta(db))
+
+
+def test_lookup_tables_match_reference_rules():
+    """Stage 3: the device-built tables hold, per cell, exactly the positions of the reference's
+    table in its retrieval order (ascending for lw <= 8, descending for the megablast table)."""
+    p = dict(O.RM_PARAMS, mask_level=101)
+    mt, db, q = (G / "comparison.matrix").read_text(), (G / "db.fa").read_text(), (G / "query.fa").read_text()
+    s = searcher(p, mt, "comparison.matrix", db)
+    qs = [api.encode(seq) for _, seq in api.read_fasta(q)]
+    got = s.stage(qs, 3)
+    comp = np.array([3, 2, 1, 0, 5, 4, 7, 6, 8, 9, 13, 12, 11, 10, 14, 15], np.uint8)
+    for qi, e in enumerate(qs):
+        n = len(e) - 2
+        comb = np.concatenate([e[1:n + 1], [14], comp[e[1:n + 1][::-1]]]).astype(np.int64)
+        lw = 8 if 2 * n < 8500 else 11 if 2 * n < 300000 else 12  # choose_lut_width, word 14
+        ent = []
+        for s0 in range(2 * n + 1):
+            end = n - 1 if s0 < n else 2 * n
+            if s0 == n or s0 + lw - 1 > end:
+                continue
+            w = comb[s0:s0 + lw]
+            if (w > 3).any():
+                continue
+            c = 0
+            for b in w:
+                c = (c << 2) | int(b)
+            ent.append((c, s0))
+        ent.sort(key=lambda t: (t[0], t[1] if lw <= 8 else -t[1]))
+        want = np.array([(qi, c, x) for c, x in ent], dtype=np.uint32).reshape(-1, 3)
+        assert np.array_equal(got[got[:, 0] == qi], want), qi
