@@ -129,7 +129,10 @@ int rmb_format_tabular(const rmb_ctx* ctx, const rmb_results* res, const char* c
  * prelim endpoint purge (strand, qs, qe, ss, se, score, q_seed, s_seed: 8 uint32), for every
  * (query, subject) pair in pair order; stage 3 = the query lookup tables (query, cell, position:
  * 3 uint32 per entry in retrieval order; position 0xffffffff flags a cell whose presence bit
- * disagrees with its entries) -- blast/nalookup.rs:301 / blast/mblookup.rs:190.  *records is malloc'd; free with rmb_text_free. */
+ * disagrees with its entries) -- blast/nalookup.rs:301 / blast/mblookup.rs:190; stage 4 = the
+ * traceback of every post-purge prelim in the order engine.rs:1471-1485 visits them, before the
+ * Phase 2b containment filter (strand, status 0 = alignment / 1 = none, score, q0, q1, s0, s1 in
+ * the DP frame, number of edit runs, FNV-1a of the runs: 9 uint32) -- engine.rs:2953-3039.  *records is malloc'd; free with rmb_text_free. */
 int rmb_debug_stage(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
                     int32_t stage, uint32_t** records, uint64_t* n_records, char* err, size_t errlen);
 

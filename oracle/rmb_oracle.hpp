@@ -172,6 +172,10 @@ std::vector<AlignResult> search_query(const std::vector<uint8_t>& query, const s
                                       const std::vector<Subject>& db, const Params& p,
                                       const Matrix& m, int threads, Counters* counters);
 
+// Traceback stage tap: every post-purge prelim of one pair, unfiltered (see the engine).
+std::vector<uint32_t> pair_tracebacks(const QueryLookup& ql, const std::vector<uint8_t>& query, const Subject& subj,
+                                      const Params& p, const Matrix& m);
+
 // engine.rs:863 (cross-subject mode, oid = subject index)
 void apply_mask_level(std::vector<AlignResult>& r, uint32_t mask_level);
 // engine.rs:998

@@ -183,6 +183,11 @@ int rmbo_stage_text(const char* query_fasta, const char* db_fasta, const char* m
                                                  q.seq.size() - 2, db.empty() ? 0 : total / db.size());
             QueryLookup ql = build_query_lookup(q.seq, pq);
             for (auto& s : db) {
+                if (stage == 4) {
+                    auto v = pair_tracebacks(ql, q.seq, s, pq, m);
+                    rec.insert(rec.end(), v.begin(), v.end());
+                    continue;
+                }
                 std::vector<SeedRecord> seeds;
                 std::vector<UngappedHit> ung;
                 std::vector<PrelimHsp> pre;
@@ -202,7 +207,7 @@ int rmbo_stage_text(const char* query_fasta, const char* db_fasta, const char* m
         uint32_t* o = (uint32_t*)malloc(std::max<size_t>(rec.size(), 1) * 4);
         if (!rec.empty()) memcpy(o, rec.data(), rec.size() * 4);
         *out = o;
-        *n_out = rec.size() / (stage == 0 ? 3 : stage == 1 ? 6 : 8);
+        *n_out = rec.size() / (stage == 0 ? 3 : stage == 1 ? 6 : stage == 2 ? 8 : 9);
         return 0;
     } catch (const std::exception& e) {
         set_err(err, errlen, e.what());

@@ -1071,6 +1071,51 @@ std::vector<AlignResult> search_pair(const QueryLookup& ql, const std::vector<ui
     return phase2b(query, ql.query_rc, qid, subj, std::move(pre), p, m, taps.counters);
 }
 
+// Traceback of every post-purge prelim of one pair, in the order traceback_phase visits them
+// (engine.rs:1471-1485 stable sort), containment not applied: per prelim (strand, status
+// 0 = alignment / 1 = none, score, q0, q1, s0, s1 in the DP frame, n_ops, FNV-1a of the ops).
+std::vector<uint32_t> pair_tracebacks(const QueryLookup& ql, const std::vector<uint8_t>& query, const Subject& subj,
+                                      const Params& p, const Matrix& m) {
+    std::vector<uint32_t> out;
+    std::vector<PrelimHsp> pre;
+    Taps t;
+    t.prelims = &pre;
+    search_pair(ql, query, "", subj, p, m, t);
+    const uint32_t qa = (uint32_t)query.size() - 2, sl = subj.len();
+    std::stable_sort(pre.begin(), pre.end(), [&](const PrelimHsp& a, const PrelimHsp& b) {
+        uint32_t fsa = a.strand == PLUS ? a.s_start : sl - a.s_end, fsb = b.strand == PLUS ? b.s_start : sl - b.s_end;
+        uint32_t fea = a.strand == PLUS ? a.s_end : sl - a.s_start, feb = b.strand == PLUS ? b.s_end : sl - b.s_start;
+        uint32_t qoa = a.strand == PLUS ? a.q_start : qa - a.q_end, qob = b.strand == PLUS ? b.q_start : qa - b.q_end;
+        uint32_t qea = a.strand == PLUS ? a.q_end : qa - a.q_start, qeb = b.strand == PLUS ? b.q_end : qa - b.q_start;
+        if (a.score != b.score) return a.score > b.score;
+        if (fsa != fsb) return fsa < fsb;
+        if (fea != feb) return fea > feb;
+        if (qoa != qob) return qoa < qob;
+        return qea > qeb;
+    });
+    for (const PrelimHsp& ph : pre) {
+        const bool plus = ph.strand == PLUS;
+        const std::vector<uint8_t>& sfs = plus ? subj.align : subj.align_rc;
+        uint32_t nq, ns;
+        improve_seed(query.data() + 1, qa, sfs.data() + 1, sfs.size() - 2, ph.q_seed, ph.s_seed, ph.q_start, ph.q_end,
+                     ph.s_start, ph.s_end, !plus, nq, ns);
+        const uint32_t tq = plus ? nq : qa - 1 - nq, ts = plus ? ns : sl - 1 - ns;
+        int32_t sc = 0;
+        uint32_t q0 = 0, q1 = 0, s0 = 0, s1 = 0;
+        Script es;
+        const bool ok = gapped_bidir(plus ? query : ql.query_rc, subj.align, tq, ts, p.gap_open, p.gap_extend,
+                                     p.xdrop_gap_final, m, sc, q0, q1, s0, s1, es, nullptr);
+        uint32_t h = 2166136261u;
+        for (const Op& o : es) {
+            const uint32_t v = ((uint32_t)o.op << 30) | o.n;
+            for (int b = 0; b < 4; ++b) h = (h ^ ((v >> (8 * b)) & 0xffu)) * 16777619u;
+        }
+        if (!ok) { sc = 0; q0 = q1 = s0 = s1 = 0; es.clear(); h = 2166136261u; }
+        out.insert(out.end(), {(uint32_t)ph.strand, ok ? 0u : 1u, (uint32_t)sc, q0, q1, s0, s1, (uint32_t)es.size(), h});
+    }
+    return out;
+}
+
 // engine.rs:863-974 apply_mask_level (cross-subject mode; oid = subject index)
 void apply_mask_level(std::vector<AlignResult>& res, uint32_t level) {
     if (level >= 100) return;

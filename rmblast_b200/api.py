@@ -324,7 +324,7 @@ class Searcher:
         nrec = C.c_uint64()
         err = C.create_string_buffer(1024)
         _check(lib().rmb_debug_stage(self._ctx, n, qp, ql, stage, C.byref(rec), C.byref(nrec), err, 1024), err)
-        width = (3, 6, 8, 3)[stage]
+        width = (3, 6, 8, 3, 9)[stage]
         try:
             a = np.ctypeslib.as_array(rec, shape=(int(nrec.value) * width,)).copy() if nrec.value else np.zeros(0, np.uint32)
         finally:

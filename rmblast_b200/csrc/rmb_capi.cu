@@ -174,6 +174,7 @@ struct Taps {
     std::vector<uint32_t>* ungapped = nullptr;  // strand, qs, qe, ss, se, score
     std::vector<uint32_t>* prelims = nullptr;   // strand, qs, qe, ss, se, score, q_seed, s_seed
     std::vector<uint32_t>* lookup = nullptr;    // query, cell, position (retrieval order)
+    std::vector<uint32_t>* tracebacks = nullptr;  // strand, status, score, q0, q1, s0, s1, n_ops, ops hash
 };
 
 // One search over resident queries: per-query hits in the reference's order.
@@ -612,6 +613,23 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         }
         ctr.tb_dp += tin.size();
         ctr.ms_traceback += ms_since(t0);
+        if (taps && taps->tracebacks) {
+            for (size_t k = 0; k < tin.size(); ++k) {
+                const TbResult& r = tres[k];
+                uint32_t h = 2166136261u;  // FNV-1a over the run-length ops
+                for (const RunOp& o : r.script) {
+                    const uint32_t v = ((uint32_t)o.op << 30) | o.n;
+                    for (int b = 0; b < 4; ++b) h = (h ^ ((v >> (8 * b)) & 0xffu)) * 16777619u;
+                }
+                const bool ok = r.status == 0;
+                taps->tracebacks->insert(taps->tracebacks->end(),
+                                         {tin[k].strand, ok ? 0u : 1u, ok ? (uint32_t)r.score : 0u, ok ? r.q0 : 0u,
+                                          ok ? r.q1 : 0u, ok ? r.s0 : 0u, ok ? r.s1 : 0u,
+                                          ok ? (uint32_t)r.script.size() : 0u, ok ? h : 2166136261u});
+            }
+            qb = qe;
+            continue;
+        }
 
         // ---- host Phase 2b per pair, then per query
         t0 = std::chrono::steady_clock::now();
@@ -947,7 +965,7 @@ int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const 
     try {
         if (!C || !records || !n_records) throw Fail(RMB_EINVAL, "null argument");
         if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_debug_stage");
-        if (stage < 0 || stage > 3) throw Fail(RMB_EINVAL, "stage must be 0..3");
+        if (stage < 0 || stage > 4) throw Fail(RMB_EINVAL, "stage must be 0..4");
         CK(cudaSetDevice(C->p.device));
         std::unique_ptr<rmb_queries, void (*)(rmb_queries*)> H(make_queries(C, nq, query, qlen), rmb_queries_free);
         std::vector<uint32_t> v;
@@ -955,11 +973,12 @@ int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const 
         if (stage == 0) t.seeds = &v;
         else if (stage == 1) t.ungapped = &v;
         else if (stage == 2) t.prelims = &v;
-        else t.lookup = &v;
+        else if (stage == 3) t.lookup = &v;
+        else t.tracebacks = &v;
         std::vector<std::vector<Hit>> hits;
         rmb_counters ctr{};
         run_search(*C, *H, hits, ctr, &t);
-        const uint64_t width = stage == 0 ? 3 : stage == 1 ? 6 : stage == 2 ? 8 : 3;
+        const uint64_t width = stage == 0 ? 3 : stage == 1 ? 6 : stage == 2 ? 8 : stage == 3 ? 3 : 9;
         uint32_t* r = (uint32_t*)malloc(std::max<size_t>(v.size(), 1) * 4);
         if (!r) throw std::bad_alloc();
         if (!v.empty()) memcpy(r, v.data(), v.size() * 4);

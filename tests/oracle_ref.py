@@ -83,7 +83,7 @@ def stage_text(query_fasta: str, db_fasta: str, matrix_text: str, matrix_name: s
                                C.byref(oparams(p)), stage, C.byref(rec), C.byref(n), err, 512)
     if rc:
         raise RuntimeError(err.value.decode())
-    width = (3, 6, 8)[stage]
+    width = {0: 3, 1: 6, 2: 8, 4: 9}[stage]
     try:
         a = np.ctypeslib.as_array(rec, shape=(int(n.value) * width,)).copy() if n.value else np.zeros(0, np.uint32)
     finally:

@@ -176,3 +176,21 @@ def test_lookup_tables_match_reference_rules():
         ent.sort(key=lambda t: (t[0], t[1] if lw <= 8 else -t[1]))
         want = np.array([(qi, c, x) for c, x in ent], dtype=np.uint32).reshape(-1, 3)
         assert np.array_equal(got[got[:, 0] == qi], want), qi
+
+
+@pytest.mark.parametrize("case", ["golden", "small_default"])
+def test_traceback_stage_matches_oracle(case):
+    """Stage 4: improve_seed + traceback DP + gap pruning of every prelim, unfiltered."""
+    if case == "golden":
+        p = dict(O.RM_PARAMS, mask_level=101)
+        mt, mn, db, q = (G / "comparison.matrix").read_text(), "comparison.matrix", (G / "db.fa").read_text(), \
+            (G / "query.fa").read_text()
+    else:
+        q, db, p = synthetic("small", 0.05, synth.DEFAULT_FLAGS)
+        mt, mn = synth.MATRIX_TEXT, synth.MATRIX_NAME
+    s = searcher(p, mt, mn, db)
+    qs = [api.encode(seq) for _, seq in api.read_fasta(q)]
+    got = s.stage(qs, 4)
+    want = O.stage_text(q, db, mt, mn, p, 4)
+    assert len(want) > 0
+    assert np.array_equal(got, want)
