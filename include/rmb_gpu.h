@@ -154,6 +154,25 @@ void rmb_results_free(rmb_results* res);
 void rmb_text_free(void* p);
 void rmb_ctx_destroy(rmb_ctx* ctx);
 
+/* Traceback of one (query, subject) pair's prelim HSPs without any allocation.  It has no
+ * counterpart in the reference; it is the GPU traceback of stage 4 above for callers that may not
+ * call cudaMalloc -- code embedded in a process whose device memory belongs to another allocator
+ * (a caching allocator that must account for every byte, a stream-ordered pool) or running where
+ * an allocation could fail or stall.  All pointers are device memory the caller owns:
+ * query/query_rc and subject/subject_rc are sentinel-wrapped BLASTNA (the subject with its
+ * ambiguity codes restored), prelims n x 8 uint32 in the stage-2 record layout, out n x 9 uint32
+ * in the stage-4 layout (status 2 = did not fit the scratch), ops n x ops_cap edit runs.
+ * The scratch is a fixed 32 MiB array in the library that every GPU loading the library holds
+ * until the process exits; query + subject must satisfy 8 (subject + 2) + 8 (query + 2) + 64 KiB
+ * <= 32 MiB or the call fails with RMB_ELIMIT.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  Calls share the
+ * array: two calls whose work overlaps on the GPU race.  The call waits for its stream. */
+int rmb_traceback_noalloc(int32_t device, const uint8_t* query, const uint8_t* query_rc, uint32_t qlen,
+                          const uint8_t* subject, const uint8_t* subject_rc, uint32_t slen, const uint32_t* prelims,
+                          uint32_t n, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap_final,
+                          const int32_t scores[256], uint32_t* out, uint32_t* ops, uint32_t ops_cap, void* stream,
+                          char* err, size_t errlen);
+
 /* Measurement helper: sustained int32 add/max throughput of the device in Tops/s (the
  * roofline denominator for the integer DP kernels). */
 int rmb_probe_int32_peak(int32_t device, double* tops, char* err, size_t errlen);

@@ -1196,3 +1196,218 @@ cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t
     return cudaGetLastError();
 }
 }  // namespace rmb
+
+// ---------------------------------------------------------------------------------------
+// Traceback without allocation (rmb_traceback_noalloc in include/rmb_gpu.h).
+//
+// For callers that may not call cudaMalloc: a library embedded in a process whose device memory
+// is owned by another allocator (a caching allocator that must see every byte, a stream-ordered
+// pool, a CUDA graph being captured), or code running where an allocation could fail or stall.
+// The per-thread scratch of the traceback (DP band, row table, trace bytes) comes from this
+// fixed array, which every GPU that loads the library holds until the process exits.
+// ---------------------------------------------------------------------------------------
+#include <mutex>
+
+#include "../../include/rmb_gpu.h"
+
+namespace rmb {
+
+constexpr uint64_t NOALLOC_SCRATCH_BYTES = 32ull << 20;  // 32 MiB
+constexpr uint32_t NOALLOC_MAX_THREADS = 256;
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+static __device__ unsigned int g_noalloc_overflow;
+
+struct NoallocSeqs {
+    const uint8_t* q;      // query, sentinel-wrapped
+    const uint8_t* qrc;    // its reverse complement, sentinel-wrapped
+    const uint8_t* s;      // subject with ambiguity codes restored, sentinel-wrapped
+    const uint8_t* src;    // its reverse complement, sentinel-wrapped
+    uint32_t qlen, slen;
+};
+
+// k_traceback for one (query, subject) pair: the same improve_seed + bidirectional traceback +
+// gap pruning, the scratch taken from `scratch` (the address of g_noalloc_scratch).
+__global__ void __launch_bounds__(128) k_traceback_noalloc(NoallocSeqs S, DevParams P, uint32_t n,
+                                                            const uint32_t* __restrict__ pre,
+                                                            uint32_t* __restrict__ out, uint32_t* __restrict__ ops_out,
+                                                            uint32_t ops_cap, uint8_t* __restrict__ scratch,
+                                                            uint64_t per_thread, uint64_t band_cells,
+                                                            uint32_t rows_cap, unsigned int* overflow) {
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P.matrix[i];
+    __syncthreads();
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint8_t* base = scratch + tid * per_thread;
+    TbScratch T;
+    T.band = (int2*)base;
+    T.rows = (uint2*)(base + band_cells * sizeof(int2));
+    T.rows_cap = rows_cap;
+    T.trace = base + band_cells * sizeof(int2) + (uint64_t)rows_cap * sizeof(uint2);
+    T.trace_cap = per_thread - band_cells * sizeof(int2) - (uint64_t)rows_cap * sizeof(uint2);
+    const uint32_t qa = S.qlen, sa = S.slen;
+    for (uint64_t t = tid; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        // record: strand, q_start, q_end, s_start, s_end, score, q_seed, s_seed
+        const uint32_t* r = pre + t * 8;
+        const bool plus = r[0] == 0;
+        uint32_t nq, ns;
+        improve_seed(S.q + 1, qa, (plus ? S.s : S.src) + 1, sa, r[6], r[7], r[1], r[2], r[3], r[4], !plus, nq, ns);
+        const uint32_t tq = plus ? nq : qa - 1 - nq, ts = plus ? ns : sa - 1 - ns;
+        const uint8_t* qa_ = (plus ? S.q : S.qrc) + 1;
+        const uint8_t* sa_ = S.s + 1;
+        uint32_t* ops = ops_out + t * (uint64_t)ops_cap;
+        uint32_t* o = out + t * 9;
+        uint64_t cells = 0, need = 0;
+        int32_t ls, rs = 0;
+        uint32_t la, lb, ra = 0, rb = 0, nl = 0, nr = 0;
+        int st = align_ex_tb<true>(qa_, sa_, tq + 1, ts + 1, P.gap_open, P.gap_extend, P.xdrop_gap_final, mat, T, ls,
+                                   la, lb, ops, ops_cap, nl, cells, need);
+        if (st == 0) {
+            const uint32_t rq = tq + 1, rsd = ts + 1;
+            const uint32_t rm = qa > rq ? qa - rq : 0, rn = sa > rsd ? sa - rsd : 0;
+            if (rm > 0 && rn > 0)
+                st = align_ex_tb<false>(qa_ + rq, sa_ + rsd, rm, rn, P.gap_open, P.gap_extend, P.xdrop_gap_final, mat,
+                                        T, rs, ra, rb, ops + nl, ops_cap - nl, nr, cells, need);
+        }
+        if (st != 0) {
+            atomicAdd(overflow, 1u);
+            o[0] = r[0];
+            o[1] = 2u;  // did not fit the scratch
+            for (int k = 2; k < 9; ++k) o[k] = 0;
+            continue;
+        }
+        for (uint32_t i = 0, j = nr ? nr - 1 : 0; i < j; ++i, --j) {
+            const uint32_t tmp = ops[nl + i];
+            ops[nl + i] = ops[nl + j];
+            ops[nl + j] = tmp;
+        }
+        uint32_t nops = nl;
+        for (uint32_t i = 0; i < nr; ++i) {
+            const uint32_t v = ops[nl + i];
+            if (nops > 0 && (ops[nops - 1] >> 30) == (v >> 30)) ops[nops - 1] += v & 0x3fffffffu;
+            else ops[nops++] = v;
+        }
+        int32_t total = ls + rs;
+        uint32_t q_start = tq + 1 - la, s_start = ts + 1 - lb, q_end = tq + 1 + ra, s_end = ts + 1 + rb;
+        uint32_t first = 0;
+        while (first < nops && (ops[first] >> 30) != 0) {
+            const uint32_t op = ops[first] >> 30, cnt = ops[first] & 0x3fffffffu;
+            total += P.gap_open + (int32_t)cnt * P.gap_extend;
+            if (op == 1) s_start += cnt;
+            else q_start += cnt;
+            ++first;
+        }
+        while (nops > first && (ops[nops - 1] >> 30) != 0) {
+            const uint32_t op = ops[nops - 1] >> 30, cnt = ops[nops - 1] & 0x3fffffffu;
+            total += P.gap_open + (int32_t)cnt * P.gap_extend;
+            if (op == 1) s_end -= cnt;
+            else q_end -= cnt;
+            --nops;
+        }
+        if (first) {
+            for (uint32_t i = first; i < nops; ++i) ops[i - first] = ops[i];
+            nops -= first;
+        }
+        o[0] = r[0];
+        if (total < 0) {
+            o[1] = 1u;
+            for (int k = 2; k < 8; ++k) o[k] = 0;
+            o[8] = 2166136261u;
+            continue;
+        }
+        uint32_t h = 2166136261u;
+        for (uint32_t i = 0; i < nops; ++i)
+            for (int b = 0; b < 4; ++b) h = (h ^ ((ops[i] >> (8 * b)) & 0xffu)) * 16777619u;
+        o[1] = 0u;
+        o[2] = (uint32_t)total;
+        o[3] = q_start;
+        o[4] = q_end;
+        o[5] = s_start;
+        o[6] = s_end;
+        o[7] = nops;
+        o[8] = h;
+    }
+}
+
+// Device address of the scratch array and the overflow counter, looked up once per device.
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[64];
+static void* g_noalloc_flag[64];
+
+static cudaError_t noalloc_setup(int device, uint8_t** scratch, unsigned int** flag) {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    if (!g_noalloc_addr[device]) {
+        void* a = nullptr;
+        void* f = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress(&f, g_noalloc_overflow);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[device] = a;
+        g_noalloc_flag[device] = f;
+    }
+    *scratch = (uint8_t*)g_noalloc_addr[device];
+    *flag = (unsigned int*)g_noalloc_flag[device];
+    return cudaSuccess;
+}
+
+}  // namespace rmb
+
+extern "C" int rmb_traceback_noalloc(int32_t device, const uint8_t* query, const uint8_t* query_rc, uint32_t qlen,
+                                     const uint8_t* subject, const uint8_t* subject_rc, uint32_t slen,
+                                     const uint32_t* prelims, uint32_t n, int32_t gap_open, int32_t gap_extend,
+                                     int32_t xdrop_gap_final, const int32_t scores[256], uint32_t* out,
+                                     uint32_t* ops, uint32_t ops_cap, void* stream, char* err, size_t errlen) {
+    using namespace rmb;
+    auto fail = [&](int code, const char* msg) {
+        if (err && errlen) {
+            size_t i = 0;
+            for (; msg[i] && i + 1 < errlen; ++i) err[i] = msg[i];
+            err[i] = 0;
+        }
+        return code;
+    };
+    if (!query || !query_rc || !subject || !subject_rc || !scores || (n && (!prelims || !out || !ops)))
+        return fail(RMB_EINVAL, "null argument");
+    if (ops_cap == 0) return fail(RMB_EINVAL, "ops_cap must be positive");
+    if (gap_open < 0 || gap_extend < 1 || xdrop_gap_final < 0) return fail(RMB_EINVAL, "gap costs or X-drop out of range");
+    // band (slen + 2 cells) + row table (qlen + 2 rows) + at least 64 KiB of trace per thread
+    const uint64_t band_cells = (uint64_t)slen + 2;
+    const uint32_t rows_cap = qlen + 2;
+    const uint64_t fixed = band_cells * sizeof(int2) + (uint64_t)rows_cap * sizeof(uint2);
+    const uint64_t min_thread = ((fixed + (64ull << 10)) + 255) & ~255ull;
+    if (min_thread > NOALLOC_SCRATCH_BYTES)
+        return fail(RMB_ELIMIT, "query and subject too long for the 32 MiB scratch of rmb_traceback_noalloc "
+                                "(8 bytes x (subject + 2) + 8 bytes x (query + 2) + 64 KiB must fit)");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+    uint8_t* scratch = nullptr;
+    unsigned int* flag = nullptr;
+    if ((e = noalloc_setup(device, &scratch, &flag)) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), st)) != cudaSuccess)
+        return fail(RMB_ECUDA, cudaGetErrorString(e));
+    if (n == 0) return RMB_OK;
+    uint32_t threads = (uint32_t)(NOALLOC_SCRATCH_BYTES / min_thread);
+    if (threads > NOALLOC_MAX_THREADS) threads = NOALLOC_MAX_THREADS;
+    if (threads > n) threads = n;
+    const uint32_t block = threads >= 128 ? 128 : threads;
+    const uint32_t grid = threads / block;
+    const uint64_t per_thread = (NOALLOC_SCRATCH_BYTES / ((uint64_t)grid * block)) & ~255ull;  // >= min_thread
+    DevParams P{};
+    P.gap_open = gap_open;
+    P.gap_extend = gap_extend;
+    P.xdrop_gap_final = xdrop_gap_final;
+    for (int i = 0; i < 256; ++i) P.matrix[i] = scores[i];
+    NoallocSeqs S{query, query_rc, subject, subject_rc, qlen, slen};
+    k_traceback_noalloc<<<grid, block, 0, st>>>(S, P, n, prelims, out, ops, ops_cap, scratch, per_thread, band_cells,
+                                                 rows_cap, flag);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+    unsigned int over = 0;
+    if ((e = cudaMemcpyAsync(&over, flag, sizeof over, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return fail(RMB_ECUDA, cudaGetErrorString(e));
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+    if (over) return fail(RMB_ELIMIT, "some alignments did not fit the fixed scratch (status 2 in their records)");
+    return RMB_OK;
+}
