@@ -561,8 +561,9 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
                 const uint32_t rows_cap = qmax + 2;
                 const uint64_t per_thread = ((band_cells * 8 + (uint64_t)rows_cap * 8 + trace_cap) + 255) & ~255ull;
                 const uint64_t budget = 8ull << 30;
-                uint32_t threads = (uint32_t)std::min<uint64_t>(todo.size(), std::max<uint64_t>(32, budget / per_thread));
-                threads = (threads + 127) / 128 * 128;
+                // one warp per scratch slot, blocks of 8 warps
+                uint32_t threads = (uint32_t)std::min<uint64_t>(todo.size(), std::max<uint64_t>(8, budget / per_thread));
+                threads = (threads + 7) / 8 * 8;
                 upload(C.tb_in, chunk_in, st);
                 C.tb_out.ensure(todo.size() * sizeof(TbOut));
                 C.tb_ops.ensure(todo.size() * (uint64_t)ops_cap * 4);

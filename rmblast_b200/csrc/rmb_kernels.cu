@@ -8,12 +8,12 @@
 //                 one thread per hit, computed for all hits ahead of the dedup.
 //   k_dedup       the order-dependent diagonal hash (search/diag_hash.rs) replayed per pair in
 //                 scan order on the precomputed extensions, one thread per pair.
-//   k_prelim      preliminary score-only X-drop DP (search/gapped.rs:124-418) of every ungapped
-//                 record, one thread per record, the DP band in a shared-memory ring;
+//   k_prelim_warp preliminary score-only X-drop DP (search/gapped.rs:124-418) of every ungapped
+//                 record, one warp per record, the DP band in a shared-memory ring;
 //                 k_prelim_wide reruns the records whose band outgrew the ring with the band in
-//                 global memory.
-//   k_traceback   improve_seed + traceback X-drop DP + trace walk (engine.rs:383-572,
-//                 engine.rs:2953-3039, search/gapped.rs:450-757), one thread per prelim HSP.
+//                 global memory (one thread per record).
+//   k_traceback_warp  improve_seed + traceback X-drop DP + trace walk (engine.rs:383-572,
+//                 engine.rs:2953-3039, search/gapped.rs:450-757), one warp per prelim HSP.
 //
 // All scores are int32; the arithmetic and the order of every comparison follow the cited
 // reference functions so results are bit-identical.
@@ -422,6 +422,152 @@ __device__ bool so_dp(const uint8_t* __restrict__ a, const uint8_t* __restrict__
     return true;
 }
 
+// ---------------------------------------------------------------------------------------
+// Warp-cooperative score-only X-drop DP: the same rows as so_dp, each row computed by the 32
+// lanes of a warp over consecutive band cells, in chunks of 32.
+//
+// Exactness.  In the reference's row loop (gapped.rs:222-296) the horizontal-gap value F
+// decays by ge at every unpruned cell and keeps its value at a pruned one, and the prune test
+// uses the running row-major best.  Let F* be the plain recurrence F*(b+1) =
+// max(F*(b) - ge, t(b) - goe) applied at every cell, t = max(diagonal, vertical gap).  By
+// induction over the row, at every cell either F = F* or both are below T = best - X (a pruned
+// cell has F <= cell < T, so its frozen F stays below T and so does F*), hence
+// max(t, F) and max(t, F*) agree on every cell that survives, on every prune decision, on the
+// stored cells, on the end-of-row F that drives the band extension, and on the running best
+// (pruned cells are below it).  F* is a max-plus prefix scan and the running best a prefix max,
+// both warp scans.
+// ---------------------------------------------------------------------------------------
+template <bool REVERSE, class Band>
+__device__ bool so_dp_warp(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint32_t m, uint32_t n,
+                           int32_t go, int32_t ge, int32_t x_dropoff, const int32_t* __restrict__ mat, Band band,
+                           DpResult& res, uint64_t& cells) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    res = DpResult{0, 0, 0};
+    if (m == 0 || n == 0) return true;
+    const int32_t goe = go + ge;
+    const int32_t xdrop = x_dropoff > goe ? x_dropoff : goe;
+    // first row: cells 0..J, J = min(n, (xdrop - goe) / ge + 1)
+    const uint32_t J = min(n, (uint32_t)((xdrop - goe) / ge) + 1u);
+    if (!band.fits(J, 0)) return false;
+    for (uint32_t j = lane; j <= J; j += 32) {
+        if (j == 0) band.set(0, make_int2(0, -goe));
+        else {
+            const int32_t sc = -goe - (int32_t)(j - 1) * ge;
+            band.set(j, make_int2(sc, sc - goe));
+        }
+    }
+    uint32_t b_size = J + 1, first_b = 0, best_a = 0, best_b = 0;
+    int32_t best = 0;
+    for (uint32_t ai = 0; ai < m; ++ai) {
+        __syncwarp();
+        const uint32_t ap = REVERSE ? m - 1 - ai : ai;
+        const int32_t* row = mat + ((a[ap] & 15) << 4);
+        cells += b_size - first_b;
+        int32_t carry_h = MININT;   // old H of the cell left of the chunk
+        int32_t carry_g = MININT;   // F* entering the chunk
+        int32_t carry_best = best;  // running best entering the chunk
+        int32_t row_max = MININT;
+        uint32_t row_arg = 0, last_b = first_b, new_first = first_b;
+        bool leading = true;
+        for (uint32_t c0 = first_b; c0 < b_size; c0 += 32) {
+            const uint32_t bi = c0 + lane;
+            const bool valid = bi < b_size;
+            const int2 cur = valid ? band.get(bi) : make_int2(MININT, MININT);
+            int32_t hl = __shfl_up_sync(FULL, cur.x, 1);
+            if (lane == 0) hl = carry_h;
+            int32_t d = MININT;
+            if (valid && bi != first_b) d = hl + row[b[REVERSE ? n - bi : bi - 1]];
+            const int32_t t = d > cur.y ? d : cur.y;
+            // G(b) = max(G(b-1) - ge, t(b) - goe); F*(b) = G(b-1)
+            int32_t g = valid ? t - goe : MININT;
+#pragma unroll
+            for (uint32_t k = 1; k < 32; k <<= 1) {
+                const int32_t o = __shfl_up_sync(FULL, g, k);
+                if (lane >= k) {
+                    const int32_t v = o - (int32_t)k * ge;
+                    if (v > g) g = v;
+                }
+            }
+            {
+                const int32_t v = carry_g - (int32_t)(lane + 1) * ge;
+                if (v > g) g = v;
+            }
+            int32_t f = __shfl_up_sync(FULL, g, 1);
+            if (lane == 0) f = carry_g;
+            const int32_t cell = valid ? (t > f ? t : f) : MININT;
+            // running best before this cell
+            int32_t mx = cell;
+#pragma unroll
+            for (uint32_t k = 1; k < 32; k <<= 1) {
+                const int32_t o = __shfl_up_sync(FULL, mx, k);
+                if (lane >= k && o > mx) mx = o;
+            }
+            int32_t before = __shfl_up_sync(FULL, mx, 1);
+            if (lane == 0) before = carry_best;
+            if (carry_best > before) before = carry_best;
+            const bool pruned = valid && (before - cell > xdrop);
+            const bool alive = valid && !pruned;
+            const unsigned alive_mask = __ballot_sync(FULL, alive);
+            const unsigned valid_mask = __ballot_sync(FULL, valid);
+            uint32_t lead_end = 0;  // lanes below this are in the leading pruned run
+            if (leading) {
+                if (alive_mask) {
+                    lead_end = __ffs(alive_mask) - 1;
+                    new_first += lead_end;
+                    leading = false;
+                } else {
+                    lead_end = 32;
+                    new_first += __popc(valid_mask);
+                }
+            }
+            if (alive) {
+                const int32_t col_ext = cur.y - ge, open = cell - goe;
+                band.set(bi, make_int2(cell, col_ext > open ? col_ext : open));
+            } else if (pruned && lane >= lead_end) {
+                band.set_best(bi, MININT);
+            }
+            if (alive_mask) last_b = c0 + 31 - __clz(alive_mask);
+            const int32_t cmax = __shfl_sync(FULL, mx, 31);  // max over the chunk (invalid lanes are MININT)
+            if (cmax > row_max) {
+                row_max = cmax;
+                row_arg = c0 + __ffs(__ballot_sync(FULL, valid && cell == cmax)) - 1;
+            }
+            if (cmax > carry_best) carry_best = cmax;
+            const uint32_t last_lane = 31 - __clz(valid_mask);
+            carry_g = __shfl_sync(FULL, g, last_lane);
+            carry_h = __shfl_sync(FULL, cur.x, 31);
+        }
+        first_b = new_first;
+        if (row_max > best) {
+            best = row_max;
+            best_b = row_arg;
+            best_a = ai + 1;
+        }
+        if (first_b >= b_size) break;
+        int32_t gap_row = carry_g;
+        if (last_b + 1 < b_size) {
+            b_size = last_b + 1;
+        } else if (gap_row >= best - xdrop && b_size <= n) {
+            const uint32_t k = min((uint32_t)((gap_row - (best - xdrop)) / ge) + 1u, n + 1 - b_size);
+            if (!band.fits(b_size + k - 1, first_b)) return false;
+            __syncwarp();
+            for (uint32_t i = lane; i < k; i += 32) {
+                const int32_t v = gap_row - (int32_t)i * ge;
+                band.set(b_size + i, make_int2(v, v - goe));
+            }
+            b_size += k;
+        }
+        if (b_size <= n) {
+            if (!band.fits(b_size, first_b)) return false;
+            if (lane == 0) band.set(b_size, make_int2(MININT, MININT));
+            ++b_size;
+        }
+    }
+    res = DpResult{best, best_a, best_b};
+    return true;
+}
+
 // engine.rs:1850-1895 prelim_pivot: (pivot_q, pivot_s, tb_q, tb_s)
 __device__ __forceinline__ void prelim_pivot(bool plus, uint32_t q_seed, uint32_t s_seed, uint32_t s_start,
                                              uint32_t s_end, uint32_t qa, uint32_t sa, uint32_t lw, uint32_t o[4]) {
@@ -507,6 +653,66 @@ __global__ void __launch_bounds__(128) k_prelim(DevLib L, DevQueries Q, const De
     }
     for (int o = 16; o; o >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o);
     if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// One ungapped record per warp; each warp's band lives in a RING_W-cell shared-memory ring.
+template <int RING_W>
+__global__ void __launch_bounds__(256) k_prelim_warp(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                      uint64_t n, const uint32_t* __restrict__ idx,
+                                                      const SeedHit* __restrict__ hits,
+                                                      const uint32_t* __restrict__ hit_pair,
+                                                      const UngBox* __restrict__ ub, PrelimOut* __restrict__ out,
+                                                      uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide,
+                                                      unsigned long long* __restrict__ cells_total) {
+    __shared__ int2 ring[(256 / 32) * RING_W];
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    RingBand band{ring + wib * RING_W, RING_W - 1};
+    uint64_t cells = 0;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t t = warp; t < n; t += nwarps) {
+        const uint32_t i = idx[t];
+        const uint32_t pair = hit_pair[i];
+        const SeedHit h = hits[i];
+        const UngBox u = ub[i];
+        const uint32_t qi = pair / L.n, si = pair % L.n;
+        const uint32_t qa = Q.len[qi], sa = L.len[si];
+        const bool plus = !(h.qs >> 31);
+        uint32_t piv[4];
+        prelim_pivot(plus, h.qs & 0x7fffffffu, h.s, u.s_start, u.s_end, qa, sa, (uint32_t)Q.lw[qi], piv);
+        const int32_t xd = P->xdrop_gap < u.score ? P->xdrop_gap : u.score;
+        const uint8_t* qseq = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
+        const uint8_t* sseq = L.plus + L.plus_off[si] + 1;
+        const uint32_t qp = piv[0], sp = piv[1];
+        DpResult l, r{0, 0, 0};
+        uint64_t c = 0;
+        bool ok = so_dp_warp<true>(sseq, qseq, sp, qp, P->gap_open, P->gap_extend, xd, mat, band, l, c);
+        const uint32_t rm = sa > sp ? sa - sp : 0, rn = qa > qp ? qa - qp : 0;
+        if (ok && rm > 0 && rn > 0)
+            ok = so_dp_warp<false>(sseq + sp, qseq + qp, rm, rn, P->gap_open, P->gap_extend, xd, mat, band, r, c);
+        if (!ok) {
+            if (lane == 0) wide[atomicAdd(n_wide, 1u)] = (uint32_t)t;
+            continue;
+        }
+        cells += c;
+        if (lane == 0) {
+            PrelimOut o{INT32_MIN, 0, 0, 0, 0, 0, 0};
+            const int32_t total = l.score + r.score;
+            if (total >= 0) {
+                uint32_t q0 = qp - l.b_len, s0 = sp - l.a_len, q1 = qp + r.b_len, s1 = sp + r.a_len;
+                if (!plus) {
+                    const uint32_t t0 = qa - q1, t1 = qa - q0, t2 = sa - s1, t3 = sa - s0;
+                    q0 = t0; q1 = t1; s0 = t2; s1 = t3;
+                }
+                if (total >= P->gapped_cutoff) o = PrelimOut{total, q0, q1, s0, s1, piv[2], piv[3]};
+            }
+            out[t] = o;
+        }
+    }
+    if (lane == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
 }
 
 // The records whose band outgrew the ring, with the band at absolute indices in global memory
@@ -797,33 +1003,242 @@ __device__ int align_ex_tb(const uint8_t* __restrict__ a, const uint8_t* __restr
     return 0;
 }
 
-__global__ void __launch_bounds__(128) k_traceback(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
-                                                    uint32_t n, const TbIn* __restrict__ in, TbOut* __restrict__ out,
-                                                    uint32_t* __restrict__ ops_out, uint32_t ops_cap,
-                                                    uint8_t* __restrict__ scratch, uint64_t scratch_per_thread,
-                                                    uint64_t band_cells, uint32_t rows_cap,
-                                                    unsigned long long* __restrict__ cells_total) {
+// Warp-cooperative align_ex (gapped.rs:450-689) + traceback_flat (692-757): the rows of
+// so_dp_warp with the per-cell op byte (SUB / GAP_B / GAP_A with the extend flags) written by
+// the lanes in row order, then the walk by lane 0.  With F* in place of the reference's F the
+// op bytes can differ only on cells below the X-drop threshold, and no traceback path visits
+// such a cell: a cell on the path holds a value at or above it (cells below are pruned), and a
+// horizontal-gap step into a cell needs F >= threshold there, where F = F*.
+// Returns 0 ok, 2 scratch overflow, 3 walk did not reach the origin.  ops_rev is written by
+// lane 0 as in align_ex_tb (last op first).
+template <bool REVERSE>
+__device__ int align_ex_tb_warp(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint32_t m,
+                                uint32_t n, int32_t go, int32_t ge, int32_t x_dropoff, const int32_t* __restrict__ mat,
+                                TbScratch& S, int32_t& score_out, uint32_t& a_len, uint32_t& b_len, uint32_t* ops_rev,
+                                uint32_t ops_cap, uint32_t& n_ops, uint64_t& cells, uint64_t& need) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    score_out = 0;
+    a_len = b_len = 0;
+    n_ops = 0;
+    if (m == 0 || n == 0) return 0;
+    const int32_t goe = go + ge;
+    const int32_t xdrop = x_dropoff > goe ? x_dropoff : goe;
+    const uint32_t J = min(n, (uint32_t)((xdrop - goe) / ge) + 1u);
+    if (J + 1 > S.trace_cap || S.rows_cap < 1) { need = S.trace_cap * 2 + 4096; return 2; }
+    for (uint32_t j = lane; j <= J; j += 32) {
+        if (j == 0) {
+            S.band[0] = make_int2(0, -goe);
+            S.trace[0] = T_GAP_B;
+        } else {
+            const int32_t sc = -goe - (int32_t)(j - 1) * ge;
+            S.band[j] = make_int2(sc, sc - goe);
+            S.trace[j] = T_GAP_A;
+        }
+    }
+    if (lane == 0) S.rows[0] = make_uint2(0, 0);
+    uint64_t flen = J + 1;
+    uint32_t nrows = 1;
+    uint32_t b_size = J + 1, first_b = 0, best_a = 0, best_b = 0;
+    int32_t best = 0;
+    for (uint32_t ai = 0; ai < m; ++ai) {
+        __syncwarp();
+        const uint32_t ap = REVERSE ? m - 1 - ai : ai;
+        const int32_t* row = mat + ((a[ap] & 15) << 4);
+        const uint32_t first0 = first_b;
+        if (nrows >= S.rows_cap || flen + (b_size - first0) > S.trace_cap) { need = S.trace_cap * 2 + 4096; return 2; }
+        if (lane == 0) S.rows[nrows] = make_uint2((uint32_t)flen, first0);
+        ++nrows;
+        cells += b_size - first_b;
+        int32_t carry_h = MININT, carry_g = MININT, carry_best = best, row_max = MININT;
+        uint32_t row_arg = 0, last_b = first_b, new_first = first_b;
+        bool leading = true;
+        for (uint32_t c0 = first_b; c0 < b_size; c0 += 32) {
+            const uint32_t bi = c0 + lane;
+            const bool valid = bi < b_size;
+            const int2 cur = valid ? S.band[bi] : make_int2(MININT, MININT);
+            int32_t hl = __shfl_up_sync(FULL, cur.x, 1);
+            if (lane == 0) hl = carry_h;
+            int32_t d = MININT;
+            if (valid && bi != first_b) d = hl + row[b[REVERSE ? n - bi : bi - 1] & 15];
+            int32_t g = valid ? (d > cur.y ? d : cur.y) - goe : MININT;
+#pragma unroll
+            for (uint32_t k = 1; k < 32; k <<= 1) {
+                const int32_t o = __shfl_up_sync(FULL, g, k);
+                if (lane >= k) {
+                    const int32_t v = o - (int32_t)k * ge;
+                    if (v > g) g = v;
+                }
+            }
+            {
+                const int32_t v = carry_g - (int32_t)(lane + 1) * ge;
+                if (v > g) g = v;
+            }
+            int32_t f = __shfl_up_sync(FULL, g, 1);
+            if (lane == 0) f = carry_g;
+            // op choice with the reference's tie order: diagonal, then vertical, then horizontal
+            uint8_t op = T_SUB;
+            int32_t cell = d;
+            if (cur.y > cell) { cell = cur.y; op = T_GAP_B; }
+            if (f > cell) { cell = f; op = T_GAP_A; }
+            if (!valid) cell = MININT;
+            int32_t mx = cell;
+#pragma unroll
+            for (uint32_t k = 1; k < 32; k <<= 1) {
+                const int32_t o = __shfl_up_sync(FULL, mx, k);
+                if (lane >= k && o > mx) mx = o;
+            }
+            int32_t before = __shfl_up_sync(FULL, mx, 1);
+            if (lane == 0) before = carry_best;
+            if (carry_best > before) before = carry_best;
+            const bool pruned = valid && (before - cell > xdrop);
+            const bool alive = valid && !pruned;
+            const unsigned alive_mask = __ballot_sync(FULL, alive);
+            const unsigned valid_mask = __ballot_sync(FULL, valid);
+            uint32_t lead_end = 0;
+            if (leading) {
+                if (alive_mask) {
+                    lead_end = __ffs(alive_mask) - 1;
+                    new_first += lead_end;
+                    leading = false;
+                } else {
+                    lead_end = 32;
+                    new_first += __popc(valid_mask);
+                }
+            }
+            if (alive) {
+                const int32_t gcol = cur.y - ge, open = cell - goe;
+                int32_t bg;
+                if (gcol < open) bg = open;
+                else { bg = gcol; op |= T_EXT_B; }
+                S.band[bi] = make_int2(cell, bg);
+                if (!(f - ge < open)) op |= T_EXT_A;
+            } else if (pruned && lane >= lead_end) {
+                S.band[bi].x = MININT;
+            }
+            if (valid) S.trace[flen + (bi - first0)] = op;
+            if (alive_mask) last_b = c0 + 31 - __clz(alive_mask);
+            const int32_t cmax = __shfl_sync(FULL, mx, 31);
+            if (cmax > row_max) {
+                row_max = cmax;
+                row_arg = c0 + __ffs(__ballot_sync(FULL, valid && cell == cmax)) - 1;
+            }
+            if (cmax > carry_best) carry_best = cmax;
+            carry_g = __shfl_sync(FULL, g, 31 - __clz(valid_mask));
+            carry_h = __shfl_sync(FULL, cur.x, 31);
+        }
+        flen += b_size - first0;
+        first_b = new_first;
+        if (row_max > best) {
+            best = row_max;
+            best_b = row_arg;
+            best_a = ai + 1;
+        }
+        if (first_b >= b_size) break;
+        const int32_t gap_row = carry_g;
+        if (last_b + 1 < b_size) {
+            b_size = last_b + 1;
+        } else if (gap_row >= best - xdrop && b_size <= n) {
+            const uint32_t k = min((uint32_t)((gap_row - (best - xdrop)) / ge) + 1u, n + 1 - b_size);
+            if (flen + k > S.trace_cap) { need = S.trace_cap * 2 + 4096; return 2; }
+            __syncwarp();
+            for (uint32_t i = lane; i < k; i += 32) {
+                const int32_t v = gap_row - (int32_t)i * ge;
+                S.band[b_size + i] = make_int2(v, v - goe);
+                S.trace[flen + i] = T_GAP_A;
+            }
+            flen += k;
+            b_size += k;
+        }
+        if (b_size <= n) {
+            if (lane == 0) S.band[b_size] = make_int2(MININT, MININT);
+            ++b_size;
+        }
+    }
+    __syncwarp();
+    score_out = best;
+    a_len = best_a;
+    b_len = best_b;
+    if (best_a == 0 && best_b == 0) return 0;
+    int st = 0;
+    if (lane == 0) {
+        uint32_t aa = best_a, bq = best_b;
+        uint8_t prev = T_SUB;
+        uint32_t cur_op = 0xffffffffu, cur_n = 0, nops = 0;
+        const uint64_t steps = (uint64_t)best_a + best_b;
+        for (uint64_t s2 = 0; s2 < steps && st == 0; ++s2) {
+            const uint2 ri = S.rows[aa];
+            const uint64_t row_end = aa + 1 < nrows ? S.rows[aa + 1].x : flen;
+            uint8_t raw = T_GAP_A;
+            if (bq >= ri.y) {
+                const uint64_t k = (uint64_t)ri.x + (bq - ri.y);
+                raw = k < row_end ? S.trace[k] : T_GAP_A;
+            }
+            uint8_t op;
+            if ((prev & T_MASK) == T_GAP_A) op = (raw & T_EXT_A) ? T_GAP_A : (raw & T_MASK);
+            else if ((prev & T_MASK) == T_GAP_B) op = (raw & T_EXT_B) ? T_GAP_B : (raw & T_MASK);
+            else op = raw & T_MASK;
+            prev = op;
+            uint32_t eop;
+            if (op == T_GAP_A) { eop = 1; bq = bq ? bq - 1 : 0; }
+            else if (op == T_GAP_B) { eop = 2; aa = aa ? aa - 1 : 0; }
+            else { eop = 0; aa = aa ? aa - 1 : 0; bq = bq ? bq - 1 : 0; }
+            if (eop == cur_op) ++cur_n;
+            else {
+                if (cur_n) {
+                    if (nops >= ops_cap) { st = 2; break; }
+                    ops_rev[nops++] = (cur_op << 30) | cur_n;
+                }
+                cur_op = eop;
+                cur_n = 1;
+            }
+            if (aa == 0 && bq == 0) break;
+        }
+        if (st == 0 && cur_n) {
+            if (nops >= ops_cap) st = 2;
+            else ops_rev[nops++] = (cur_op << 30) | cur_n;
+        }
+        if (st == 0 && (aa != 0 || bq != 0)) st = 3;
+        n_ops = nops;
+    }
+    st = __shfl_sync(FULL, st, 0);
+    n_ops = __shfl_sync(FULL, n_ops, 0);
+    if (st == 2) need = 0;
+    return st;
+}
+
+// One prelim per warp: improve_seed, the two warp DPs, script merge and gap pruning.
+__global__ void __launch_bounds__(256) k_traceback_warp(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                         uint32_t n, const TbIn* __restrict__ in,
+                                                         TbOut* __restrict__ out, uint32_t* __restrict__ ops_out,
+                                                         uint32_t ops_cap, uint8_t* __restrict__ scratch,
+                                                         uint64_t per_warp, uint64_t band_cells, uint32_t rows_cap,
+                                                         unsigned long long* __restrict__ cells_total) {
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
     __syncthreads();
-    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint8_t* base = scratch + tid * scratch_per_thread;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    uint8_t* base = scratch + warp * per_warp;
     TbScratch S;
     S.band = (int2*)base;
     S.rows = (uint2*)(base + band_cells * sizeof(int2));
     S.rows_cap = rows_cap;
     S.trace = base + band_cells * sizeof(int2) + (uint64_t)rows_cap * sizeof(uint2);
-    S.trace_cap = scratch_per_thread - band_cells * sizeof(int2) - (uint64_t)rows_cap * sizeof(uint2);
+    S.trace_cap = per_warp - band_cells * sizeof(int2) - (uint64_t)rows_cap * sizeof(uint2);
     uint64_t cells = 0;
-    for (uint64_t t = tid; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t t = warp; t < n; t += nwarps) {
         const TbIn h = in[t];
         const uint32_t qi = h.pair / L.n, si = h.pair % L.n;
         const uint32_t qa = Q.len[qi], sa = L.len[si];
         const bool plus = h.strand == 0;
         const uint8_t* qfwd = Q.q + Q.off[qi] + 1;
         const uint8_t* sfs = (plus ? L.align : L.align_rc) + L.plus_off[si] + 1;
-        uint32_t nq, ns;
-        improve_seed(qfwd, qa, sfs, sa, h.q_seed, h.s_seed, h.q_start, h.q_end, h.s_start, h.s_end, !plus, nq, ns);
+        uint32_t nq = 0, ns = 0;
+        if (lane == 0) improve_seed(qfwd, qa, sfs, sa, h.q_seed, h.s_seed, h.q_start, h.q_end, h.s_start, h.s_end, !plus, nq, ns);
+        nq = __shfl_sync(0xffffffffu, nq, 0);
+        ns = __shfl_sync(0xffffffffu, ns, 0);
         const uint32_t tq = plus ? nq : qa - 1 - nq, ts = plus ? ns : sa - 1 - ns;
         const uint8_t* qa_ = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
         const uint8_t* sa_ = L.align + L.plus_off[si] + 1;
@@ -832,25 +1247,25 @@ __global__ void __launch_bounds__(128) k_traceback(DevLib L, DevQueries Q, const
         uint64_t need = 0;
         int32_t ls, rs = 0;
         uint32_t la, lb, ra = 0, rb = 0, nl = 0, nr = 0;
-        int st = align_ex_tb<true>(qa_, sa_, tq + 1, ts + 1, P->gap_open, P->gap_extend, P->xdrop_gap_final, mat, S, ls, la,
-                                   lb, ops, ops_cap, nl, cells, need);
-        // left script is written last-op-first of the reversed DP, i.e. already in forward order
+        int st = align_ex_tb_warp<true>(qa_, sa_, tq + 1, ts + 1, P->gap_open, P->gap_extend, P->xdrop_gap_final, mat,
+                                        S, ls, la, lb, ops, ops_cap, nl, cells, need);
         if (st == 0) {
             const uint32_t rq = tq + 1, rsd = ts + 1;
             const uint32_t rm = qa > rq ? qa - rq : 0, rn = sa > rsd ? sa - rsd : 0;
             if (rm > 0 && rn > 0)
-                st = align_ex_tb<false>(qa_ + rq, sa_ + rsd, rm, rn, P->gap_open, P->gap_extend, P->xdrop_gap_final,
-                                        mat, S, rs, ra, rb, ops + nl, ops_cap - nl, nr, cells, need);
+                st = align_ex_tb_warp<false>(qa_ + rq, sa_ + rsd, rm, rn, P->gap_open, P->gap_extend,
+                                             P->xdrop_gap_final, mat, S, rs, ra, rb, ops + nl, ops_cap - nl, nr, cells,
+                                             need);
         }
+        if (lane != 0) continue;
         if (st != 0) {
             o.status = st == 3 ? 3 : 2;
             o.need = (uint32_t)min(need, (uint64_t)0xffffffffu);
             out[t] = o;
             continue;
         }
-        // right script: reverse it in place to forward order, then merge at the junction
         for (uint32_t i = 0, j = nr ? nr - 1 : 0; i < j; ++i, --j) {
-            uint32_t tmp = ops[nl + i];
+            const uint32_t tmp = ops[nl + i];
             ops[nl + i] = ops[nl + j];
             ops[nl + j] = tmp;
         }
@@ -861,8 +1276,7 @@ __global__ void __launch_bounds__(128) k_traceback(DevLib L, DevQueries Q, const
             else ops[nops++] = v;
         }
         int32_t total = ls + rs;
-        uint32_t q_start = tq + 1 - la, s_start = ts + 1 - lb;
-        uint32_t q_end = tq + 1 + ra, s_end = ts + 1 + rb;
+        uint32_t q_start = tq + 1 - la, s_start = ts + 1 - lb, q_end = tq + 1 + ra, s_end = ts + 1 + rb;
         uint32_t first = 0;
         while (first < nops && (ops[first] >> 30) != 0) {
             const uint32_t op = ops[first] >> 30, cnt = ops[first] & 0x3fffffffu;
@@ -887,7 +1301,6 @@ __global__ void __launch_bounds__(128) k_traceback(DevLib L, DevQueries Q, const
             out[t] = o;
             continue;
         }
-        o.status = 0;
         o.score = total;
         o.q0 = q_start;
         o.q1 = q_end;
@@ -896,8 +1309,7 @@ __global__ void __launch_bounds__(128) k_traceback(DevLib L, DevQueries Q, const
         o.n_ops = nops;
         out[t] = o;
     }
-    for (int o2 = 16; o2; o2 >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o2);
-    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
+    if (lane == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -944,21 +1356,17 @@ cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32
 
 size_t diag_cell_bytes() { return sizeof(DiagCell); }
 
-constexpr int PRELIM_W = 64;
+constexpr int PRELIM_RING = 256;
 
 cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n, const uint32_t* idx,
                           const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub, PrelimOut* out,
                           uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st) {
     if (!n) return cudaSuccess;
-    const int block = 128;
-    const size_t smem = (size_t)block * PRELIM_W * sizeof(int2);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_prelim<PRELIM_W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
-    k_prelim<PRELIM_W><<<grid_for(n, block, 3, sms), block, smem, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide,
-                                                                      n_wide, cells);
+    const int block = 256;
+    const uint64_t blocks_wanted = (n + 7) / 8;
+    const uint64_t cap = (uint64_t)sms * 8;
+    const int grid = (int)(blocks_wanted < cap ? blocks_wanted : cap);
+    k_prelim_warp<PRELIM_RING><<<grid, block, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide, n_wide, cells);
     return cudaGetLastError();
 }
 
@@ -978,11 +1386,13 @@ cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevPara
                              TbOut* out, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch, uint64_t per_thread,
                              uint64_t band_cells, uint32_t rows_cap, uint32_t threads, unsigned long long* cells,
                              cudaStream_t st) {
+    // `threads` scratch slots of `per_thread` bytes: one warp per slot
     if (!n) return cudaSuccess;
-    const int block = 128;
-    const int grid = (int)((threads + block - 1) / block);
-    k_traceback<<<grid, block, 0, st>>>(L, Q, P, n, in, out, ops, ops_cap, scratch, per_thread, band_cells, rows_cap,
-                                        cells);
+    const int block = 256;
+    const uint32_t warps = threads;
+    const int grid = (int)((warps * 32 + block - 1) / block);
+    k_traceback_warp<<<grid, block, 0, st>>>(L, Q, P, n, in, out, ops, ops_cap, scratch, per_thread, band_cells,
+                                             rows_cap, cells);
     return cudaGetLastError();
 }
 
