@@ -437,6 +437,21 @@ __device__ bool so_dp(const uint8_t* __restrict__ a, const uint8_t* __restrict__
 // (pruned cells are below it).  F* is a max-plus prefix scan and the running best a prefix max,
 // both warp scans.
 // ---------------------------------------------------------------------------------------
+// Number of band-extension cells of the row loops (gapped.rs:313-327): the i = 0, 1, ... with
+// gap_row - i ge >= thr, at most `room`; gap_row >= thr.  Counted by ballot, 32 at a time.
+__device__ __forceinline__ uint32_t ext_count(int32_t gap_row, int32_t thr, int32_t ge, uint32_t room) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t k = 0;
+    for (;;) {
+        const uint32_t i = k + lane;
+        const bool ok = i < room && (int64_t)gap_row - (int64_t)i * ge >= (int64_t)thr;
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        const uint32_t c = __popc(m);
+        k += c;
+        if (c < 32) return k;
+    }
+}
+
 template <bool REVERSE, class Band>
 __device__ bool so_dp_warp(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint32_t m, uint32_t n,
                            int32_t go, int32_t ge, int32_t x_dropoff, const int32_t* __restrict__ mat, Band band,
@@ -478,34 +493,36 @@ __device__ bool so_dp_warp(const uint8_t* __restrict__ a, const uint8_t* __restr
             if (lane == 0) hl = carry_h;
             int32_t d = MININT;
             if (valid && bi != first_b) d = hl + row[b[REVERSE ? n - bi : bi - 1]];
-            const int32_t t = d > cur.y ? d : cur.y;
-            // G(b) = max(G(b-1) - ge, t(b) - goe); F*(b) = G(b-1)
-            int32_t g = valid ? t - goe : MININT;
+            const int32_t t = valid ? (d > cur.y ? d : cur.y) : MININT;
+            // Chunk maximum of t = chunk maximum of the cells (F* never exceeds an earlier t).
+            const int32_t tmax = __reduce_max_sync(FULL, t);
+            const int32_t thr = carry_best - xdrop;  // threshold at the chunk start (only rises)
+            int32_t g, f;
+            if (carry_g >= thr || tmax - goe >= thr) {
+                // G(b) = max(G(b-1) - ge, t(b) - goe); F*(b) = G(b-1)
+                // shfl_up hands a lane below the offset its own value, and max(g - k ge, g) = g,
+                // so every lane takes the step
+                g = valid ? t - goe : MININT;
 #pragma unroll
-            for (uint32_t k = 1; k < 32; k <<= 1) {
-                const int32_t o = __shfl_up_sync(FULL, g, k);
-                if (lane >= k) {
-                    const int32_t v = o - (int32_t)k * ge;
-                    if (v > g) g = v;
-                }
+                for (uint32_t k = 1; k < 32; k <<= 1) g = __viaddmax_s32(__shfl_up_sync(FULL, g, k), -(int32_t)k * ge, g);
+                g = __viaddmax_s32(carry_g, -(int32_t)(lane + 1) * ge, g);
+                f = __shfl_up_sync(FULL, g, 1);
+                if (lane == 0) f = carry_g;
+            } else {
+                // every F* of the chunk is below the threshold: it decides nothing, and any value
+                // below the threshold carried on leaves the later cells' decisions unchanged
+                f = MININT;
+                g = carry_g > tmax - goe ? carry_g : tmax - goe;
             }
-            {
-                const int32_t v = carry_g - (int32_t)(lane + 1) * ge;
-                if (v > g) g = v;
-            }
-            int32_t f = __shfl_up_sync(FULL, g, 1);
-            if (lane == 0) f = carry_g;
-            const int32_t cell = valid ? (t > f ? t : f) : MININT;
-            // running best before this cell
-            int32_t mx = cell;
+            const int32_t cell = valid ? max(t, f) : MININT;
+            // running best before this cell: max(carry_best, earlier t of the chunk)
+            int32_t before = carry_best, mx = t;
+            if (tmax > carry_best) {
 #pragma unroll
-            for (uint32_t k = 1; k < 32; k <<= 1) {
-                const int32_t o = __shfl_up_sync(FULL, mx, k);
-                if (lane >= k && o > mx) mx = o;
+                for (uint32_t k = 1; k < 32; k <<= 1) mx = max(mx, __shfl_up_sync(FULL, mx, k));
+                const int32_t ex = __shfl_up_sync(FULL, mx, 1);
+                if (lane != 0) before = max(before, ex);
             }
-            int32_t before = __shfl_up_sync(FULL, mx, 1);
-            if (lane == 0) before = carry_best;
-            if (carry_best > before) before = carry_best;
             const bool pruned = valid && (before - cell > xdrop);
             const bool alive = valid && !pruned;
             const unsigned alive_mask = __ballot_sync(FULL, alive);
@@ -521,19 +538,15 @@ __device__ bool so_dp_warp(const uint8_t* __restrict__ a, const uint8_t* __restr
                     new_first += __popc(valid_mask);
                 }
             }
-            if (alive) {
-                const int32_t col_ext = cur.y - ge, open = cell - goe;
-                band.set(bi, make_int2(cell, col_ext > open ? col_ext : open));
-            } else if (pruned && lane >= lead_end) {
+            if (alive) band.set(bi, make_int2(cell, __viaddmax_s32(cur.y, -ge, cell - goe))); else if (pruned && lane >= lead_end) {
                 band.set_best(bi, MININT);
             }
             if (alive_mask) last_b = c0 + 31 - __clz(alive_mask);
-            const int32_t cmax = __shfl_sync(FULL, mx, 31);  // max over the chunk (invalid lanes are MININT)
-            if (cmax > row_max) {
-                row_max = cmax;
-                row_arg = c0 + __ffs(__ballot_sync(FULL, valid && cell == cmax)) - 1;
+            if (tmax > row_max) {
+                row_max = tmax;
+                row_arg = c0 + __ffs(__ballot_sync(FULL, valid && t == tmax)) - 1;
             }
-            if (cmax > carry_best) carry_best = cmax;
+            if (tmax > carry_best) carry_best = tmax;
             const uint32_t last_lane = 31 - __clz(valid_mask);
             carry_g = __shfl_sync(FULL, g, last_lane);
             carry_h = __shfl_sync(FULL, cur.x, 31);
@@ -549,7 +562,7 @@ __device__ bool so_dp_warp(const uint8_t* __restrict__ a, const uint8_t* __restr
         if (last_b + 1 < b_size) {
             b_size = last_b + 1;
         } else if (gap_row >= best - xdrop && b_size <= n) {
-            const uint32_t k = min((uint32_t)((gap_row - (best - xdrop)) / ge) + 1u, n + 1 - b_size);
+            const uint32_t k = ext_count(gap_row, best - xdrop, ge, n + 1 - b_size);
             if (!band.fits(b_size + k - 1, first_b)) return false;
             __syncwarp();
             for (uint32_t i = lane; i < k; i += 32) {
@@ -1061,36 +1074,38 @@ __device__ int align_ex_tb_warp(const uint8_t* __restrict__ a, const uint8_t* __
             if (lane == 0) hl = carry_h;
             int32_t d = MININT;
             if (valid && bi != first_b) d = hl + row[b[REVERSE ? n - bi : bi - 1] & 15];
-            int32_t g = valid ? (d > cur.y ? d : cur.y) - goe : MININT;
+            const int32_t t = valid ? (d > cur.y ? d : cur.y) : MININT;
+            const int32_t tmax = __reduce_max_sync(FULL, t);
+            const int32_t thr = carry_best - xdrop;
+            int32_t g, f;
+            if (carry_g >= thr || tmax - goe >= thr) {
+                // shfl_up hands a lane below the offset its own value, and max(g - k ge, g) = g,
+                // so every lane takes the step
+                g = valid ? t - goe : MININT;
 #pragma unroll
-            for (uint32_t k = 1; k < 32; k <<= 1) {
-                const int32_t o = __shfl_up_sync(FULL, g, k);
-                if (lane >= k) {
-                    const int32_t v = o - (int32_t)k * ge;
-                    if (v > g) g = v;
-                }
+                for (uint32_t k = 1; k < 32; k <<= 1) g = __viaddmax_s32(__shfl_up_sync(FULL, g, k), -(int32_t)k * ge, g);
+                g = __viaddmax_s32(carry_g, -(int32_t)(lane + 1) * ge, g);
+                f = __shfl_up_sync(FULL, g, 1);
+                if (lane == 0) f = carry_g;
+            } else {
+                // F* below the threshold over the whole chunk: no surviving cell, prune decision or
+                // traceback step can see it (see the function comment)
+                f = MININT;
+                g = carry_g > tmax - goe ? carry_g : tmax - goe;
             }
-            {
-                const int32_t v = carry_g - (int32_t)(lane + 1) * ge;
-                if (v > g) g = v;
-            }
-            int32_t f = __shfl_up_sync(FULL, g, 1);
-            if (lane == 0) f = carry_g;
             // op choice with the reference's tie order: diagonal, then vertical, then horizontal
             uint8_t op = T_SUB;
             int32_t cell = d;
             if (cur.y > cell) { cell = cur.y; op = T_GAP_B; }
             if (f > cell) { cell = f; op = T_GAP_A; }
             if (!valid) cell = MININT;
-            int32_t mx = cell;
+            int32_t before = carry_best, mx = t;
+            if (tmax > carry_best) {
 #pragma unroll
-            for (uint32_t k = 1; k < 32; k <<= 1) {
-                const int32_t o = __shfl_up_sync(FULL, mx, k);
-                if (lane >= k && o > mx) mx = o;
+                for (uint32_t k = 1; k < 32; k <<= 1) mx = max(mx, __shfl_up_sync(FULL, mx, k));
+                const int32_t ex = __shfl_up_sync(FULL, mx, 1);
+                if (lane != 0) before = max(before, ex);
             }
-            int32_t before = __shfl_up_sync(FULL, mx, 1);
-            if (lane == 0) before = carry_best;
-            if (carry_best > before) before = carry_best;
             const bool pruned = valid && (before - cell > xdrop);
             const bool alive = valid && !pruned;
             const unsigned alive_mask = __ballot_sync(FULL, alive);
@@ -1118,12 +1133,11 @@ __device__ int align_ex_tb_warp(const uint8_t* __restrict__ a, const uint8_t* __
             }
             if (valid) S.trace[flen + (bi - first0)] = op;
             if (alive_mask) last_b = c0 + 31 - __clz(alive_mask);
-            const int32_t cmax = __shfl_sync(FULL, mx, 31);
-            if (cmax > row_max) {
-                row_max = cmax;
-                row_arg = c0 + __ffs(__ballot_sync(FULL, valid && cell == cmax)) - 1;
+            if (tmax > row_max) {
+                row_max = tmax;
+                row_arg = c0 + __ffs(__ballot_sync(FULL, valid && t == tmax)) - 1;
             }
-            if (cmax > carry_best) carry_best = cmax;
+            if (tmax > carry_best) carry_best = tmax;
             carry_g = __shfl_sync(FULL, g, 31 - __clz(valid_mask));
             carry_h = __shfl_sync(FULL, cur.x, 31);
         }
@@ -1139,7 +1153,7 @@ __device__ int align_ex_tb_warp(const uint8_t* __restrict__ a, const uint8_t* __
         if (last_b + 1 < b_size) {
             b_size = last_b + 1;
         } else if (gap_row >= best - xdrop && b_size <= n) {
-            const uint32_t k = min((uint32_t)((gap_row - (best - xdrop)) / ge) + 1u, n + 1 - b_size);
+            const uint32_t k = ext_count(gap_row, best - xdrop, ge, n + 1 - b_size);
             if (flen + k > S.trace_cap) { need = S.trace_cap * 2 + 4096; return 2; }
             __syncwarp();
             for (uint32_t i = lane; i < k; i += 32) {
