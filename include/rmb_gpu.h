@@ -40,7 +40,8 @@ typedef struct rmb_params {
     int32_t ungapped_cutoff;
     int32_t device;       /* CUDA device ordinal */
     int32_t schedule;     /* 0 = FIFO (only value accepted) */
-    int32_t reserved;
+    int32_t kernels;      /* 0 = automatic; 1 = run every preliminary DP on the warp-cooperative
+                             kernel (the thread-per-extension kernel's fallback), for testing */
 } rmb_params;
 
 typedef struct rmb_ctx rmb_ctx;

@@ -32,7 +32,7 @@ class _Params(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "gap_open", "gap_extend", "word_size", "xdrop_ungap", "xdrop_gap", "xdrop_gap_final",
         "min_raw_gapped_score", "complexity_adjust", "dust", "mask_level", "ungapped_cutoff",
-        "device", "schedule", "reserved")]
+        "device", "schedule", "kernels")]
 
 
 class _Hsp(C.Structure):
@@ -180,11 +180,13 @@ class SearchParams:
     mask_level: int = -1
     ungapped_cutoff: int = -1
     device: int = 0
+    # 0: automatic kernel choice; 1: every preliminary DP on the warp-cooperative kernel
+    kernels: int = 0
 
     def _c(self) -> _Params:
         return _Params(self.gap_open, self.gap_extend, self.word_size, self.xdrop_ungap, self.xdrop_gap,
                        self.xdrop_gap_final, self.min_raw_gapped_score, int(self.complexity_adjust), int(self.dust),
-                       self.mask_level, self.ungapped_cutoff, self.device, 0, 0)
+                       self.mask_level, self.ungapped_cutoff, self.device, 0, self.kernels)
 
 
 class SubjectDb:

@@ -46,7 +46,8 @@ struct DBuf {  // growable device buffer
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
-        size_t nc = std::max<size_t>(n, 256);
+        // whole 16-byte words, so an aligned word read around any valid byte stays inside
+        size_t nc = std::max<size_t>((n + 15) & ~(size_t)15, 256);
         CK(cudaMalloc(&p, nc));
         cap = nc;
     }
@@ -140,7 +141,8 @@ struct rmb_ctx {
     DBuf d_plus, d_rc, d_align, d_align_rc, d_packed, d_plus_off, d_packed_off, d_len, d_params;
     // per-batch device buffers
     DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
-    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, n_wide, band, sel,
+    bool prelim_stream = false;  // thread-per-extension prelim kernel (else the warp kernel)
+    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, n_wide, band, sel,
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
     DevLib L{};
 };
@@ -432,15 +434,40 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
         CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
         ev.start(st);
-        CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
-                         C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(), C.wide.as<uint32_t>(),
-                         C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(), C.sms, st));
+        if (C.prelim_stream)
+            CK(launch_prelim_stream(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
+                                    C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
+                                    C.po.as<PrelimOut>(), C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
+                                    C.cells.as<unsigned long long>(), C.sms, st));
+        else
+            CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
+                             C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
+                             C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(),
+                             C.sms, st));
         ev.stop(st);
         ctr.launches += nu ? 1 : 0;
         uint32_t nw = 0;
         CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctr.gpu_ms_prelim += ev.ms();
+        DBuf* wide_list = &C.wide;
+        if (nw && C.prelim_stream) {
+            // records whose band window outgrew the thread ring: the warp kernel's 256-cell rings
+            C.wide2.ensure((uint64_t)nw * 4);
+            CK(cudaMemsetAsync(C.n_wide.p, 0, 4, st));
+            EvTimer e2;
+            e2.start(st);
+            CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(), C.ung_idx.as<uint32_t>(),
+                             C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
+                             C.wide2.as<uint32_t>(), C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(),
+                             C.sms, st));
+            e2.stop(st);
+            ctr.launches += 1;
+            CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ctr.gpu_ms_prelim += e2.ms();
+            wide_list = &C.wide2;
+        }
         if (nw) {
             uint32_t qmax = 0;
             for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
@@ -450,7 +477,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
             EvTimer ew;
             ew.start(st);
             ctr.launches += 1;
-            CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(), C.ung_idx.as<uint32_t>(),
+            CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, wide_list->as<uint32_t>(), C.ung_idx.as<uint32_t>(),
                                   C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
                                   C.po.as<PrelimOut>(), C.band.as<int2>(), cap, threads,
                                   C.cells.as<unsigned long long>(), C.fails.as<unsigned int>(), st));
@@ -693,6 +720,7 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
             throw Fail(RMB_EINVAL, "negative X-drop or cutoff");
         if (p.dust) throw Fail(RMB_EINVAL, "query DUST masking is not supported by this library (pass dust = 0)");
         if (p.schedule != 0) throw Fail(RMB_EINVAL, "only the FIFO schedule (0) is supported");
+        if (p.kernels != 0 && p.kernels != 1) throw Fail(RMB_EINVAL, "kernels must be 0 (automatic) or 1 (warp prelim)");
         C = new rmb_ctx();
         C->p = p;
         C->matrix_name = matrix_name ? matrix_name : "";
@@ -722,6 +750,7 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         dp.xdrop_gap_final = p.xdrop_gap_final;
         dp.gapped_cutoff = C->gp.gapped_cutoff;
         for (int i = 0; i < 256; ++i) dp.matrix[i] = scores[i];
+        C->prelim_stream = p.kernels == 0 && prelim_stream_eligible(dp.matrix, p.gap_open, p.gap_extend, p.xdrop_gap);
         C->d_params.ensure(sizeof(DevParams));
         CK(cudaMemcpy(C->d_params.p, &dp, sizeof dp, cudaMemcpyHostToDevice));
         *out = C;
@@ -1064,7 +1093,7 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->d_len, &C->d_params, &C->pv, &C->pv_off, &C->cs, &C->cs_off, &C->pos_off, &C->lut_keys,
                    &C->lut_vals, &C->lut_keys2, &C->lut_vals2, &C->lut_counts,
                    &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
-                   &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->n_wide, &C->band,
+                   &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
                    &C->tb_scratch};
     for (DBuf* b : all) b->release();

@@ -17,6 +17,7 @@
 //
 // All scores are int32; the arithmetic and the order of every comparison follow the cited
 // reference functions so results are bit-identical.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -668,13 +669,15 @@ __global__ void __launch_bounds__(128) k_prelim(DevLib L, DevQueries Q, const De
     if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
 }
 
-// One ungapped record per warp; each warp's band lives in a RING_W-cell shared-memory ring.
+// One ungapped record per warp (records list[0..n), or 0..n without a list); each warp's band
+// lives in a RING_W-cell shared-memory ring.
 template <int RING_W>
 __global__ void __launch_bounds__(256) k_prelim_warp(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                       uint64_t n, const uint32_t* __restrict__ idx,
                                                       const SeedHit* __restrict__ hits,
                                                       const uint32_t* __restrict__ hit_pair,
                                                       const UngBox* __restrict__ ub, PrelimOut* __restrict__ out,
+                                                      const uint32_t* __restrict__ list,
                                                       uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide,
                                                       unsigned long long* __restrict__ cells_total) {
     __shared__ int2 ring[(256 / 32) * RING_W];
@@ -686,7 +689,8 @@ __global__ void __launch_bounds__(256) k_prelim_warp(DevLib L, DevQueries Q, con
     uint64_t cells = 0;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t t = warp; t < n; t += nwarps) {
+    for (uint64_t k = warp; k < n; k += nwarps) {
+        const uint64_t t = list ? list[k] : k;
         const uint32_t i = idx[t];
         const uint32_t pair = hit_pair[i];
         const SeedHit h = hits[i];
@@ -754,6 +758,268 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
         cells += c;
     }
     if (cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// ---------------------------------------------------------------------------------------
+// Thread-per-extension score-only X-drop DP over a flat cell stream.
+//
+// Each thread runs the two extensions of one ungapped record after another (left, reversed,
+// then right), one DP cell per loop iteration, and takes the next record from a per-block queue
+// when it is done.  Row ends, new rows and new records are short branches inside the one cell
+// loop, so the lanes of a warp stay together whatever the row widths and record lengths are;
+// the warp-cooperative kernel instead spends a whole 32-lane chunk and a row of fixed costs on
+// every row, while the rows here average about 22 cells.
+//
+// The cell step is the reference's (search/gapped.rs:222-296).  Storage differs in three ways,
+// none of which changes a result:
+//  - Band entries that the reference writes in a loop, the initial row (gapped.rs:187-200), the
+//    end-of-row extension cells and the MININT sentinel (gapped.rs:307-334), are not written:
+//    the next row computes them from (vlo, vhi, ext_val) when it reads them.  Every other band
+//    entry a row reads was written by the row before.
+//  - An entry is two int16 (cell, vertical gap) relative to the X-drop threshold T0 at the start
+//    of the row that wrote it, clamped below at T0 + FLOOR.  Live values lie in
+//    [T0, T0 + X + max score] (X <= 127, scores <= 127, checked by the host); a value below
+//    T0 + FLOOR stays below every later threshold even after adding the best score, so the
+//    clamp only moves values that can no longer make a cell survive.
+//  - Score rows are int8, with every score below -(X + 1) held as -(X + 1) (see the matrix
+//    setup below).
+//  - The band window of a row (b_size - first_b cells) must fit the RING-entry ring; a record
+//    whose window grows past it, or whose cell count passes STREAM_MAX_CELLS, is listed for
+//    the warp kernel.
+// ---------------------------------------------------------------------------------------
+constexpr int STREAM_RING = 64;
+// A record whose two extensions pass this many cells is handed to the warp kernel: one thread
+// takes ~0.1 us a cell, so the few extensions thousands of rows long would hold their warp
+// (and the end of the launch) for milliseconds, while a warp does one of their rows in a few
+// hundred cycles.
+constexpr uint32_t STREAM_MAX_CELLS = 8192;
+constexpr int STREAM_BLOCK = 128;
+constexpr int STREAM_BLOCKS_PER_SM = 6;
+constexpr int32_t STREAM_FLOOR = -16384;
+
+__device__ __forceinline__ int32_t score_int8(const uint4 r, uint32_t c) {
+    // r: the 16 int8 scores of the row residue; c: the column residue (0..15)
+    const uint32_t lo = (c & 8) ? r.z : r.x, hi = (c & 8) ? r.w : r.y;
+    const uint32_t k = c & 7;
+    uint32_t v;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(v) : "r"(lo), "r"(hi), "r"(k * 0x1111u + 0x8880u));
+    return (int32_t)v;
+}
+__device__ __forceinline__ uint32_t stream_enc(int32_t x, int32_t y, int32_t base) {
+    const int32_t ex = max(x - base, STREAM_FLOOR), ey = max(y - base, STREAM_FLOOR);
+    return __byte_perm((uint32_t)ex, (uint32_t)ey, 0x5410);
+}
+
+__global__ void __launch_bounds__(STREAM_BLOCK, STREAM_BLOCKS_PER_SM)
+k_prelim_stream(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint64_t n,
+                const uint32_t* __restrict__ idx, const SeedHit* __restrict__ hits,
+                const uint32_t* __restrict__ hit_pair, const UngBox* __restrict__ ub, PrelimOut* __restrict__ out,
+                uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide, unsigned int* __restrict__ queue,
+                unsigned long long* __restrict__ cells_total) {
+    __shared__ uint32_t ring[STREAM_RING * STREAM_BLOCK];
+    __shared__ uint4 smat[16];
+    if (threadIdx.x < 16) {
+        // scores below -(X + 1), X the largest X-drop of any record, only ever make a diagonal
+        // value below the threshold (a stored cell never exceeds the running best), so they are
+        // all held as -(X + 1)
+        const int32_t xmax = max(P->xdrop_gap, P->gap_open + P->gap_extend);
+        uint32_t w[4];
+        for (int q = 0; q < 4; ++q) {
+            w[q] = 0;
+            for (int k = 0; k < 4; ++k) {
+                const int32_t v = max(P->matrix[threadIdx.x * 16 + q * 4 + k], -(xmax + 1));
+                w[q] |= ((uint32_t)v & 0xffu) << (8 * k);
+            }
+        }
+        smat[threadIdx.x] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    __syncthreads();
+    uint32_t* const my = ring + threadIdx.x;  // band entry j at my[(j % RING) * BLOCK]
+    const int32_t ge = P->gap_extend, goe = P->gap_open + ge;
+    const float inv_ge = 1.0f / (float)ge;
+    const int32_t cutoff = P->gapped_cutoff;
+
+    // record
+    uint64_t t = 0;
+    uint32_t qa = 0, sa = 0, qp = 0, sp = 0, tbq = 0, tbs = 0, rec_cells = 0;
+    bool plus = true;
+    int32_t xdrop = 0;
+    const uint8_t *qseq = nullptr, *sseq = nullptr;
+    int32_t l_score = 0;
+    uint32_t l_a = 0, l_b = 0;
+    int phase = 0;  // 0: need a record, 1: left extension, 2: right extension
+    // extension: row residue a[ai] at abase[dir * ai]; column residue b[bi] at qal[pb + dir * bi]
+    const uint8_t *abase = nullptr, *qal = nullptr;
+    int32_t dir = 1, pb = 0, r0 = 0, wcur = INT32_MIN;
+    uint8_t a_nx = 0;
+    uint32_t m = 0, nb = 0, ai = 0, bi = 0, first_b = 0, b_size = 0, last_b = 0, best_a = 0, best_b = 0, vlo = 0,
+             vhi = 0;
+    int32_t best = 0, prev_best = 0, thr = 0, sc = 0, gap_row = 0, ext_val = 0, base_prev = 0, base_cur = 0;
+    uint4 srow = make_uint4(0, 0, 0, 0);
+    uint32_t bw = 0;
+    // records come from one queue for the grid; the next index is fetched one record ahead
+    unsigned int next_t = atomicAdd(queue, 1u);
+    unsigned long long cells = 0;
+    bool fetch = true;  // no extension running: finish the last one and start the next
+    bool dp_fail = false;
+
+    auto new_row = [&]() {
+        srow = smat[a_nx & 15];
+        if (ai + 1 < m) a_nx = abase[(ptrdiff_t)dir * (ptrdiff_t)(ai + 1)];  // next row's residue
+        sc = MININT; gap_row = MININT;
+        last_b = first_b; prev_best = best; bi = first_b;
+        base_prev = base_cur; base_cur = thr;
+        rec_cells += b_size - first_b;
+    };
+
+    // The loop ends for the whole warp at once (lanes out of records idle until then): the
+    // warp-wide vote at the top of every iteration brings the lanes back together after a row
+    // end or a record change, so the cell step always runs with every busy lane.
+    bool out_of_records = false;
+    for (;;) {
+        if (!__any_sync(0xffffffffu, !out_of_records)) break;
+        if (!fetch && !out_of_records) {
+            // one cell (gapped.rs:234-262)
+            const uint32_t w = my[(bi % STREAM_RING) * STREAM_BLOCK];
+            int32_t cx = ((int32_t)(w << 16) >> 16) + base_prev, cy = ((int32_t)w >> 16) + base_prev;
+            if (bi >= vlo) {
+                const bool e = bi < vhi;
+                const int32_t v = ext_val - (int32_t)(bi - vlo) * ge;
+                cx = e ? v : MININT;
+                cy = e ? v - goe : MININT;
+            }
+            const int32_t pos = pb + dir * (int32_t)bi;
+            if ((pos >> 2) != wcur) {
+                wcur = pos >> 2;
+                bw = *(const uint32_t*)(qal + (ptrdiff_t)(pos & ~3));
+            }
+            const uint32_t code = __byte_perm(bw, 0, (uint32_t)pos & 3u) & 15u;
+            const int32_t nxt = bi < nb ? cx + score_int8(srow, code) : 0;
+            const int32_t cell = max(max(sc, cy), gap_row);
+            const bool alive = cell >= thr;
+            if (!alive && bi == first_b) ++first_b;
+            if (alive) last_b = bi;
+            if (cell > best) { best = cell; best_b = bi; thr = cell - xdrop; }
+            const int32_t open = cell - goe;
+            const int32_t ny = max(cy - ge, open);
+            if (alive) gap_row = max(gap_row - ge, open);
+            my[(bi % STREAM_RING) * STREAM_BLOCK] = stream_enc(alive ? cell : MININT, alive ? ny : cy, base_cur);
+            sc = nxt;
+            if (++bi >= b_size) {
+                // end of row (gapped.rs:298-334)
+                if (best > prev_best) best_a = ai + 1;
+                if (first_b >= b_size) {
+                    fetch = true;
+                } else {
+                    if (last_b + 1 < b_size) {
+                        b_size = last_b + 1;
+                        vlo = vhi = b_size;
+                    } else {
+                        uint32_t k = 0;
+                        if (b_size <= nb && gap_row >= thr) {
+                            const int32_t num = gap_row - thr;  // 0 <= num <= xdrop
+                            int32_t q = __float2int_rz((float)num * inv_ge);
+                            if ((q + 1) * ge <= num) ++q;
+                            else if (q * ge > num) --q;
+                            k = min((uint32_t)q + 1u, nb + 1 - b_size);
+                        }
+                        vlo = b_size; ext_val = gap_row;
+                        b_size += k;
+                        vhi = b_size;
+                    }
+                    if (b_size <= nb) ++b_size;
+                    if (b_size - first_b > (uint32_t)STREAM_RING || rec_cells + (b_size - first_b) > STREAM_MAX_CELLS) {
+                        dp_fail = true;
+                        fetch = true;
+                    } else if (++ai >= m) {
+                        fetch = true;
+                    } else {
+                        new_row();
+                    }
+                }
+            }
+        }
+        if (fetch && !out_of_records) {
+            // the extension that just ended (best, best_a, best_b; zero for an empty one), then the
+            // next non-empty extension
+            while (fetch) {
+                if (phase != 0 && dp_fail) {
+                    wide[atomicAdd(n_wide, 1u)] = (uint32_t)t;
+                    phase = 0;
+                }
+                if (phase == 1) {
+                    l_score = best; l_a = best_a; l_b = best_b;
+                    const uint32_t rm = sa > sp ? sa - sp : 0, rn = qa > qp ? qa - qp : 0;
+                    if (rm > 0 && rn > 0) {
+                        abase = sseq + sp; pb = r0 + (int32_t)qp; m = rm; nb = rn; dir = 1;
+                        phase = 2;
+                    } else {
+                        best = 0; best_a = 0; best_b = 0;
+                        phase = 3;
+                    }
+                } else if (phase == 2 || phase == 3) {
+                    // both extensions done: engine.rs:1380-1397
+                    PrelimOut o{INT32_MIN, 0, 0, 0, 0, 0, 0};
+                    const int32_t total = l_score + best;
+                    if (total >= 0) {
+                        uint32_t q0 = qp - l_b, s0 = sp - l_a, q1 = qp + best_b, s1 = sp + best_a;
+                        if (!plus) {
+                            const uint32_t t0 = qa - q1, t1 = qa - q0, t2 = sa - s1, t3 = sa - s0;
+                            q0 = t0; q1 = t1; s0 = t2; s1 = t3;
+                        }
+                        if (total >= cutoff) o = PrelimOut{total, q0, q1, s0, s1, tbq, tbs};
+                    }
+                    out[t] = o;
+                    cells += rec_cells;
+                    phase = 0;
+                }
+                if (phase == 0) {
+                    // next record
+                    t = next_t;
+                    if (t >= n) { out_of_records = true; break; }
+                    next_t = atomicAdd(queue, 1u);
+                    const uint32_t i = idx[t];
+                    const uint32_t pair = hit_pair[i];
+                    const SeedHit h = hits[i];
+                    const UngBox u = ub[i];
+                    const uint32_t qi = pair / L.n, si = pair % L.n;
+                    qa = Q.len[qi];
+                    sa = L.len[si];
+                    plus = !(h.qs >> 31);
+                    uint32_t piv[4];
+                    prelim_pivot(plus, h.qs & 0x7fffffffu, h.s, u.s_start, u.s_end, qa, sa, (uint32_t)Q.lw[qi], piv);
+                    const int32_t xd = P->xdrop_gap < u.score ? P->xdrop_gap : u.score;
+                    xdrop = xd > goe ? xd : goe;
+                    qseq = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
+                    sseq = L.plus + L.plus_off[si] + 1;
+                    qal = (const uint8_t*)((uintptr_t)qseq & ~(uintptr_t)3);
+                    r0 = (int32_t)(qseq - qal);
+                    qp = piv[0]; sp = piv[1]; tbq = piv[2]; tbs = piv[3];
+                    rec_cells = 0;
+                    abase = sseq; pb = r0; m = sp; nb = qp; dir = -1;
+                    phase = 1;
+                }
+                if (phase == 3) continue;
+                // start the extension set up above (gapped.rs:165-200)
+                dp_fail = false;
+                best = 0; best_a = 0; best_b = 0;
+                if (m == 0 || nb == 0) continue;  // empty: result 0
+                if (dir < 0) { abase += m - 1; pb += (int32_t)nb - 1; }
+                const uint32_t jmax = (uint32_t)((xdrop - goe) / ge) + 1u;
+                const uint32_t J = jmax < nb ? jmax : nb;
+                if (J + 1 > (uint32_t)STREAM_RING) { dp_fail = true; continue; }
+                // initial row, computed on read: entries 1..J
+                b_size = J + 1; vlo = 1; vhi = J + 1; ext_val = -goe;
+                first_b = 0; ai = 0; thr = -xdrop; base_cur = -xdrop;
+                my[0] = stream_enc(0, -goe, base_cur);
+                wcur = INT32_MIN;
+                a_nx = abase[0];
+                new_row();
+                fetch = false;
+            }
+        }
+    }
+    if (cells) atomicAdd(cells_total, cells);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1372,15 +1638,40 @@ size_t diag_cell_bytes() { return sizeof(DiagCell); }
 
 constexpr int PRELIM_RING = 256;
 
-cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n, const uint32_t* idx,
-                          const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub, PrelimOut* out,
-                          uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st) {
+cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n, const uint32_t* list,
+                          const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                          PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
+                          cudaStream_t st) {
     if (!n) return cudaSuccess;
     const int block = 256;
     const uint64_t blocks_wanted = (n + 7) / 8;
     const uint64_t cap = (uint64_t)sms * 8;
     const int grid = (int)(blocks_wanted < cap ? blocks_wanted : cap);
-    k_prelim_warp<PRELIM_RING><<<grid, block, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide, n_wide, cells);
+    k_prelim_warp<PRELIM_RING><<<grid, block, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, list, wide, n_wide,
+                                                       cells);
+    return cudaGetLastError();
+}
+
+bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap) {
+    // int8 score rows: positive scores <= 127 and X + 1 <= 128 for the clamp of the negative ones
+    const int32_t xmax = std::max(xdrop_gap, gap_open + gap_extend);
+    if (gap_extend < 1 || gap_open < 0 || xmax > 127) return false;
+    for (int i = 0; i < 256; ++i)
+        if (matrix256[i] > 127) return false;
+    return true;
+}
+
+cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                                 const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                                 PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells,
+                                 int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
+    const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
+    const int grid = (int)(want < cap ? want : cap);
+    // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
+    k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide, n_wide, n_wide + 1,
+                                                   cells);
     return cudaGetLastError();
 }
 

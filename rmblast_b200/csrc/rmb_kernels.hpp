@@ -17,9 +17,18 @@ size_t diag_cell_bytes();
 cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32_t ucut, uint64_t pair0,
                          uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits, const UngBox* ub, uint8_t* flags,
                          uint32_t* scratch, void* cells, int sms, cudaStream_t st);
-cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n, const uint32_t* idx,
-                          const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub, PrelimOut* out,
-                          uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st);
+cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n, const uint32_t* list,
+                          const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                          PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
+                          cudaStream_t st);
+// Whether the thread-per-extension kernel's int16 band entries and int8 score rows hold the
+// parameters exactly (positive scores <= 127; X-drop and gap_open + gap_extend <= 127).
+// launch_prelim_stream uses n_wide[0] (overflow count) and n_wide[1] (record queue), both zeroed.
+bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap);
+cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                                 const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                                 PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells,
+                                 int sms, cudaStream_t st);
 cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_wide,
                                const uint32_t* wide, const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair,
                                const UngBox* ub, PrelimOut* out, int2* band_mem, uint64_t band_cap, uint32_t threads,

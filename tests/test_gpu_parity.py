@@ -19,13 +19,13 @@ def _built():
     build.build()
 
 
-def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str):
+def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str, kernels: int = 0):
     m = api.ScoreMatrix.from_text(matrix_text, matrix_name)
     sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
                           xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
                           min_raw_gapped_score=p["min_raw_gapped_score"],
                           complexity_adjust=bool(p.get("complexity_adjust", 0)), dust=False,
-                          mask_level=p.get("mask_level", -1))
+                          mask_level=p.get("mask_level", -1), kernels=kernels)
     return api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
 
 
@@ -118,6 +118,26 @@ def test_word_sizes_stage_taps_and_output(ws):
     res = s.search(qs, [n for n, _ in recs])
     want_txt, _, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
     assert res.tabular(FIELDS) == want_txt
+
+
+@pytest.mark.parametrize("kernels", [0, 1])
+@pytest.mark.parametrize("gaps", [(20, 5, 100, 0.2), (3, 1, 120, 0.03)])
+def test_prelim_kernels_match_oracle(kernels, gaps):
+    """Both preliminary-DP paths: the thread-per-extension kernel with its fallback for bands wider
+    than its ring (cheap gaps with a large X-drop widen the band), and the warp kernel alone."""
+    qf, dbf, p = synthetic("small", gaps[3], synth.RM_FLAGS)
+    p.update(gap_open=gaps[0], gap_extend=gaps[1], xdrop_gap=gaps[2])
+    s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, kernels=kernels)
+    recs = api.read_fasta(qf)
+    qs = [api.encode(seq) for _, seq in recs]
+    got = s.stage(qs, 2)
+    want = O.stage_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, 2)
+    assert len(want) > 10
+    assert sorted(map(tuple, got.tolist())) == sorted(map(tuple, want.tolist()))
+    res = s.search(qs, [n for n, _ in recs])
+    want_txt, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert res.tabular(FIELDS) == want_txt
+    assert res.counters["so_cells"] >= ctr["so_cells"]
 
 
 def test_golden_stage_taps_match_oracle():
