@@ -732,6 +732,104 @@ __global__ void __launch_bounds__(256) k_prelim_warp(DevLib L, DevQueries Q, con
     if (lane == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
 }
 
+// Geometry of one ungapped record's preliminary DP (engine.rs:1350-1372).
+struct RecGeom {
+    bool plus;
+    uint32_t qa, sa, qp, sp, tbq, tbs;
+    int32_t xd;
+    const uint8_t *qseq, *sseq;
+};
+__device__ __forceinline__ RecGeom rec_geom(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t i,
+                                            const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub) {
+    const uint32_t pair = hit_pair[i];
+    const SeedHit h = hits[i];
+    const UngBox u = ub[i];
+    const uint32_t qi = pair / L.n, si = pair % L.n;
+    RecGeom g;
+    g.qa = Q.len[qi];
+    g.sa = L.len[si];
+    g.plus = !(h.qs >> 31);
+    uint32_t piv[4];
+    prelim_pivot(g.plus, h.qs & 0x7fffffffu, h.s, u.s_start, u.s_end, g.qa, g.sa, (uint32_t)Q.lw[qi], piv);
+    g.xd = P->xdrop_gap < u.score ? P->xdrop_gap : u.score;
+    g.qseq = (g.plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
+    g.sseq = L.plus + L.plus_off[si] + 1;
+    g.qp = piv[0]; g.sp = piv[1]; g.tbq = piv[2]; g.tbs = piv[3];
+    return g;
+}
+
+// The records list[0..n_list) with each of their two extensions on its own warp: task 2k is
+// record list[k]'s left extension, 2k + 1 its right one.  Results (score, a_len, b_len, ok) go
+// to dres[task]; k_prelim_combine joins them.  These are the records the thread kernel passed
+// on, a few of them thousands of rows long, so the launch lasts as long as its longest
+// extension and not its longest record.
+template <int RING_W>
+__global__ void __launch_bounds__(256) k_prelim_warp_dir(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                          uint32_t n_list, const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ idx,
+                                                          const SeedHit* __restrict__ hits,
+                                                          const uint32_t* __restrict__ hit_pair,
+                                                          const UngBox* __restrict__ ub, int4* __restrict__ dres,
+                                                          unsigned long long* __restrict__ cells_total) {
+    __shared__ int2 ring[(256 / 32) * RING_W];
+    __shared__ int32_t mat[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    RingBand band{ring + wib * RING_W, RING_W - 1};
+    uint64_t cells = 0;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t k = warp; k < 2ull * n_list; k += nwarps) {
+        const RecGeom g = rec_geom(L, Q, P, idx[list[k >> 1]], hits, hit_pair, ub);
+        DpResult r{0, 0, 0};
+        uint64_t c = 0;
+        bool ok = true;
+        if (!(k & 1)) {
+            ok = so_dp_warp<true>(g.sseq, g.qseq, g.sp, g.qp, P->gap_open, P->gap_extend, g.xd, mat, band, r, c);
+        } else {
+            const uint32_t rm = g.sa > g.sp ? g.sa - g.sp : 0, rn = g.qa > g.qp ? g.qa - g.qp : 0;
+            if (rm > 0 && rn > 0)
+                ok = so_dp_warp<false>(g.sseq + g.sp, g.qseq + g.qp, rm, rn, P->gap_open, P->gap_extend, g.xd, mat,
+                                       band, r, c);
+        }
+        if (ok) cells += c;
+        if (lane == 0) dres[k] = make_int4(r.score, (int32_t)r.a_len, (int32_t)r.b_len, ok ? 1 : 0);
+    }
+    if (lane == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// Joins k_prelim_warp_dir's two extensions of each listed record (engine.rs:1380-1397); a record
+// with an extension wider than the warp ring goes to `wide`.
+__global__ void k_prelim_combine(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint32_t n_list,
+                                 const uint32_t* __restrict__ list, const uint32_t* __restrict__ idx,
+                                 const SeedHit* __restrict__ hits, const uint32_t* __restrict__ hit_pair,
+                                 const UngBox* __restrict__ ub, const int4* __restrict__ dres,
+                                 PrelimOut* __restrict__ out, uint32_t* __restrict__ wide,
+                                 unsigned int* __restrict__ n_wide) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_list) return;
+    const uint32_t t = list[k];
+    const int4 l = dres[2 * k], r = dres[2 * k + 1];
+    if (!l.w || !r.w) {
+        wide[atomicAdd(n_wide, 1u)] = t;
+        return;
+    }
+    const RecGeom g = rec_geom(L, Q, P, idx[t], hits, hit_pair, ub);
+    PrelimOut o{INT32_MIN, 0, 0, 0, 0, 0, 0};
+    const int32_t total = l.x + r.x;
+    if (total >= 0) {
+        uint32_t q0 = g.qp - (uint32_t)l.z, s0 = g.sp - (uint32_t)l.y, q1 = g.qp + (uint32_t)r.z,
+                 s1 = g.sp + (uint32_t)r.y;
+        if (!g.plus) {
+            const uint32_t t0 = g.qa - q1, t1 = g.qa - q0, t2 = g.sa - s1, t3 = g.sa - s0;
+            q0 = t0; q1 = t1; s0 = t2; s1 = t3;
+        }
+        if (total >= P->gapped_cutoff) o = PrelimOut{total, q0, q1, s0, s1, g.tbq, g.tbs};
+    }
+    out[t] = o;
+}
+
 // The records whose band outgrew the ring, with the band at absolute indices in global memory
 // (`band_cap` cells per thread, at least the longest inner sequence + 2).
 __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
@@ -1672,6 +1770,24 @@ cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const Dev
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
     k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide, n_wide, n_wide + 1,
                                                    cells);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_list,
+                                const uint32_t* list, const uint32_t* idx, const SeedHit* hits,
+                                const uint32_t* hit_pair, const UngBox* ub, int4* dres, PrelimOut* out,
+                                uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
+                                cudaStream_t st) {
+    if (!n_list) return cudaSuccess;
+    const int block = 256;
+    const uint64_t blocks_wanted = (2ull * n_list + 7) / 8;
+    const uint64_t cap = (uint64_t)sms * 8;
+    const int grid = (int)(blocks_wanted < cap ? blocks_wanted : cap);
+    k_prelim_warp_dir<PRELIM_RING><<<grid, block, 0, st>>>(L, Q, P, n_list, list, idx, hits, hit_pair, ub, dres, cells);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_prelim_combine<<<(n_list + 127) / 128, 128, 0, st>>>(L, Q, P, n_list, list, idx, hits, hit_pair, ub, dres, out,
+                                                          wide, n_wide);
     return cudaGetLastError();
 }
 

@@ -29,6 +29,13 @@ cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const Dev
                                  const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                  PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells,
                                  int sms, cudaStream_t st);
+// Records `list` (the thread kernel's overflow), one warp per extension; dres holds 2 x n_list
+// int4.  Records that overflow the warp rings go to `wide` (count in n_wide[0]).
+cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_list,
+                                const uint32_t* list, const uint32_t* idx, const SeedHit* hits,
+                                const uint32_t* hit_pair, const UngBox* ub, int4* dres, PrelimOut* out,
+                                uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
+                                cudaStream_t st);
 cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_wide,
                                const uint32_t* wide, const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair,
                                const UngBox* ub, PrelimOut* out, int2* band_mem, uint64_t band_cap, uint32_t threads,
