@@ -142,7 +142,7 @@ struct rmb_ctx {
     // per-batch device buffers
     DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     bool prelim_stream = false;  // thread-per-extension prelim kernel (else the warp kernel)
-    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, n_wide, band, sel,
+    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
     DevLib L{};
 };
@@ -434,11 +434,14 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
         CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
         ev.start(st);
-        if (C.prelim_stream)
+        if (C.prelim_stream) {
+            C.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
             CK(launch_prelim_stream(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
-                                    C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
+                                    C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p,
                                     C.po.as<PrelimOut>(), C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
                                     C.cells.as<unsigned long long>(), C.sms, st));
+            ctr.launches += nu ? 1 : 0;
+        }
         else
             CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
                              C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
@@ -1094,7 +1097,7 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->d_len, &C->d_params, &C->pv, &C->pv_off, &C->cs, &C->cs_off, &C->pos_off, &C->lut_keys,
                    &C->lut_vals, &C->lut_keys2, &C->lut_vals2, &C->lut_counts,
                    &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
-                   &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->n_wide, &C->band,
+                   &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->geo, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
                    &C->tb_scratch};
     for (DBuf* b : all) b->release();

@@ -862,7 +862,7 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
 // Thread-per-extension score-only X-drop DP over a flat cell stream.
 //
 // Each thread runs the two extensions of one ungapped record after another (left, reversed,
-// then right), one DP cell per loop iteration, and takes the next record from a per-block queue
+// then right), one DP cell per loop iteration, and takes the next record from a grid-wide queue
 // when it is done.  Row ends, new rows and new records are short branches inside the one cell
 // loop, so the lanes of a warp stay together whatever the row widths and record lengths are;
 // the warp-cooperative kernel instead spends a whole 32-lane chunk and a row of fixed costs on
@@ -872,15 +872,16 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
 // none of which changes a result:
 //  - Band entries that the reference writes in a loop, the initial row (gapped.rs:187-200), the
 //    end-of-row extension cells and the MININT sentinel (gapped.rs:307-334), are not written:
-//    the next row computes them from (vlo, vhi, ext_val) when it reads them.  Every other band
-//    entry a row reads was written by the row before.
-//  - An entry is two int16 (cell, vertical gap) relative to the X-drop threshold T0 at the start
-//    of the row that wrote it, clamped below at T0 + FLOOR.  Live values lie in
-//    [T0, T0 + X + max score] (X <= 127, scores <= 127, checked by the host); a value below
-//    T0 + FLOOR stays below every later threshold even after adding the best score, so the
-//    clamp only moves values that can no longer make a cell survive.
-//  - Score rows are int8, with every score below -(X + 1) held as -(X + 1) (see the matrix
-//    setup below).
+//    the next row computes them from (vlo, nvirt, ext_val) when it reads them.  Every other
+//    band entry a row reads was written by the row before.
+//  - An entry is 32 bits: cell and vertical gap as 14-bit values relative to the X-drop
+//    threshold T0 at the start of the row that wrote it, clamped below at T0 + FLOOR, and the
+//    column residue.  Live values lie in [T0, T0 + X + max score] (X <= 8000, scores <= 127,
+//    checked by the host); a value below T0 + FLOOR stays below every later threshold even after
+//    adding the best score, so the clamp only moves values that can no longer make a cell
+//    survive (MININT included).  A band index's residue is copied in (with those of up to three
+//    neighbours, one word load) the first time a row reaches it; every index at or past that
+//    frontier is a computed entry, so only its residue bits are live.
 //  - The band window of a row (b_size - first_b cells) must fit the RING-entry ring; a record
 //    whose window grows past it, or whose cell count passes STREAM_MAX_CELLS, is listed for
 //    the warp kernel.
@@ -893,48 +894,66 @@ constexpr int STREAM_RING = 64;
 constexpr uint32_t STREAM_MAX_CELLS = 8192;
 constexpr int STREAM_BLOCK = 128;
 constexpr int STREAM_BLOCKS_PER_SM = 6;
-constexpr int32_t STREAM_FLOOR = -16384;
+constexpr int32_t STREAM_FLOOR = -8192;
 
-__device__ __forceinline__ int32_t score_int8(const uint4 r, uint32_t c) {
-    // r: the 16 int8 scores of the row residue; c: the column residue (0..15)
-    const uint32_t lo = (c & 8) ? r.z : r.x, hi = (c & 8) ? r.w : r.y;
-    const uint32_t k = c & 7;
-    uint32_t v;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(v) : "r"(lo), "r"(hi), "r"(k * 0x1111u + 0x8880u));
-    return (int32_t)v;
+// One record's DP geometry (engine.rs:1350-1372), written by k_prelim_prep so that the DP kernel
+// starts a record with one 48-byte load: query and subject sequence starts (record frame),
+// their lengths, the pivot, the traceback seed, X = max(min(xdrop_gap, ungapped score),
+// gap_open + gap_extend), and the strand with the first row residue of each extension.
+struct __align__(16) PrelimGeo {
+    uint64_t qseq, sseq;
+    uint32_t qa, sa, qp, sp;
+    uint32_t tbq, tbs, xdrop, flags;  // flags: plus | a[sp - 1] << 8 | a[sp] << 16
+};
+
+__global__ void __launch_bounds__(256) k_prelim_prep(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                      uint64_t n, const uint32_t* __restrict__ idx,
+                                                      const SeedHit* __restrict__ hits,
+                                                      const uint32_t* __restrict__ hit_pair,
+                                                      const UngBox* __restrict__ ub, PrelimGeo* __restrict__ geo) {
+    const int32_t goe = P->gap_open + P->gap_extend;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const RecGeom g = rec_geom(L, Q, P, idx[t], hits, hit_pair, ub);
+        const uint8_t al = g.sp > 0 ? g.sseq[g.sp - 1] : 0, ar = g.sa > g.sp ? g.sseq[g.sp] : 0;
+        PrelimGeo o;
+        o.qseq = (uint64_t)g.qseq;
+        o.sseq = (uint64_t)g.sseq;
+        o.qa = g.qa; o.sa = g.sa; o.qp = g.qp; o.sp = g.sp;
+        o.tbq = g.tbq; o.tbs = g.tbs;
+        o.xdrop = (uint32_t)(g.xd > goe ? g.xd : goe);
+        o.flags = (g.plus ? 1u : 0u) | ((uint32_t)al << 8) | ((uint32_t)ar << 16);
+        geo[t] = o;
+    }
 }
-__device__ __forceinline__ uint32_t stream_enc(int32_t x, int32_t y, int32_t base) {
-    const int32_t ex = max(x - base, STREAM_FLOOR), ey = max(y - base, STREAM_FLOOR);
-    return __byte_perm((uint32_t)ex, (uint32_t)ey, 0x5410);
+
+// Band entry: bits 0-13 cell, 14-27 vertical gap (14-bit two's complement, relative to the
+// row threshold), 28-31 the column residue b[j].  stream_pack keeps w's residue bits.
+__device__ __forceinline__ uint32_t stream_pack(int32_t ex, int32_t ey, uint32_t w) {
+    uint32_t r;
+    asm("bfi.b32 %0, %1, %2, 14, 14;" : "=r"(r) : "r"((uint32_t)ey), "r"(w));
+    asm("bfi.b32 %0, %1, %0, 0, 14;" : "+r"(r) : "r"((uint32_t)ex));
+    return r;
 }
 
 __global__ void __launch_bounds__(STREAM_BLOCK, STREAM_BLOCKS_PER_SM)
-k_prelim_stream(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint64_t n,
-                const uint32_t* __restrict__ idx, const SeedHit* __restrict__ hits,
-                const uint32_t* __restrict__ hit_pair, const UngBox* __restrict__ ub, PrelimOut* __restrict__ out,
+k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __restrict__ geo,
+                PrelimOut* __restrict__ out,
                 uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide, unsigned int* __restrict__ queue,
                 unsigned long long* __restrict__ cells_total) {
     __shared__ uint32_t ring[STREAM_RING * STREAM_BLOCK];
-    __shared__ uint4 smat[16];
-    if (threadIdx.x < 16) {
+    __shared__ int32_t smat[256];
+    {
         // scores below -(X + 1), X the largest X-drop of any record, only ever make a diagonal
         // value below the threshold (a stored cell never exceeds the running best), so they are
-        // all held as -(X + 1)
+        // all held as -(X + 1), which keeps every sum far from overflow
         const int32_t xmax = max(P->xdrop_gap, P->gap_open + P->gap_extend);
-        uint32_t w[4];
-        for (int q = 0; q < 4; ++q) {
-            w[q] = 0;
-            for (int k = 0; k < 4; ++k) {
-                const int32_t v = max(P->matrix[threadIdx.x * 16 + q * 4 + k], -(xmax + 1));
-                w[q] |= ((uint32_t)v & 0xffu) << (8 * k);
-            }
-        }
-        smat[threadIdx.x] = make_uint4(w[0], w[1], w[2], w[3]);
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) smat[i] = max(P->matrix[i], -(xmax + 1));
     }
     __syncthreads();
     uint32_t* const my = ring + threadIdx.x;  // band entry j at my[(j % RING) * BLOCK]
     const int32_t ge = P->gap_extend, goe = P->gap_open + ge;
-    const float inv_ge = 1.0f / (float)ge;
+    // floor(num / ge) = (num * ge_magic) >> 32 for 0 <= num <= 8000 (ge <= 8000)
+    const uint64_t ge_magic = (0x100000000ull + (uint64_t)ge - 1) / (uint64_t)ge;
     const int32_t cutoff = P->gapped_cutoff;
 
     // record
@@ -945,95 +964,105 @@ k_prelim_stream(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint64_
     const uint8_t *qseq = nullptr, *sseq = nullptr;
     int32_t l_score = 0;
     uint32_t l_a = 0, l_b = 0;
-    int phase = 0;  // 0: need a record, 1: left extension, 2: right extension
+    int phase = 0;  // 0: need a record, 1: left extension, 2: right extension, 3: no right extension
     // extension: row residue a[ai] at abase[dir * ai]; column residue b[bi] at qal[pb + dir * bi]
     const uint8_t *abase = nullptr, *qal = nullptr;
-    int32_t dir = 1, pb = 0, r0 = 0, wcur = INT32_MIN;
-    uint8_t a_nx = 0;
+    int32_t dir = 1, pb = 0, r0 = 0;
+    uint32_t filled = 0;  // residues of band indices [.., filled) are in the ring
+    uint8_t a_nx = 0, a0_left = 0, a0_right = 0;
     uint32_t m = 0, nb = 0, ai = 0, bi = 0, first_b = 0, b_size = 0, last_b = 0, best_a = 0, best_b = 0, vlo = 0,
-             vhi = 0;
-    int32_t best = 0, prev_best = 0, thr = 0, sc = 0, gap_row = 0, ext_val = 0, base_prev = 0, base_cur = 0;
-    uint4 srow = make_uint4(0, 0, 0, 0);
-    uint32_t bw = 0;
+             nvirt = 0, srow = 0;
+    int32_t best = 0, prev_best = 0, thr = 0, sc = 0, gap_row = 0, ext_val = 0, base_prev = 0, base_cur = 0,
+            floor_cur = 0;
+    unsigned long long cells = 0;
     // records come from one queue for the grid; the next index is fetched one record ahead
     unsigned int next_t = atomicAdd(queue, 1u);
-    unsigned long long cells = 0;
     bool fetch = true;  // no extension running: finish the last one and start the next
     bool dp_fail = false;
 
     auto new_row = [&]() {
-        srow = smat[a_nx & 15];
+        srow = (uint32_t)(a_nx & 15) * 16u;
         if (ai + 1 < m) a_nx = abase[(ptrdiff_t)dir * (ptrdiff_t)(ai + 1)];  // next row's residue
         sc = MININT; gap_row = MININT;
         last_b = first_b; prev_best = best; bi = first_b;
-        base_prev = base_cur; base_cur = thr;
+        base_prev = base_cur; base_cur = thr; floor_cur = thr + STREAM_FLOOR;
         rec_cells += b_size - first_b;
+    };
+    // copy the residues of band indices filled.. (up to 4, one aligned word of the column
+    // sequence; only indices below `limit`: the ring holds RING of them) into the ring
+    auto fill_word = [&](uint32_t limit) {
+        const int32_t addr = pb + dir * (int32_t)filled;
+        const uint32_t wv = *(const uint32_t*)(qal + (ptrdiff_t)(addr & ~3));
+        const uint32_t cnt = dir > 0 ? 4u - (uint32_t)(addr & 3) : (uint32_t)(addr & 3) + 1u;
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t i = filled + q;
+            if (q < cnt && i < limit) {
+                const int32_t aq = addr + dir * (int32_t)q;
+                my[(i % STREAM_RING) * STREAM_BLOCK] = ((wv >> ((aq & 3) * 8)) & 15u) << 28;
+            }
+        }
+        filled += min(cnt, limit - filled);
     };
 
     // The loop ends for the whole warp at once (lanes out of records idle until then): the
     // warp-wide vote at the top of every iteration brings the lanes back together after a row
-    // end or a record change, so the cell step always runs with every busy lane.
+    // end or a record change, so the cell steps run with every busy lane.
     bool out_of_records = false;
     for (;;) {
         if (!__any_sync(0xffffffffu, !out_of_records)) break;
-        if (!fetch && !out_of_records) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (fetch || out_of_records) continue;
             // one cell (gapped.rs:234-262)
-            const uint32_t w = my[(bi % STREAM_RING) * STREAM_BLOCK];
-            int32_t cx = ((int32_t)(w << 16) >> 16) + base_prev, cy = ((int32_t)w >> 16) + base_prev;
-            if (bi >= vlo) {
-                const bool e = bi < vhi;
+            const uint32_t slot = (bi % STREAM_RING) * STREAM_BLOCK;
+            uint32_t w = my[slot];
+            if (bi >= filled) {  // first visit of this band index: bring in its residue
+                fill_word(min(nb + 1, first_b + (uint32_t)STREAM_RING));
+                w = my[slot];
+            }
+            int32_t cx = ((int32_t)(w << 18) >> 18) + base_prev, cy = ((int32_t)(w << 4) >> 18) + base_prev;
+            if (bi >= vlo) {  // extension cell or sentinel of the previous row end
+                const bool e = bi - vlo < nvirt;
                 const int32_t v = ext_val - (int32_t)(bi - vlo) * ge;
                 cx = e ? v : MININT;
                 cy = e ? v - goe : MININT;
             }
-            const int32_t pos = pb + dir * (int32_t)bi;
-            if ((pos >> 2) != wcur) {
-                wcur = pos >> 2;
-                bw = *(const uint32_t*)(qal + (ptrdiff_t)(pos & ~3));
-            }
-            const uint32_t code = __byte_perm(bw, 0, (uint32_t)pos & 3u) & 15u;
-            const int32_t nxt = bi < nb ? cx + score_int8(srow, code) : 0;
+            const uint32_t code = w >> 28;
+            const int32_t nxt = bi < nb ? cx + smat[srow + code] : 0;
             const int32_t cell = max(max(sc, cy), gap_row);
             const bool alive = cell >= thr;
             if (!alive && bi == first_b) ++first_b;
             if (alive) last_b = bi;
             if (cell > best) { best = cell; best_b = bi; thr = cell - xdrop; }
             const int32_t open = cell - goe;
-            const int32_t ny = max(cy - ge, open);
             if (alive) gap_row = max(gap_row - ge, open);
-            my[(bi % STREAM_RING) * STREAM_BLOCK] = stream_enc(alive ? cell : MININT, alive ? ny : cy, base_cur);
+            const int32_t ex = alive ? cell - base_cur : STREAM_FLOOR;
+            const int32_t ey = max(alive ? max(cy - ge, open) : cy, floor_cur) - base_cur;
+            my[slot] = stream_pack(ex, ey, w);
             sc = nxt;
             if (++bi >= b_size) {
-                // end of row (gapped.rs:298-334)
+                // end of row (gapped.rs:298-334), as straight-line code
                 if (best > prev_best) best_a = ai + 1;
-                if (first_b >= b_size) {
+                const bool empty = first_b >= b_size;
+                const bool shrink = last_b + 1 < b_size;
+                const int32_t num = gap_row - thr;  // <= xdrop (gap_row never exceeds best)
+                uint32_t k = 0;
+                if (!shrink && b_size <= nb && num >= 0)
+                    k = min((uint32_t)(((uint64_t)(uint32_t)num * ge_magic) >> 32) + 1u, nb + 1 - b_size);
+                const uint32_t nbs = shrink ? last_b + 1 : b_size + k;
+                vlo = shrink ? nbs : b_size;
+                nvirt = nbs - vlo;
+                ext_val = gap_row;
+                b_size = nbs + (nbs <= nb ? 1u : 0u);  // + the MININT sentinel
+                ++ai;
+                const bool over = b_size - first_b > (uint32_t)STREAM_RING ||
+                                  rec_cells + (b_size - first_b) > STREAM_MAX_CELLS;
+                if (empty || ai >= m || over) {
+                    dp_fail = !empty && ai < m;
                     fetch = true;
                 } else {
-                    if (last_b + 1 < b_size) {
-                        b_size = last_b + 1;
-                        vlo = vhi = b_size;
-                    } else {
-                        uint32_t k = 0;
-                        if (b_size <= nb && gap_row >= thr) {
-                            const int32_t num = gap_row - thr;  // 0 <= num <= xdrop
-                            int32_t q = __float2int_rz((float)num * inv_ge);
-                            if ((q + 1) * ge <= num) ++q;
-                            else if (q * ge > num) --q;
-                            k = min((uint32_t)q + 1u, nb + 1 - b_size);
-                        }
-                        vlo = b_size; ext_val = gap_row;
-                        b_size += k;
-                        vhi = b_size;
-                    }
-                    if (b_size <= nb) ++b_size;
-                    if (b_size - first_b > (uint32_t)STREAM_RING || rec_cells + (b_size - first_b) > STREAM_MAX_CELLS) {
-                        dp_fail = true;
-                        fetch = true;
-                    } else if (++ai >= m) {
-                        fetch = true;
-                    } else {
-                        new_row();
-                    }
+                    new_row();
                 }
             }
         }
@@ -1076,23 +1105,17 @@ k_prelim_stream(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint64_
                     t = next_t;
                     if (t >= n) { out_of_records = true; break; }
                     next_t = atomicAdd(queue, 1u);
-                    const uint32_t i = idx[t];
-                    const uint32_t pair = hit_pair[i];
-                    const SeedHit h = hits[i];
-                    const UngBox u = ub[i];
-                    const uint32_t qi = pair / L.n, si = pair % L.n;
-                    qa = Q.len[qi];
-                    sa = L.len[si];
-                    plus = !(h.qs >> 31);
-                    uint32_t piv[4];
-                    prelim_pivot(plus, h.qs & 0x7fffffffu, h.s, u.s_start, u.s_end, qa, sa, (uint32_t)Q.lw[qi], piv);
-                    const int32_t xd = P->xdrop_gap < u.score ? P->xdrop_gap : u.score;
-                    xdrop = xd > goe ? xd : goe;
-                    qseq = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
-                    sseq = L.plus + L.plus_off[si] + 1;
+                    const uint4* gp = reinterpret_cast<const uint4*>(geo + t);
+                    const uint4 g0 = gp[0], g1 = gp[1], g2 = gp[2];
+                    qseq = (const uint8_t*)(((uint64_t)g0.y << 32) | g0.x);
+                    sseq = (const uint8_t*)(((uint64_t)g0.w << 32) | g0.z);
+                    qa = g1.x; sa = g1.y; qp = g1.z; sp = g1.w;
+                    tbq = g2.x; tbs = g2.y; xdrop = (int32_t)g2.z;
+                    plus = g2.w & 1u;
+                    a0_left = (uint8_t)(g2.w >> 8);
+                    a0_right = (uint8_t)(g2.w >> 16);
                     qal = (const uint8_t*)((uintptr_t)qseq & ~(uintptr_t)3);
                     r0 = (int32_t)(qseq - qal);
-                    qp = piv[0]; sp = piv[1]; tbq = piv[2]; tbs = piv[3];
                     rec_cells = 0;
                     abase = sseq; pb = r0; m = sp; nb = qp; dir = -1;
                     phase = 1;
@@ -1107,11 +1130,12 @@ k_prelim_stream(DevLib L, DevQueries Q, const DevParams* __restrict__ P, uint64_
                 const uint32_t J = jmax < nb ? jmax : nb;
                 if (J + 1 > (uint32_t)STREAM_RING) { dp_fail = true; continue; }
                 // initial row, computed on read: entries 1..J
-                b_size = J + 1; vlo = 1; vhi = J + 1; ext_val = -goe;
+                b_size = J + 1; vlo = 1; nvirt = J; ext_val = -goe;
                 first_b = 0; ai = 0; thr = -xdrop; base_cur = -xdrop;
-                my[0] = stream_enc(0, -goe, base_cur);
-                wcur = INT32_MIN;
-                a_nx = abase[0];
+                filled = 0;
+                fill_word(min(nb + 1, (uint32_t)STREAM_RING));  // index 0 holds a written cell
+                my[0] = stream_pack(0 - base_cur, -goe - base_cur, my[0]);
+                a_nx = dir < 0 ? a0_left : a0_right;
                 new_row();
                 fetch = false;
             }
@@ -1751,25 +1775,30 @@ cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams*
 }
 
 bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap) {
-    // int8 score rows: positive scores <= 127 and X + 1 <= 128 for the clamp of the negative ones
+    // 14-bit band values: live ones within X + max score of the row threshold, dead ones at
+    // FLOOR = -8192 (below every later threshold minus the best score)
     const int32_t xmax = std::max(xdrop_gap, gap_open + gap_extend);
-    if (gap_extend < 1 || gap_open < 0 || xmax > 127) return false;
+    if (gap_extend < 1 || gap_open < 0 || xmax > 8000) return false;
     for (int i = 0; i < 256; ++i)
         if (matrix256[i] > 127) return false;
     return true;
 }
 
+size_t prelim_geo_bytes() { return sizeof(PrelimGeo); }
+
 cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                  const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
-                                 PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells,
-                                 int sms, cudaStream_t st) {
+                                 void* geo, PrelimOut* out, uint32_t* wide, unsigned int* n_wide,
+                                 unsigned long long* cells, int sms, cudaStream_t st) {
     if (!n) return cudaSuccess;
+    k_prelim_prep<<<grid_for(n, 256, 8, sms), 256, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, (PrelimGeo*)geo);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
     const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
     const int grid = (int)(want < cap ? want : cap);
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
-    k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, out, wide, n_wide, n_wide + 1,
-                                                   cells);
+    k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1, cells);
     return cudaGetLastError();
 }
 

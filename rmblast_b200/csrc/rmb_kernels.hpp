@@ -22,13 +22,15 @@ cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams*
                           PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
                           cudaStream_t st);
 // Whether the thread-per-extension kernel's int16 band entries and int8 score rows hold the
-// parameters exactly (positive scores <= 127; X-drop and gap_open + gap_extend <= 127).
+// parameters exactly (scores <= 127; X-drop and gap_open + gap_extend <= 8000).
 // launch_prelim_stream uses n_wide[0] (overflow count) and n_wide[1] (record queue), both zeroed.
 bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap);
+// geo: n x prelim_geo_bytes() of scratch for the per-record geometry.
+size_t prelim_geo_bytes();
 cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                  const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
-                                 PrelimOut* out, uint32_t* wide, unsigned int* n_wide, unsigned long long* cells,
-                                 int sms, cudaStream_t st);
+                                 void* geo, PrelimOut* out, uint32_t* wide, unsigned int* n_wide,
+                                 unsigned long long* cells, int sms, cudaStream_t st);
 // Records `list` (the thread kernel's overflow), one warp per extension; dres holds 2 x n_list
 // int4.  Records that overflow the warp rings go to `wide` (count in n_wide[0]).
 cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_list,
