@@ -34,6 +34,11 @@ sys.path.insert(0, str(ROOT))
 
 FIELDS = "6 score perc_sub qseqid qstart qend sseqid sstart send"
 OPS_PER_CELL = 11  # int32 add/sub/max/compare per DP cell in search/gapped.rs:234-262
+# DRAM bytes (read + write) per ungapped record of k_prelim_stream, from one ncu capture of
+# `bench.py --scale 0.01` (profiles/k_prelim_stream_plain.md); the traffic is per record (the
+# 48-byte geometry read, the 28-byte result write, sequence words), so a launch's traffic is
+# this times its records
+PRELIM_STREAM_DRAM_BYTES_PER_RECORD = 61.6
 
 
 def parse():
@@ -231,7 +236,13 @@ def main():
     peak_int = api.int32_peak_tops(local)
     prelim_ms = c["gpu_ms_prelim"]
     so_cells = c["so_cells"]
-    achieved = so_cells * OPS_PER_CELL / (prelim_ms * 1e-3) / 1e12 if prelim_ms > 0 else 0.0
+    # the dominant kernel: k_prelim_stream (one launch per step), timed alone with CUDA events
+    main_ms, main_cells = c["gpu_ms_prelim_main"], c["so_cells_main"]
+    if main_ms <= 0:  # parameters outside the thread kernel's range: the warp kernel does it all
+        main_ms, main_cells = prelim_ms, so_cells
+    achieved = main_cells * OPS_PER_CELL / (main_ms * 1e-3) / 1e12 if main_ms > 0 else 0.0
+    traffic = (PRELIM_STREAM_DRAM_BYTES_PER_RECORD * c["prelim_dp"]
+               if PRELIM_STREAM_DRAM_BYTES_PER_RECORD and c["gpu_ms_prelim_main"] > 0 else None)
     value = bases * world / (ms_step * 1e-3) / 1e6
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
@@ -253,12 +264,17 @@ def main():
         "counts": {k: int(c[k]) for k in ("word_hits", "ungapped", "prelim_dp", "prelims", "tb_dp", "finals",
                                           "so_cells", "tb_cells")},
         "hsps": n_hsps,
-        "roofline": {"kernel": "k_prelim (score-only X-drop DP)", "bound": "int32", "achieved": achieved,
+        "roofline": {"kernel": "k_prelim_stream (score-only X-drop DP)", "bound": "int32", "achieved": achieved,
                      "peak": peak_int, "unit": "Tops/s", "frac": achieved / peak_int if peak_int else None,
-                     "traffic": None,
-                     "note": f"{OPS_PER_CELL} int32 ops per DP cell x cells / k_prelim event time; peak = "
-                             "rmb_probe_int32_peak measured in this run (hbm_gbs "
-                             f"{peaks.get('hbm_gbs')} GB/s of measured does not bound this kernel)"},
+                     "traffic": traffic, "kernel_ms": main_ms, "cells": main_cells,
+                     "hbm": {"achieved_gbs": traffic / (main_ms * 1e-3) / 1e9 if traffic else None,
+                             "peak_gbs": peaks.get("hbm_gbs"),
+                             "frac": (traffic / (main_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]
+                                      if traffic and peaks.get("hbm_gbs") else None)},
+                     "note": f"{OPS_PER_CELL} int32 ops per DP cell (the reference's cell step) x cells of the "
+                             "records k_prelim_stream completed / its event time; peak = rmb_probe_int32_peak "
+                             "(dependent int32 add/max throughput of this GPU) measured in this run; the kernel "
+                             "is bound by integer issue, not by HBM (hbm.frac) or tensor cores"},
         "gpu_launches": int(c["launches"]) * args.steps,
         "clocks": clk.summary(),
         "e2e": {"value": bases * world / (e2e_ms * 1e-3) / 1e6, "unit": "Mbp/s", "h2d_bytes_per_step": h2d,

@@ -87,6 +87,10 @@ typedef struct rmb_counters {
      * this library's own kernel launches (CUB scans/sorts/selects not counted) */
     double gpu_ms_scan, gpu_ms_ungapped, gpu_ms_dedup, gpu_ms_prelim, gpu_ms_traceback, gpu_ms_lookup;
     uint64_t launches;
+    /* the preliminary DP's main kernel alone: its device time and the DP cells of the records
+     * it completed (the rest of gpu_ms_prelim / so_cells is its fallbacks and setup) */
+    double gpu_ms_prelim_main;
+    uint64_t so_cells_main;
 } rmb_counters;
 
 /* Results of rmb_search_batch, in the reference's output order per query

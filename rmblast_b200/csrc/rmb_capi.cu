@@ -434,13 +434,18 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
         CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
         ev.start(st);
+        EvTimer ev_main;
         if (C.prelim_stream) {
             C.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
-            CK(launch_prelim_stream(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
-                                    C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p,
-                                    C.po.as<PrelimOut>(), C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
-                                    C.cells.as<unsigned long long>(), C.sms, st));
+            CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
+                                  C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p, C.sms,
+                                  st));
             ctr.launches += nu ? 1 : 0;
+            ev_main.start(st);
+            CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
+                                    C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
+                                    C.cells.as<unsigned long long>(), C.sms, st));
+            ev_main.stop(st);
         }
         else
             CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
@@ -450,9 +455,15 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         ev.stop(st);
         ctr.launches += nu ? 1 : 0;
         uint32_t nw = 0;
+        unsigned long long main_cells = 0;
         CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&main_cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctr.gpu_ms_prelim += ev.ms();
+        if (C.prelim_stream) {
+            ctr.gpu_ms_prelim_main += ev_main.ms();
+            ctr.so_cells_main += main_cells;
+        }
         DBuf* wide_list = &C.wide;
         if (nw && C.prelim_stream) {
             // records whose band window outgrew the thread ring: the warp kernel's 256-cell rings

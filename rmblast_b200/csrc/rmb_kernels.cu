@@ -883,15 +883,16 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
 //    neighbours, one word load) the first time a row reaches it; every index at or past that
 //    frontier is a computed entry, so only its residue bits are live.
 //  - The band window of a row (b_size - first_b cells) must fit the RING-entry ring; a record
-//    whose window grows past it, or whose cell count passes STREAM_MAX_CELLS, is listed for
-//    the warp kernel.
+//    whose window grows past it, or whose cell count passes the budget, is listed for the warp
+//    kernel.
 // ---------------------------------------------------------------------------------------
 constexpr int STREAM_RING = 64;
-// A record whose two extensions pass this many cells is handed to the warp kernel: one thread
-// takes ~0.1 us a cell, so the few extensions thousands of rows long would hold their warp
-// (and the end of the launch) for milliseconds, while a warp does one of their rows in a few
-// hundred cycles.
-constexpr uint32_t STREAM_MAX_CELLS = 8192;
+// A record whose two extensions pass `max_cells` cells is handed to the warp kernel: one thread
+// takes ~0.15 us a cell, so the few extensions thousands of rows long would hold their warp (and
+// the end of the launch) for milliseconds, while a warp does one of their rows in a few hundred
+// cycles.  The launch takes ~10 ns a record, so the host sets the budget to records / 750 (a
+// tail of ~2%), within [STREAM_MIN_CELLS, STREAM_MAX_CELLS].
+constexpr uint32_t STREAM_MIN_CELLS = 8192, STREAM_MAX_CELLS = 65536;
 constexpr int STREAM_BLOCK = 128;
 constexpr int STREAM_BLOCKS_PER_SM = 6;
 constexpr int32_t STREAM_FLOOR = -8192;
@@ -939,7 +940,7 @@ __global__ void __launch_bounds__(STREAM_BLOCK, STREAM_BLOCKS_PER_SM)
 k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __restrict__ geo,
                 PrelimOut* __restrict__ out,
                 uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide, unsigned int* __restrict__ queue,
-                unsigned long long* __restrict__ cells_total) {
+                unsigned long long* __restrict__ cells_total, uint32_t max_cells) {
     __shared__ uint32_t ring[STREAM_RING * STREAM_BLOCK];
     __shared__ int32_t smat[256];
     {
@@ -1057,7 +1058,7 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
                 b_size = nbs + (nbs <= nb ? 1u : 0u);  // + the MININT sentinel
                 ++ai;
                 const bool over = b_size - first_b > (uint32_t)STREAM_RING ||
-                                  rec_cells + (b_size - first_b) > STREAM_MAX_CELLS;
+                                  rec_cells + (b_size - first_b) > max_cells;
                 if (empty || ai >= m || over) {
                     dp_fail = !empty && ai < m;
                     fetch = true;
@@ -1786,19 +1787,26 @@ bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t 
 
 size_t prelim_geo_bytes() { return sizeof(PrelimGeo); }
 
-cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
-                                 const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
-                                 void* geo, PrelimOut* out, uint32_t* wide, unsigned int* n_wide,
-                                 unsigned long long* cells, int sms, cudaStream_t st) {
+cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                               const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                               void* geo, int sms, cudaStream_t st) {
     if (!n) return cudaSuccess;
     k_prelim_prep<<<grid_for(n, 256, 8, sms), 256, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, (PrelimGeo*)geo);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
+                                 unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
     const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
     const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
     const int grid = (int)(want < cap ? want : cap);
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
-    k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1, cells);
+    const uint64_t budget = n / 750;
+    const uint32_t max_cells = (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
+                                          : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
+    k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1, cells,
+                                                   max_cells);
     return cudaGetLastError();
 }
 

@@ -27,10 +27,11 @@ cudaError_t launch_prelim(const DevLib& L, const DevQueries& Q, const DevParams*
 bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap);
 // geo: n x prelim_geo_bytes() of scratch for the per-record geometry.
 size_t prelim_geo_bytes();
-cudaError_t launch_prelim_stream(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
-                                 const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
-                                 void* geo, PrelimOut* out, uint32_t* wide, unsigned int* n_wide,
-                                 unsigned long long* cells, int sms, cudaStream_t st);
+cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                               const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                               void* geo, int sms, cudaStream_t st);
+cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
+                                 unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st);
 // Records `list` (the thread kernel's overflow), one warp per extension; dres holds 2 x n_list
 // int4.  Records that overflow the warp rings go to `wide` (count in n_wide[0]).
 cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_list,
