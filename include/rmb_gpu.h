@@ -30,8 +30,11 @@ extern "C" {
 
 /* Search options: rmblast-lib/src/options.rs:12-67 SearchParams.  mask_level < 0 or
  * >= 100 disables masklevel (main.rs:560).  ungapped_cutoff < 0 derives it as the
- * reference does per query (search/ka_cutoff.rs:126).  dust must be 0 (query DUST
- * masking is not implemented in this library; the call fails with RMB_EINVAL). */
+ * reference does per query (search/ka_cutoff.rs:126).  dust = 1 masks low-complexity
+ * query intervals with NCBI symmetric DUST (window 64, level 20, linker 1; filter/dust.rs)
+ * before the lookup tables and the exact word extension, as the reference does
+ * (engine.rs:606-616); the masked copy is made on the device on the first search of a
+ * query set. */
 typedef struct rmb_params {
     int32_t gap_open, gap_extend, word_size;
     int32_t xdrop_ungap, xdrop_gap, xdrop_gap_final;

@@ -142,6 +142,7 @@ struct rmb_ctx {
     // per-batch device buffers
     DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     bool prelim_stream = false;  // thread-per-extension prelim kernel (else the warp kernel)
+    DBuf dust_scratch;           // per-thread DUST interval lists
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
     DevLib L{};
@@ -155,11 +156,15 @@ struct rmb_queries {
     std::vector<uint64_t> off;     // offset of query i in host / d_q / d_qrc
     std::vector<uint32_t> len;
     DBuf d_q, d_qrc, d_off, d_len;
+    DBuf d_qm, d_qmrc;   // DUST-masked queries and their reverse complements (made on first use)
+    bool dusted = false;
     void release() {
         d_q.release();
         d_qrc.release();
         d_off.release();
         d_len.release();
+        d_qm.release();
+        d_qmrc.release();
     }
 };
 
@@ -198,6 +203,36 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
     }
     cudaStream_t st = C.st;
     upload(C.lw, lw_all, st);
+    if (P.dust && !QH.dusted && nq) {
+        // DUST masking of the query set (engine.rs:606-616 -> filter/dust.rs:462), on the device;
+        // the masked copy feeds the lookup tables and the exact word extension only
+        auto t0 = std::chrono::steady_clock::now();
+        const size_t bytes = QH.host.size();
+        QH.d_qm.ensure(bytes);
+        QH.d_qmrc.ensure(bytes);
+        CK(cudaMemcpyAsync(QH.d_qm.p, QH.d_q.p, bytes, cudaMemcpyDeviceToDevice, st));
+        const uint32_t nt = dust_threads(nq, C.sms);
+        C.dust_scratch.ensure(dust_scratch_bytes(nt));
+        C.fails.ensure(16);
+        CK(cudaMemsetAsync(C.fails.p, 0, 4, st));
+        EvTimer ev;
+        ev.start(st);
+        CK(launch_dust(QH.d_q.as<uint8_t>(), QH.d_off.as<uint64_t>(), QH.d_len.as<uint32_t>(), nq,
+                       QH.d_qm.as<uint8_t>(), C.dust_scratch.p, nt, C.fails.as<unsigned int>(), st));
+        CK(launch_revcomp(QH.d_qm.as<uint8_t>(), QH.d_off.as<uint64_t>(), QH.d_len.as<uint32_t>(), nq,
+                          QH.d_qmrc.as<uint8_t>(), st));
+        ev.stop(st);
+        ctr.launches += 2;
+        unsigned int over = 0;
+        CK(cudaMemcpyAsync(&over, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (over) throw Fail(RMB_ELIMIT, "DUST interval list outgrew its fixed capacity");
+        ctr.gpu_ms_lookup += ev.ms();
+        ctr.ms_lookup += ms_since(t0);
+        QH.dusted = true;
+    }
+    const uint8_t* qmask = P.dust ? QH.d_qm.as<uint8_t>() : QH.d_q.as<uint8_t>();
+    const uint8_t* qmask_rc = P.dust ? QH.d_qmrc.as<uint8_t>() : QH.d_qrc.as<uint8_t>();
     // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table size.
     uint32_t qb = 0;
     while (qb < nq) {
@@ -237,7 +272,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         C.lut_vals.ensure(npos * 4);
         C.lut_keys2.ensure(npos * 4);
         C.lut_vals2.ensure(npos * 4);
-        DevQueries Q{QH.d_q.as<uint8_t>(),       QH.d_qrc.as<uint8_t>(),  QH.d_q.as<uint8_t>(),
+        DevQueries Q{QH.d_q.as<uint8_t>(),       QH.d_qrc.as<uint8_t>(),  qmask, qmask_rc,
                      QH.d_off.as<uint64_t>() + qb, QH.d_len.as<uint32_t>() + qb, C.pv.as<uint32_t>(),
                      C.pv_off.as<uint64_t>(),    C.cs.as<uint32_t>(),     C.cs_off.as<uint64_t>(),
                      C.cq.as<uint32_t>(),        C.cq_off.as<uint64_t>(), C.lw.as<int32_t>() + qb, nb};
@@ -733,7 +768,6 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         if (p.gap_open < 0 || p.gap_extend < 1) throw Fail(RMB_EINVAL, "gap costs out of range");
         if (p.xdrop_ungap < 0 || p.xdrop_gap < 0 || p.xdrop_gap_final < 0 || p.min_raw_gapped_score < 0)
             throw Fail(RMB_EINVAL, "negative X-drop or cutoff");
-        if (p.dust) throw Fail(RMB_EINVAL, "query DUST masking is not supported by this library (pass dust = 0)");
         if (p.schedule != 0) throw Fail(RMB_EINVAL, "only the FIFO schedule (0) is supported");
         if (p.kernels != 0 && p.kernels != 1) throw Fail(RMB_EINVAL, "kernels must be 0 (automatic) or 1 (warp prelim)");
         C = new rmb_ctx();
@@ -1110,7 +1144,7 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
                    &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->geo, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
-                   &C->tb_scratch};
+                   &C->tb_scratch, &C->dust_scratch};
     for (DBuf* b : all) b->release();
     if (C->st) cudaStreamDestroy(C->st);
     delete C;

@@ -31,7 +31,8 @@ struct DevLib {
 struct DevQueries {
     const uint8_t* q;
     const uint8_t* qrc;
-    const uint8_t* qmask;
+    const uint8_t* qmask;     // DUST-masked q (q itself when masking is off): table and exact word extension
+    const uint8_t* qmask_rc;  // reverse complement of qmask
     const uint64_t* off;
     const uint32_t* len;
     const uint32_t* pv;

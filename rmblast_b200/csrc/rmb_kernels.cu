@@ -22,6 +22,7 @@
 #include <cstdio>
 
 #include "rmb_device.cuh"
+#include "rmb_dust.cuh"
 #include "rmb_kernels.hpp"
 
 namespace rmb {
@@ -1931,8 +1932,8 @@ __global__ void k_lut_codes(DevQueries Q, int32_t ws, const uint64_t* __restrict
     const uint32_t qi = blockIdx.x;
     const uint32_t n = Q.len[qi];
     const int lw = Q.lw[qi];
-    const uint8_t* q = Q.q + Q.off[qi];      // sentinel-wrapped forward query
-    const uint8_t* r = Q.qrc + Q.off[qi];    // sentinel-wrapped reverse complement
+    const uint8_t* q = Q.qmask + Q.off[qi];     // sentinel-wrapped forward query (DUST-masked)
+    const uint8_t* r = Q.qmask_rc + Q.off[qi];  // its reverse complement
     const uint64_t base = pos_off[qi];
     const uint64_t cbase = Q.cs_off[qi];
     const uint32_t total = 2 * n + 1;
@@ -2061,6 +2062,33 @@ cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t
                            cudaStream_t st) {
     if (!nq) return cudaSuccess;
     k_revcomp<<<nq, 256, 0, st>>>(q, off, len, rc);
+    return cudaGetLastError();
+}
+
+// DUST masking (filter/dust.rs:462-489): one query per thread, each thread's perfect-interval
+// list in `scratch`; qm holds a copy of q and gets the masked bases (code 14).
+__global__ void __launch_bounds__(128) k_dust(const uint8_t* __restrict__ q, const uint64_t* __restrict__ off,
+                                              const uint32_t* __restrict__ len, uint32_t nq, uint8_t* __restrict__ qm,
+                                              DustPerfect* __restrict__ scratch, uint32_t nthreads,
+                                              unsigned int* __restrict__ overflow) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nthreads) return;
+    for (uint32_t i = tid; i < nq; i += nthreads) {
+        const uint64_t o = off[i] + 1;
+        if (!dust_query(q + o, len[i], qm + o, scratch + (uint64_t)tid * DUST_PERFECT_CAP)) atomicAdd(overflow, 1u);
+    }
+}
+
+uint32_t dust_threads(uint32_t nq, int sms) {
+    const uint32_t cap = (uint32_t)sms * 32u;
+    return nq < cap ? nq : cap;
+}
+size_t dust_scratch_bytes(uint32_t nthreads) { return (size_t)nthreads * DUST_PERFECT_CAP * sizeof(DustPerfect); }
+
+cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
+                        void* scratch, uint32_t nthreads, unsigned int* overflow, cudaStream_t st) {
+    if (!nq || !nthreads) return cudaSuccess;
+    k_dust<<<(nthreads + 127) / 128, 128, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow);
     return cudaGetLastError();
 }
 }  // namespace rmb

@@ -88,4 +88,10 @@ cudaError_t launch_lut_build(const DevQueries& Q, int32_t ws, uint32_t nq, const
 namespace rmb {
 cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* rc,
                            cudaStream_t st);
+// DUST masking of a query batch: qm must hold a copy of q; `scratch` holds
+// dust_scratch_bytes(nthreads); overflow counts queries whose interval list overflowed.
+uint32_t dust_threads(uint32_t nq, int sms);
+size_t dust_scratch_bytes(uint32_t nthreads);
+cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
+                        void* scratch, uint32_t nthreads, unsigned int* overflow, cudaStream_t st);
 }  // namespace rmb

@@ -24,7 +24,7 @@ def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str, kernels
     sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
                           xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
                           min_raw_gapped_score=p["min_raw_gapped_score"],
-                          complexity_adjust=bool(p.get("complexity_adjust", 0)), dust=False,
+                          complexity_adjust=bool(p.get("complexity_adjust", 0)), dust=bool(p.get("dust", 0)),
                           mask_level=p.get("mask_level", -1), kernels=kernels)
     return api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
 
@@ -41,6 +41,73 @@ def test_golden_nomask_nodust_through_c_abi():
     txt, _ = gpu_text(p, (G / "comparison.matrix").read_text(), "comparison.matrix", (G / "db.fa").read_text(),
                       (G / "query.fa").read_text(), O.RM_FIELDS)
     assert txt == (G / "expected_nomask_nodust.ncbi-2.17.1.tsv").read_text()
+
+
+DUST_GOLDENS = [
+    # name, db, query, matrix, parameters: the reference's CLI tests (rmblastn/tests/cli.rs)
+    ("rm_defaults", "db.fa", "query.fa", "comparison.matrix",
+     dict(O.RM_PARAMS, mask_level=80, complexity_adjust=1, dust=1)),
+    ("query_dash", "db.fa", "query_dash.fa", "comparison.matrix",
+     dict(O.RM_PARAMS, mask_level=80, complexity_adjust=1, dust=1)),
+    ("db_dash", "db_dash.fa", "query.fa", "comparison.matrix",
+     dict(O.RM_PARAMS, mask_level=80, complexity_adjust=1, dust=1)),
+    ("asym_freqs", "db.fa", "query.fa", "asym_freqs.matrix",
+     dict(O.RM_PARAMS, mask_level=101, complexity_adjust=1, dust=1)),
+    ("defaults", "db.fa", "query.fa", "comparison.matrix",
+     dict(gap_open=20, gap_extend=5, word_size=11, xdrop_ungap=20, xdrop_gap=30, xdrop_gap_final=100,
+          min_raw_gapped_score=0, mask_level=101, dust=1)),
+]
+
+
+@pytest.mark.parametrize("name,db,q,m,p", DUST_GOLDENS, ids=[c[0] for c in DUST_GOLDENS])
+def test_golden_with_dust_through_c_abi(name, db, q, m, p):
+    """The NCBI-2.17.1 goldens whose command lines mask the query with DUST (dust on is the
+    reference's default): the device masker, then the whole path, byte for byte."""
+    txt, _ = gpu_text(p, (G / m).read_text(), m, (G / db).read_text(), (G / q).read_text(), O.RM_FIELDS)
+    assert txt == (G / f"expected_{name}.ncbi-2.17.1.tsv").read_text()
+
+
+def with_low_complexity(seqs, seed):
+    """Plants microsatellites, poly-A tails, near-repeats and N runs: DUST's cases."""
+    rng = np.random.default_rng(seed)
+    units = [b"CA", b"A", b"AAAAT", b"GGC", b"TTAGGG", b"ACGTTGCA", b"AT"]
+    out = []
+    for s in seqs:
+        s = bytearray(s.tobytes())
+        for _ in range(max(1, len(s) // 3000)):
+            u = units[rng.integers(len(units))]
+            rep = bytearray(u * int(rng.integers(8, 120)))
+            for k in range(len(rep)):  # a few point mutations: low but not zero complexity
+                if rng.random() < 0.04:
+                    rep[k] = b"ACGTN"[rng.integers(5)]
+            at = int(rng.integers(0, max(1, len(s) - len(rep))))
+            s[at:at + len(rep)] = rep
+        out.append(np.frombuffer(bytes(s), dtype=np.uint8))
+    return out
+
+
+@pytest.mark.parametrize("ws", [7, 11, 14])
+def test_dust_on_synthetic_matches_oracle(ws):
+    qs, db, prm = synth.workload("small", scale=0.3)
+    p = dict(prm, **synth.RM_FLAGS)
+    p.update(dust=1, word_size=ws)
+    seqs = with_low_complexity([s for _, s in qs], 11 + ws)
+    qf = synth.to_fasta([n for n, _ in qs], seqs)
+    dbf = synth.to_fasta([n for n, _ in db], [s for _, s in db])
+    s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf)
+    recs = api.read_fasta(qf)
+    enc = [api.encode(x) for _, x in recs]
+    for stage in (0, 1):
+        got = s.stage(enc, stage)
+        want = O.stage_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, stage)
+        assert got.shape == want.shape, (stage, got.shape, want.shape)
+        assert np.array_equal(got, want), stage
+    res = s.search(enc, [n for n, _ in recs])
+    want_txt, _, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert res.tabular(FIELDS) == want_txt
+    # the planted runs are masked: without DUST the reference finds other seeds
+    unmasked = O.stage_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, dict(p, dust=0), 0)
+    assert unmasked.shape != want.shape or not np.array_equal(unmasked, want)
 
 
 def test_golden_db_dash_subjects_nomask():
@@ -162,10 +229,6 @@ def test_edge_cases():
     with pytest.raises(api.RmbError) as e:
         s.search([api.encode(b"A" * 1_999_800)])
     assert e.value.code == 5
-    # dust needs the query masker, which this library refuses rather than skipping
-    m = api.ScoreMatrix.from_text(mt, "comparison.matrix")
-    with pytest.raises(api.RmbError):
-        api.Searcher(api.SearchParams(dust=True), m, api.SubjectDb.from_fasta(db))
 
 
 def test_lookup_tables_match_reference_rules():
