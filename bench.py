@@ -51,10 +51,11 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the query set (tests/profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dust", action="store_true", help="mask the queries with DUST (the reference's default)")
     return ap.parse_args()
 
 
-def workload(name: str, scale: float, rank: int):
+def workload(name: str, scale: float, rank: int, dust: bool = False):
     from rmblast_b200 import synth
     seed = None if rank == 0 else 0x524D42 + 1000 + rank
     qs, db, prm = synth.workload(name, seed=seed, scale=scale)
@@ -62,6 +63,8 @@ def workload(name: str, scale: float, rank: int):
         # every rank shares the library of the workload; only the query set changes
         _, db, _ = synth.workload(name, scale=1e-9)
     p = dict(prm, **synth.RM_FLAGS)
+    if dust:
+        p["dust"] = 1
     return qs, db, p
 
 
@@ -134,7 +137,7 @@ def cpu_baseline(qs, db, p, budget_s: float):
 def reference_arm(args, rank, world):
     if rank != 0:
         return
-    qs, db, p = workload(args.workload, args.scale, 0)
+    qs, db, p = workload(args.workload, args.scale, 0, args.dust)
     # each step is a bounded sample of the same workload
     per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     vals = []
@@ -173,12 +176,12 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    qs, db, p = workload(args.workload, args.scale, rank)
+    qs, db, p = workload(args.workload, args.scale, rank, args.dust)
     m = api.ScoreMatrix.from_text(synth.MATRIX_TEXT, synth.MATRIX_NAME)
     sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
                           xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
                           min_raw_gapped_score=p["min_raw_gapped_score"], complexity_adjust=bool(p["complexity_adjust"]),
-                          mask_level=p["mask_level"], device=local)
+                          mask_level=p["mask_level"], dust=bool(p.get("dust", 0)), device=local)
     sdb = api.SubjectDb.from_records(db)
     s = api.Searcher(sp, m, sdb)
     enc = [api.encode(x) for _, x in qs]
@@ -254,13 +257,19 @@ def main():
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded genome/TE-library model)",
         "config": {"workload": args.workload, "queries_per_gpu": len(qs), "query_bp_per_gpu": bases,
                    "library": len(db), "library_bp": sdb.total_letters(), "word_size": p["word_size"],
-                   "flags": "gapopen 20 gapextend 5 complexity_adjust masklevel 80 dust no min_raw_gapped_score 200 "
-                            "xdrop_ungap 400 xdrop_gap 100 xdrop_gap_final 200",
+                   "flags": f"gapopen {p['gap_open']} gapextend {p['gap_extend']} "
+                            f"{'complexity_adjust ' if p.get('complexity_adjust') else ''}"
+                            f"masklevel {p['mask_level']} dust {'yes' if p.get('dust') else 'no'} "
+                            f"min_raw_gapped_score {p['min_raw_gapped_score']} xdrop_ungap {p['xdrop_ungap']} "
+                            f"xdrop_gap {p['xdrop_gap']} xdrop_gap_final {p['xdrop_gap_final']}",
                    "l2": "inputs larger than L2 (lookup tables and hit arrays are GBs per step)",
                    "parallelism": f"{world} independent ranks, queries sharded by rank"},
         "gcups": so_cells / (prelim_ms * 1e-3) / 1e9 if prelim_ms > 0 else None,
-        "stage_ms": {k: round(c[k], 3) for k in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
-                                                 "gpu_ms_prelim", "gpu_ms_traceback", "ms_host_2a", "ms_host_2b")},
+        "stage_ms": dict({k: round(c[k], 3) for k in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped",
+                                                      "gpu_ms_dedup", "gpu_ms_prelim", "gpu_ms_traceback",
+                                                      "ms_host_2a", "ms_host_2b")},
+                         # DUST runs once per uploaded query set: its time is the e2e search's
+                         gpu_ms_dust_e2e=round(r2.counters["gpu_ms_dust"], 3)),
         "counts": {k: int(c[k]) for k in ("word_hits", "ungapped", "prelim_dp", "prelims", "tb_dp", "finals",
                                           "so_cells", "tb_cells")},
         "hsps": n_hsps,

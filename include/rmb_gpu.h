@@ -94,6 +94,8 @@ typedef struct rmb_counters {
      * it completed (the rest of gpu_ms_prelim / so_cells is its fallbacks and setup) */
     double gpu_ms_prelim_main;
     uint64_t so_cells_main;
+    /* DUST masking of the query set (once per uploaded query set, when dust = 1) */
+    double gpu_ms_dust;
 } rmb_counters;
 
 /* Results of rmb_search_batch, in the reference's output order per query

@@ -227,7 +227,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         CK(cudaMemcpyAsync(&over, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (over) throw Fail(RMB_ELIMIT, "DUST interval list outgrew its fixed capacity");
-        ctr.gpu_ms_lookup += ev.ms();
+        ctr.gpu_ms_dust += ev.ms();
         ctr.ms_lookup += ms_since(t0);
         QH.dusted = true;
     }

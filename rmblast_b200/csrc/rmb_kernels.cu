@@ -2065,22 +2065,25 @@ cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t
     return cudaGetLastError();
 }
 
-// DUST masking (filter/dust.rs:462-489): one query per thread, each thread's perfect-interval
-// list in `scratch`; qm holds a copy of q and gets the masked bases (code 14).
-__global__ void __launch_bounds__(128) k_dust(const uint8_t* __restrict__ q, const uint64_t* __restrict__ off,
-                                              const uint32_t* __restrict__ len, uint32_t nq, uint8_t* __restrict__ qm,
-                                              DustPerfect* __restrict__ scratch, uint32_t nthreads,
-                                              unsigned int* __restrict__ overflow) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= nthreads) return;
-    for (uint32_t i = tid; i < nq; i += nthreads) {
+// DUST masking (filter/dust.rs:462-489).  A query's pass is one sequential chain of data-dependent
+// branches, so each query gets a warp of its own with one working lane: lanes of one warp on
+// different queries would diverge at nearly every step and run one after another.  Up to 32
+// such warps share an SM.  Each worker's perfect-interval list is in `scratch`; qm holds a copy
+// of q and gets the masked bases (code 14).
+__global__ void __launch_bounds__(32) k_dust(const uint8_t* __restrict__ q, const uint64_t* __restrict__ off,
+                                             const uint32_t* __restrict__ len, uint32_t nq, uint8_t* __restrict__ qm,
+                                             DustPerfect* __restrict__ scratch, uint32_t nworkers,
+                                             unsigned int* __restrict__ overflow) {
+    if (threadIdx.x != 0 || blockIdx.x >= nworkers) return;
+    for (uint32_t i = blockIdx.x; i < nq; i += nworkers) {
         const uint64_t o = off[i] + 1;
-        if (!dust_query(q + o, len[i], qm + o, scratch + (uint64_t)tid * DUST_PERFECT_CAP)) atomicAdd(overflow, 1u);
+        if (!dust_query(q + o, len[i], qm + o, scratch + (uint64_t)blockIdx.x * DUST_PERFECT_CAP))
+            atomicAdd(overflow, 1u);
     }
 }
 
 uint32_t dust_threads(uint32_t nq, int sms) {
-    const uint32_t cap = (uint32_t)sms * 32u;
+    const uint32_t cap = (uint32_t)sms * 32u;  // one working lane per warp, 32 single-warp blocks per SM
     return nq < cap ? nq : cap;
 }
 size_t dust_scratch_bytes(uint32_t nthreads) { return (size_t)nthreads * DUST_PERFECT_CAP * sizeof(DustPerfect); }
@@ -2088,7 +2091,7 @@ size_t dust_scratch_bytes(uint32_t nthreads) { return (size_t)nthreads * DUST_PE
 cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
                         void* scratch, uint32_t nthreads, unsigned int* overflow, cudaStream_t st) {
     if (!nq || !nthreads) return cudaSuccess;
-    k_dust<<<(nthreads + 127) / 128, 128, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow);
+    k_dust<<<nthreads, 32, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow);
     return cudaGetLastError();
 }
 }  // namespace rmb
