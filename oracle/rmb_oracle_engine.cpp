@@ -1205,16 +1205,174 @@ void sort_hit_list_order(std::vector<AlignResult>& res) {
     });
 }
 
+// main.rs:1018-1085 merge_chunk_prelims: NCBI's cross-chunk merge (plus strand only), called
+// once per chunk in chunk order; `split` is the chunk's start in the full query.
+void merge_chunk_prelims(std::vector<PrelimHsp>& acc, std::vector<PrelimHsp> add, uint32_t split) {
+    const uint32_t OVERLAP = 100;
+    const int64_t DIAG_CLOSE = 10;
+    auto order = [](const PrelimHsp& a, const PrelimHsp& b) {  // ScoreCompareHSPs, plus strand
+        if (a.score != b.score) return a.score > b.score;
+        if (a.s_start != b.s_start) return a.s_start < b.s_start;
+        if (a.s_end != b.s_end) return a.s_end > b.s_end;
+        if (a.q_start != b.q_start) return a.q_start < b.q_start;
+        return a.q_end > b.q_end;
+    };
+    std::vector<uint8_t> absorbed(add.size(), 0);
+    std::vector<size_t> ac, nc;
+    for (size_t i = 0; i < acc.size(); ++i)
+        if (acc[i].strand == PLUS && acc[i].q_end > split) ac.push_back(i);
+    std::stable_sort(ac.begin(), ac.end(), [&](size_t a, size_t b) { return order(acc[a], acc[b]); });
+    for (size_t j = 0; j < add.size(); ++j)
+        if (add[j].strand == PLUS && add[j].q_start < split + OVERLAP) nc.push_back(j);
+    std::stable_sort(nc.begin(), nc.end(), [&](size_t a, size_t b) { return order(add[a], add[b]); });
+    for (size_t i : ac) {
+        PrelimHsp& h1 = acc[i];
+        for (size_t j : nc) {
+            if (absorbed[j]) continue;
+            const PrelimHsp& h2 = add[j];
+            const int64_t end_diag = (int64_t)h1.q_end - (int64_t)h1.s_end;
+            const int64_t start_diag = (int64_t)h2.q_start - (int64_t)h2.s_start;
+            const int64_t dd = end_diag - start_diag;
+            if ((dd < 0 ? -dd : dd) >= DIAG_CLOSE) continue;
+            const bool start_in = h2.q_start >= h1.q_start && h2.q_start <= h1.q_end && h2.s_start >= h1.s_start &&
+                                  h2.s_start <= h1.s_end;
+            const bool end_in = h2.q_end >= h1.q_start && h2.q_end <= h1.q_end && h2.s_end >= h1.s_start &&
+                                h2.s_end <= h1.s_end;
+            if (!start_in && !end_in) continue;
+            const double density = (double)(h1.score + h2.score) /
+                                   (double)((h1.q_end - h1.q_start) + (h2.q_end - h2.q_start));
+            h1.q_start = std::min(h1.q_start, h2.q_start);
+            h1.s_start = std::min(h1.s_start, h2.s_start);
+            h1.q_end = std::max(h1.q_end, h2.q_end);
+            h1.s_end = std::max(h1.s_end, h2.s_end);
+            if (h2.score > h1.score) {
+                h1.q_seed = h2.q_seed;
+                h1.s_seed = h2.s_seed;
+                h1.score = h2.score;
+            }
+            h1.score = std::max(h1.score, (int32_t)(density * (double)(h1.q_end - h1.q_start)));
+            absorbed[j] = 1;
+        }
+    }
+    for (size_t j = 0; j < add.size(); ++j)
+        if (!absorbed[j]) acc.push_back(add[j]);
+}
+
+// main.rs:1236-1251 (SplitQuery_CalculateNumChunks + x_ComputeChunkRanges): chunk starts and
+// ends; a single chunk below 1,999,800 bp.
+std::vector<std::pair<uint32_t, uint32_t>> query_chunks(size_t qlen, int word_size) {
+    const size_t CHUNK = 1000000, OVERLAP = 100;
+    const size_t n = qlen / (CHUNK - OVERLAP);
+    std::vector<std::pair<uint32_t, uint32_t>> out;
+    if (n <= 1) {
+        out.push_back({0, (uint32_t)qlen});
+        return out;
+    }
+    size_t cs = (qlen + (n - 1) * OVERLAP) / n;
+    if (n < (cs > OVERLAP ? cs - OVERLAP : 0)) ++cs;
+    const size_t step = cs > OVERLAP ? cs - OVERLAP : 0;
+    for (size_t k = 0; k < n; ++k) {
+        const size_t b = k * step;
+        if (b >= qlen) break;
+        const size_t e = std::min(b + cs, qlen);
+        if (e - b < (size_t)word_size) break;
+        out.push_back({(uint32_t)b, (uint32_t)e});
+    }
+    return out;
+}
+
+// main.rs:1281-1400 multi-chunk search of one query: DUST on the whole query (with the chunked
+// off-by-one, engine.rs:697-707 / dust.rs:614-630), Phase 1 + 2a per chunk against every
+// subject (engine.rs:1775-1848 search_phase2a), the cross-chunk merge per subject, then
+// Phase 2b against the full query (engine.rs:1418-1431).
+static std::vector<std::vector<AlignResult>> search_chunked(const std::vector<uint8_t>& query, const std::string& qid,
+                                                           const std::vector<Subject>& db, const Params& p,
+                                                           const Matrix& m, int threads, Counters* counters) {
+    const size_t qlen = query.size() - 2;
+    std::vector<uint8_t> masked = query;
+    if (p.dust) {
+        auto iv = dust_mask(masked);
+        for (auto& [s, e] : iv)
+            if (e + 1 < qlen) masked[e + 2] = 14;
+    }
+    Params pc = p;
+    pc.dust = false;  // chunk tables come from the masked full query
+    std::vector<std::vector<PrelimHsp>> acc(db.size());
+    const auto chunks = query_chunks(qlen, p.word_size);
+    auto run_parallel = [&](auto&& body) {
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (;;) {
+                size_t i = next.fetch_add(1);
+                if (i >= db.size()) break;
+                body(i);
+            }
+        };
+        int nt = std::max(1, threads);
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+        worker();
+        for (auto& x : th) x.join();
+    };
+    for (size_t k = 0; k < chunks.size(); ++k) {
+        const uint32_t b = chunks[k].first, e = chunks[k].second;
+        std::vector<uint8_t> chunk, mchunk;
+        chunk.push_back(query.front());
+        chunk.insert(chunk.end(), query.begin() + 1 + b, query.begin() + 1 + e);
+        chunk.push_back(query.back());
+        mchunk.push_back(masked.front());
+        mchunk.insert(mchunk.end(), masked.begin() + 1 + b, masked.begin() + 1 + e);
+        mchunk.push_back(masked.back());
+        QueryLookup ql = build_query_lookup(mchunk, pc);
+        ql.query_rc = revcomp(chunk.data(), chunk.size());
+        std::vector<std::vector<PrelimHsp>> pre(db.size());
+        run_parallel([&](size_t i) {
+            const uint32_t q_len = (uint32_t)chunk.size() - 2, s_len = db[i].len();
+            if (q_len < (uint32_t)p.word_size || s_len < (uint32_t)p.word_size) return;
+            std::vector<UngappedRecord> ung;
+            collect_ungapped(chunk, ql, db[i], pc, m, nullptr, ung, nullptr);
+            sort_ungapped(ung, q_len, s_len);
+            if (ung.empty()) return;
+            pre[i] = phase2a(chunk, ql.query_rc, db[i], ung, pc, m, ql.lut.lut_word_length, nullptr);
+            for (auto& h : pre[i]) {
+                h.q_start += b;
+                h.q_end += b;
+                h.q_seed += b;
+            }
+        });
+        for (size_t i = 0; i < db.size(); ++i) {
+            if (k == 0) acc[i] = std::move(pre[i]);
+            else merge_chunk_prelims(acc[i], std::move(pre[i]), b);
+        }
+    }
+    const std::vector<uint8_t> qrc = revcomp(query.data(), query.size());
+    std::vector<std::vector<AlignResult>> per(db.size());
+    run_parallel([&](size_t i) {
+        if (acc[i].empty()) return;
+        per[i] = phase2b(query, qrc, qid, db[i], std::move(acc[i]), p, m, nullptr);
+        for (auto& r : per[i]) { r.hsp.q_len = (uint32_t)qlen; r.oid = (uint32_t)i; }
+    });
+    return per;
+}
+
 std::vector<AlignResult> search_query(const std::vector<uint8_t>& query, const std::string& qid,
                                       const std::vector<Subject>& db, const Params& p0, const Matrix& m, int threads,
                                       Counters* counters) {
     size_t qlen = query.size() - 2;
-    if (qlen >= 1999800) throw std::runtime_error("queries of 1,999,800 bp or longer take the chunked path");
     uint64_t total = 0;
     for (auto& s : db) total += s.len();
     uint64_t avg = db.empty() ? 0 : total / db.size();
     Params p = p0;
     p.ungapped_cutoff = ungapped_cutoff(p.matrix_name, p.gap_open, p.gap_extend, p.min_raw_gapped_score, qlen, avg);
+    if (query_chunks(qlen, p.word_size).size() > 1) {
+        auto per = search_chunked(query, qid, db, p, m, threads, counters);
+        std::vector<AlignResult> res;
+        for (auto& v : per)
+            for (auto& r : v) res.push_back(std::move(r));
+        apply_mask_level(res, p.mask_level);
+        sort_hit_list_order(res);
+        return res;
+    }
     QueryLookup ql = build_query_lookup(query, p);
     std::vector<std::vector<AlignResult>> per(db.size());
     std::vector<Counters> ctrs(threads > 0 ? threads : 1);

@@ -68,3 +68,20 @@ def test_oracle_matches_chr22_stage_goldens(stage, gold):
     want = (REF / "rmblast-lib/tests/data" / gold).read_text()
     assert got.count("\n") == 247629
     assert got == want
+
+
+@pytest.mark.skipif(not (REF / "tests/data/chr22.fa").exists(), reason="reference tree not mounted")
+def test_oracle_chunked_path_matches_chr22_golden(tmp_path):
+    """The multi-chunk path (a 3 Mb query: three chunks, DUST on the whole query, cross-chunk
+    merge, full-query traceback) against NCBI 2.17.1: rmblastn/tests/cli.rs:246-274."""
+    seq = "".join(ln.strip() for ln in open(REF / "tests/data/chr22.fa") if not ln.startswith(">"))
+    sl = seq[30_000_000:33_000_000]
+    q = tmp_path / "chr22_30M_33M.fa"
+    q.write_text(">chr22_30M_33M\n" + "".join(sl[i:i + 60] + "\n" for i in range(0, len(sl), 60)))
+    got = O.run_cli(["--db", str(G / "db.fa"), "--query", str(q), "--matrix", str(G / "comparison.matrix"),
+                     "--gapopen", "20", "--gapextend", "5", "--word-size", "7", "--min-raw-gapped-score", "200",
+                     "--mask-level", "80", "--num-threads", "8",
+                     "--outfmt", "6 score qseqid qstart qend sstrand sseqid sstart send"])
+    want = (REF / "rmblastn/tests/data/expected_chr22_30M-33M_ws7.ncbi-2.17.1.tsv").read_text()
+    assert got.count("\n") == 4236
+    assert got == want
