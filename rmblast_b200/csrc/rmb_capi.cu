@@ -184,9 +184,53 @@ struct Taps {
     std::vector<uint32_t>* tracebacks = nullptr;  // strand, status, score, q0, q1, s0, s1, n_ops, ops hash
 };
 
-// One search over resident queries: per-query hits in the reference's order.
-void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hits, rmb_counters& ctr,
-                Taps* taps) {
+// DUST masking of a query set (engine.rs:606-616 -> filter/dust.rs:462), on the device: the
+// masked copy and its reverse complement feed the lookup tables and the exact word extension
+// only.  `compat` is the multi-chunk path's variant (engine.rs:697-707).
+void mask_queries(rmb_ctx& C, rmb_queries& QH, bool compat, rmb_counters& ctr) {
+    cudaStream_t st = C.st;
+    const uint32_t nq = QH.n;
+    auto t0 = std::chrono::steady_clock::now();
+    const size_t bytes = QH.host.size();
+    QH.d_qm.ensure(bytes);
+    QH.d_qmrc.ensure(bytes);
+    CK(cudaMemcpyAsync(QH.d_qm.p, QH.d_q.p, bytes, cudaMemcpyDeviceToDevice, st));
+    const uint32_t nt = dust_threads(nq, C.sms);
+    C.dust_scratch.ensure(dust_scratch_bytes(nt));
+    C.fails.ensure(16);
+    CK(cudaMemsetAsync(C.fails.p, 0, 4, st));
+    EvTimer ev;
+    ev.start(st);
+    CK(launch_dust(QH.d_q.as<uint8_t>(), QH.d_off.as<uint64_t>(), QH.d_len.as<uint32_t>(), nq, QH.d_qm.as<uint8_t>(),
+                   C.dust_scratch.p, nt, C.fails.as<unsigned int>(), compat, st));
+    CK(launch_revcomp(QH.d_qm.as<uint8_t>(), QH.d_off.as<uint64_t>(), QH.d_len.as<uint32_t>(), nq,
+                      QH.d_qmrc.as<uint8_t>(), st));
+    ev.stop(st);
+    ctr.launches += 2;
+    unsigned int over = 0;
+    CK(cudaMemcpyAsync(&over, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (over) throw Fail(RMB_ELIMIT, "DUST interval list outgrew its fixed capacity");
+    ctr.gpu_ms_dust += ev.ms();
+    ctr.ms_lookup += ms_since(t0);
+    QH.dusted = true;
+}
+
+// One (query, subject) pair's Phase 2a output, in the reference's order (purge order).
+struct PairPrelims {
+    uint32_t q, s;
+    std::vector<Prelim> p;
+};
+
+bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
+                  const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
+                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps);
+
+// The search of a set of single-chunk queries.  ucut_override: per-query ungapped cutoffs (the
+// chunks of a long query take their parent's).  collect: stop after Phase 2a and hand over the
+// prelims of every pair instead of aligning them.
+void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hits, rmb_counters& ctr, Taps* taps,
+              const std::vector<int32_t>* ucut_override, std::vector<PairPrelims>* collect) {
     const rmb_params& P = C.p;
     const uint32_t ns = (uint32_t)C.ids.size();
     const uint32_t nq = QH.n;
@@ -196,41 +240,15 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
     for (uint32_t i = 0; i < nq; ++i) {
         if (qlen[i] >= 1999800u) throw Fail(RMB_ELIMIT, "queries of 1,999,800 bp or more take the chunked path");
         const uint64_t avg = ns ? C.total_letters / ns : 0;
-        ucut[i] = P.ungapped_cutoff >= 0 ? P.ungapped_cutoff
+        ucut[i] = ucut_override ? (*ucut_override)[i]
+                  : P.ungapped_cutoff >= 0 ? P.ungapped_cutoff
                                           : ungapped_cutoff_for(C.matrix_name, P.gap_open, P.gap_extend,
                                                                 P.min_raw_gapped_score, qlen[i], avg);
         lw_all[i] = choose_lut_width(P.word_size, 2ull * qlen[i]);
     }
     cudaStream_t st = C.st;
     upload(C.lw, lw_all, st);
-    if (P.dust && !QH.dusted && nq) {
-        // DUST masking of the query set (engine.rs:606-616 -> filter/dust.rs:462), on the device;
-        // the masked copy feeds the lookup tables and the exact word extension only
-        auto t0 = std::chrono::steady_clock::now();
-        const size_t bytes = QH.host.size();
-        QH.d_qm.ensure(bytes);
-        QH.d_qmrc.ensure(bytes);
-        CK(cudaMemcpyAsync(QH.d_qm.p, QH.d_q.p, bytes, cudaMemcpyDeviceToDevice, st));
-        const uint32_t nt = dust_threads(nq, C.sms);
-        C.dust_scratch.ensure(dust_scratch_bytes(nt));
-        C.fails.ensure(16);
-        CK(cudaMemsetAsync(C.fails.p, 0, 4, st));
-        EvTimer ev;
-        ev.start(st);
-        CK(launch_dust(QH.d_q.as<uint8_t>(), QH.d_off.as<uint64_t>(), QH.d_len.as<uint32_t>(), nq,
-                       QH.d_qm.as<uint8_t>(), C.dust_scratch.p, nt, C.fails.as<unsigned int>(), st));
-        CK(launch_revcomp(QH.d_qm.as<uint8_t>(), QH.d_off.as<uint64_t>(), QH.d_len.as<uint32_t>(), nq,
-                          QH.d_qmrc.as<uint8_t>(), st));
-        ev.stop(st);
-        ctr.launches += 2;
-        unsigned int over = 0;
-        CK(cudaMemcpyAsync(&over, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (over) throw Fail(RMB_ELIMIT, "DUST interval list outgrew its fixed capacity");
-        ctr.gpu_ms_dust += ev.ms();
-        ctr.ms_lookup += ms_since(t0);
-        QH.dusted = true;
-    }
+    if (P.dust && !QH.dusted && nq) mask_queries(C, QH, false, ctr);
     const uint8_t* qmask = P.dust ? QH.d_qm.as<uint8_t>() : QH.d_q.as<uint8_t>();
     const uint8_t* qmask_rc = P.dust ? QH.d_qmrc.as<uint8_t>() : QH.d_qrc.as<uint8_t>();
     // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table size.
@@ -593,7 +611,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         parallel_for(np, [&](size_t k) {
             const uint32_t qa = hqlen[pair_ids[k] / ns], sa = C.slen[pair_ids[k] % ns];
             prelims[k] = phase2a_filter(per_pair[k], qa, sa);
-            sort_prelims_for_traceback(prelims[k], qa, sa);
+            if (!collect) sort_prelims_for_traceback(prelims[k], qa, sa);
         });
         per_pair.clear();
         uint64_t n_pre = 0;
@@ -610,9 +628,46 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
             continue;
         }
         ctr.ms_host_2a += ms_since(t0);
+        if (collect) {
+            for (size_t k = 0; k < np; ++k)
+                collect->push_back(PairPrelims{qb + pair_ids[k] / ns, pair_ids[k] % ns, std::move(prelims[k])});
+            qb = qe;
+            continue;
+        }
 
-        // ---- traceback DP of every prelim (GPU), with retries for scratch overflow
+        // ---- traceback DP and host Phase 2b of every prelim
+        if (traceback_2b(C, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps)) {
+            qb = qe;
+            continue;
+        }
         t0 = std::chrono::steady_clock::now();
+        parallel_for(nb, [&](size_t i) {
+            auto& v = out_hits[qb + i];
+            apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
+            sort_hit_list_order(v, C.ids);
+        });
+        for (uint32_t i = 0; i < nb; ++i) ctr.finals += out_hits[qb + i].size();
+        ctr.ms_host_2b += ms_since(t0);
+        qb = qe;
+    }
+}
+
+// Traceback DP on the device and the host Phase 2b (engine.rs:1438-1762) of the prelims of
+// (query, subject) pairs; pair = local query * n_subjects + subject over the queries of Q, whose
+// lengths are hqlen and host copies qhost(local).  Hits go to out[local query].  Returns true
+// when the traceback stage tap took the results instead.
+bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
+                  const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
+                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps) {
+    const uint32_t ns = (uint32_t)C.ids.size();
+    const size_t np = pair_ids.size();
+    cudaStream_t st = C.st;
+    unsigned long long cells = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    {
+        // ---- traceback DP of every prelim (GPU), with retries for scratch overflow
+        uint64_t n_pre = 0;
+        for (auto& v : prelims) n_pre += v.size();
         std::vector<TbIn> tin;
         tin.reserve(n_pre);
         std::vector<uint64_t> pre_off(np + 1, 0);
@@ -705,8 +760,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
                                           ok ? r.q1 : 0u, ok ? r.s0 : 0u, ok ? r.s1 : 0u,
                                           ok ? (uint32_t)r.script.size() : 0u, ok ? h : 2166136261u});
             }
-            qb = qe;
-            continue;
+            return true;
         }
 
         // ---- host Phase 2b per pair, then per query
@@ -727,21 +781,16 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
         });
         for (size_t k = 0; k < np; ++k) {
             const uint32_t qi = pair_ids[k] / ns;
-            auto& dst = out_hits[qb + qi];
+            auto& dst = out[qi];
             for (auto& h : pair_hits[k]) {
                 h.q_len = hqlen[qi];
                 dst.push_back(std::move(h));
             }
         }
-        parallel_for(nb, [&](size_t i) {
-            auto& v = out_hits[qb + i];
-            apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
-            sort_hit_list_order(v, C.ids);
-        });
-        for (uint32_t i = 0; i < nb; ++i) ctr.finals += out_hits[qb + i].size();
         ctr.ms_host_2b += ms_since(t0);
-        qb = qe;
     }
+    (void)nb;
+    return false;
 }
 
 int fail_out(const std::exception& e, char* err, size_t errlen, int code) {
@@ -931,6 +980,238 @@ static rmb_queries* make_queries(rmb_ctx* C, uint32_t nq, const uint8_t* const* 
         throw;
     }
 }
+
+}  // extern "C"
+
+namespace {
+
+struct QueriesDeleter {
+    void operator()(rmb_queries* H) const {
+        if (!H) return;
+        H->release();
+        delete H;
+    }
+};
+using QueriesPtr = std::unique_ptr<rmb_queries, QueriesDeleter>;
+
+// main.rs:1236-1251 (NCBI SplitQuery_CalculateNumChunks + x_ComputeChunkRanges): the chunks
+// [start, end) of a query; one chunk below 1,999,800 bp.
+std::vector<std::pair<uint32_t, uint32_t>> query_chunks(uint64_t qlen, int word_size) {
+    const uint64_t CHUNK = 1000000, OVERLAP = 100;
+    const uint64_t n = qlen / (CHUNK - OVERLAP);
+    std::vector<std::pair<uint32_t, uint32_t>> out;
+    if (n <= 1) {
+        out.push_back({0, (uint32_t)qlen});
+        return out;
+    }
+    uint64_t cs = (qlen + (n - 1) * OVERLAP) / n;
+    if (n < (cs > OVERLAP ? cs - OVERLAP : 0)) ++cs;
+    const uint64_t step = cs > OVERLAP ? cs - OVERLAP : 0;
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint64_t b = k * step;
+        if (b >= qlen) break;
+        const uint64_t e = std::min(b + cs, qlen);
+        if (e - b < (uint64_t)word_size) break;
+        out.push_back({(uint32_t)b, (uint32_t)e});
+    }
+    return out;
+}
+
+// main.rs:1018-1085 merge_chunk_prelims (NCBI Blast_HSPListsMerge): a chunk's prelims, in full-
+// query coordinates, into the ones accumulated so far for the same subject; plus strand only.
+// Each accumulated candidate, best first, absorbs every close new one whose start or end lies in
+// its box, growing as it does; the merged score is the density of the two over the merged length
+// (f64, as the reference) or the better score.
+void merge_chunk_prelims(std::vector<Prelim>& acc, std::vector<Prelim>& add, uint32_t split) {
+    const uint32_t OVERLAP = 100;
+    const int64_t DIAG_CLOSE = 10;
+    auto order = [](const Prelim& a, const Prelim& b) {  // ScoreCompareHSPs for plus-strand HSPs
+        if (a.score != b.score) return a.score > b.score;
+        if (a.s_start != b.s_start) return a.s_start < b.s_start;
+        if (a.s_end != b.s_end) return a.s_end > b.s_end;
+        if (a.q_start != b.q_start) return a.q_start < b.q_start;
+        return a.q_end > b.q_end;
+    };
+    std::vector<uint8_t> absorbed(add.size(), 0);
+    std::vector<size_t> ac, nc;
+    for (size_t i = 0; i < acc.size(); ++i)
+        if (acc[i].strand == 0 && acc[i].q_end > split) ac.push_back(i);
+    std::stable_sort(ac.begin(), ac.end(), [&](size_t a, size_t b) { return order(acc[a], acc[b]); });
+    for (size_t j = 0; j < add.size(); ++j)
+        if (add[j].strand == 0 && add[j].q_start < split + OVERLAP) nc.push_back(j);
+    std::stable_sort(nc.begin(), nc.end(), [&](size_t a, size_t b) { return order(add[a], add[b]); });
+    for (size_t i : ac) {
+        Prelim& h1 = acc[i];
+        for (size_t j : nc) {
+            if (absorbed[j]) continue;
+            const Prelim& h2 = add[j];
+            const int64_t dd = ((int64_t)h1.q_end - (int64_t)h1.s_end) - ((int64_t)h2.q_start - (int64_t)h2.s_start);
+            if ((dd < 0 ? -dd : dd) >= DIAG_CLOSE) continue;
+            const bool start_in = h2.q_start >= h1.q_start && h2.q_start <= h1.q_end && h2.s_start >= h1.s_start &&
+                                  h2.s_start <= h1.s_end;
+            const bool end_in = h2.q_end >= h1.q_start && h2.q_end <= h1.q_end && h2.s_end >= h1.s_start &&
+                                h2.s_end <= h1.s_end;
+            if (!start_in && !end_in) continue;
+            const double density =
+                (double)(h1.score + h2.score) / (double)((h1.q_end - h1.q_start) + (h2.q_end - h2.q_start));
+            h1.q_start = std::min(h1.q_start, h2.q_start);
+            h1.s_start = std::min(h1.s_start, h2.s_start);
+            h1.q_end = std::max(h1.q_end, h2.q_end);
+            h1.s_end = std::max(h1.s_end, h2.s_end);
+            if (h2.score > h1.score) {
+                h1.q_seed = h2.q_seed;
+                h1.s_seed = h2.s_seed;
+                h1.score = h2.score;
+            }
+            h1.score = std::max(h1.score, (int32_t)(density * (double)(h1.q_end - h1.q_start)));
+            absorbed[j] = 1;
+        }
+    }
+    for (size_t j = 0; j < add.size(); ++j)
+        if (!absorbed[j]) acc.push_back(add[j]);
+}
+
+QueriesPtr subset_queries(rmb_ctx& C, const std::vector<const uint8_t*>& ptr, const std::vector<uint32_t>& len) {
+    return QueriesPtr(make_queries(&C, (uint32_t)ptr.size(), ptr.data(), len.data()));
+}
+
+// One search: single-chunk queries through run_core; queries of 1,999,800 bp or more through the
+// reference's multi-chunk pipeline (main.rs:1236-1400): DUST on the whole query with the chunked
+// off-by-one, Phase 1 + 2a per chunk (engine.rs:1775-1848), the cross-chunk merge per subject in
+// chunk order, then Phase 2b against the full query (engine.rs:1418-1431).
+void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hits, rmb_counters& ctr,
+                Taps* taps) {
+    const rmb_params& P = C.p;
+    const uint32_t nq = QH.n, ns = (uint32_t)C.ids.size();
+    std::vector<uint32_t> longq, shortq;
+    for (uint32_t i = 0; i < nq; ++i) (query_chunks(QH.len[i], P.word_size).size() > 1 ? longq : shortq).push_back(i);
+    if (longq.empty()) {
+        run_core(C, QH, out_hits, ctr, taps, nullptr, nullptr);
+        return;
+    }
+    if (taps) throw Fail(RMB_EINVAL, "stage taps take single-chunk queries (under 1,999,800 bp) only");
+    for (uint32_t i : longq)
+        if (QH.len[i] > 0x7fffffffu) throw Fail(RMB_ELIMIT, "queries of 2^31 bp or more are not supported");
+    out_hits.assign(nq, {});
+    auto hostq = [&](uint32_t i) { return (const uint8_t*)QH.host.data() + QH.off[i]; };
+    if (!shortq.empty()) {
+        std::vector<const uint8_t*> ptr;
+        std::vector<uint32_t> len;
+        for (uint32_t i : shortq) { ptr.push_back(hostq(i)); len.push_back(QH.len[i]); }
+        QueriesPtr QS = subset_queries(C, ptr, len);
+        std::vector<std::vector<Hit>> hs;
+        run_core(C, *QS, hs, ctr, nullptr, nullptr, nullptr);
+        for (size_t k = 0; k < shortq.size(); ++k) out_hits[shortq[k]] = std::move(hs[k]);
+    }
+    // the long queries in full, DUST-masked as one piece
+    std::vector<const uint8_t*> lptr;
+    std::vector<uint32_t> llen;
+    for (uint32_t i : longq) { lptr.push_back(hostq(i)); llen.push_back(QH.len[i]); }
+    QueriesPtr QL = subset_queries(C, lptr, llen);
+    const uint32_t nl = QL->n;
+    std::vector<uint8_t> lmask = QL->host;
+    if (P.dust) {
+        mask_queries(C, *QL, true, ctr);
+        CK(cudaMemcpy(lmask.data(), QL->d_qm.p, lmask.size(), cudaMemcpyDeviceToHost));
+    }
+    // their chunks as queries of their own: unmasked bytes for the extensions, masked bytes for the
+    // tables and the exact word extension; the ungapped cutoff of the whole query
+    const uint64_t avg = ns ? C.total_letters / ns : 0;
+    std::vector<std::vector<uint8_t>> cbytes, cmask;
+    std::vector<uint32_t> cparent, cstart, clen;
+    std::vector<int32_t> cucut;
+    for (uint32_t j = 0; j < nl; ++j) {
+        const uint8_t* q = QL->host.data() + QL->off[j];
+        const uint8_t* qm = lmask.data() + QL->off[j];
+        const uint32_t qa = QL->len[j];
+        const int32_t uc = P.ungapped_cutoff >= 0 ? P.ungapped_cutoff
+                                                  : ungapped_cutoff_for(C.matrix_name, P.gap_open, P.gap_extend,
+                                                                        P.min_raw_gapped_score, qa, avg);
+        for (auto [b, e] : query_chunks(qa, P.word_size)) {
+            std::vector<uint8_t> c, m;
+            c.push_back(q[0]);
+            c.insert(c.end(), q + 1 + b, q + 1 + e);
+            c.push_back(q[qa + 1]);
+            m.push_back(qm[0]);
+            m.insert(m.end(), qm + 1 + b, qm + 1 + e);
+            m.push_back(qm[qa + 1]);
+            cbytes.push_back(std::move(c));
+            cmask.push_back(std::move(m));
+            cparent.push_back(j);
+            cstart.push_back(b);
+            clen.push_back(e - b);
+            cucut.push_back(uc);
+        }
+    }
+    std::vector<const uint8_t*> cptr;
+    for (auto& c : cbytes) cptr.push_back(c.data());
+    QueriesPtr CH = subset_queries(C, cptr, clen);
+    if (P.dust) {
+        std::vector<uint8_t> hm(CH->host.size());
+        for (size_t k = 0; k < cmask.size(); ++k) memcpy(hm.data() + CH->off[k], cmask[k].data(), cmask[k].size());
+        CH->d_qm.ensure(hm.size());
+        CH->d_qmrc.ensure(hm.size());
+        CK(cudaMemcpy(CH->d_qm.p, hm.data(), hm.size(), cudaMemcpyHostToDevice));
+        CK(launch_revcomp(CH->d_qm.as<uint8_t>(), CH->d_off.as<uint64_t>(), CH->d_len.as<uint32_t>(), CH->n,
+                          CH->d_qmrc.as<uint8_t>(), C.st));
+        CK(cudaStreamSynchronize(C.st));
+        ctr.launches += 1;
+        CH->dusted = true;
+    }
+    std::vector<PairPrelims> col;
+    std::vector<std::vector<Hit>> unused;
+    run_core(C, *CH, unused, ctr, nullptr, &cucut, &col);
+    // the merge, per (query, subject) in chunk order; prelims to full-query coordinates
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::vector<size_t>> by_pair((size_t)nl * ns);
+    for (size_t k = 0; k < col.size(); ++k) by_pair[(size_t)cparent[col[k].q] * ns + col[k].s].push_back(k);
+    std::vector<uint32_t> pair_ids;
+    std::vector<std::vector<Prelim>> prelims;
+    for (size_t pr = 0; pr < by_pair.size(); ++pr) {
+        auto& ks = by_pair[pr];
+        if (ks.empty()) continue;
+        std::stable_sort(ks.begin(), ks.end(), [&](size_t a, size_t b) { return col[a].q < col[b].q; });
+        std::vector<Prelim> acc;
+        bool first = true;
+        for (size_t k : ks) {
+            const uint32_t b = cstart[col[k].q];
+            for (Prelim& h : col[k].p) {
+                h.q_start += b;
+                h.q_end += b;
+                h.q_seed += b;
+            }
+            // a chunk with no prelims for this pair leaves the accumulated list as it is
+            if (first && b == 0) acc = std::move(col[k].p);
+            else merge_chunk_prelims(acc, col[k].p, b);
+            first = false;
+        }
+        if (acc.empty()) continue;
+        const uint32_t qa = QL->len[pr / ns], sa = C.slen[pr % ns];
+        sort_prelims_for_traceback(acc, qa, sa);
+        pair_ids.push_back((uint32_t)pr);
+        prelims.push_back(std::move(acc));
+    }
+    ctr.ms_host_2a += ms_since(t0);
+    // Phase 2b on the full queries
+    DevQueries Q{QL->d_q.as<uint8_t>(), QL->d_qrc.as<uint8_t>(), QL->d_q.as<uint8_t>(), QL->d_qrc.as<uint8_t>(),
+                 QL->d_off.as<uint64_t>(), QL->d_len.as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr,
+                 nullptr, nullptr, nl};
+    std::vector<std::vector<Hit>> lh(nl);
+    auto qhost = [&](uint32_t j) { return (const uint8_t*)QL->host.data() + QL->off[j]; };
+    traceback_2b(C, Q, QL->len.data(), nl, qhost, pair_ids, prelims, lh.data(), ctr, nullptr);
+    t0 = std::chrono::steady_clock::now();
+    for (uint32_t j = 0; j < nl; ++j) {
+        apply_mask_level(lh[j], P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
+        sort_hit_list_order(lh[j], C.ids);
+        ctr.finals += lh[j].size();
+        out_hits[longq[j]] = std::move(lh[j]);
+    }
+    ctr.ms_host_2b += ms_since(t0);
+}
+
+}  // namespace
+
+extern "C" {
 
 static rmb_results* pack_results(const std::vector<std::vector<Hit>>& hits, const rmb_counters& ctr) {
     const uint32_t nq = (uint32_t)hits.size();

@@ -4,7 +4,8 @@
 // One query is one sequential pass, as in the reference: the pass draws NCBI CRandom numbers for
 // N bases in order (dust.rs:24-57, 339-360) and restarts a window scan from the last window start
 // after each low-complexity run (dust.rs:400-460), so the masked positions depend on the whole
-// prefix.  The device runs one query per thread; the queries of a batch run in parallel.
+// prefix.  The device runs one query per warp (one working lane); the queries of a batch run in
+// parallel.
 //
 // Storage differs from the reference's growable vectors, not the results:
 //  - the triplet list (at most window - 2 = 62 entries) is a 64-entry ring;
@@ -220,12 +221,14 @@ struct DustTriplets {
 struct DustMasker {
     uint8_t* out;  // masked copy of the query bases (no sentinel), length n
     uint32_t n;
+    bool compat;   // the multi-chunk path's off-by-one: also mask e + 1 (dust.rs:614-630)
     bool has;
     uint32_t cs, ce;
     RMB_HD void flush() {
         if (!has) return;
         const uint32_t end = ce < n - 1 ? ce : n - 1;
         for (uint32_t p = cs; p <= end; ++p) out[p] = 14;
+        if (compat && ce + 1 < n) out[ce + 1] = 14;
     }
     RMB_HD void save(DustPerfectList& perfect, uint32_t wstart) {
         if (perfect.size == 0) return;
@@ -246,14 +249,15 @@ struct DustMasker {
 };
 
 // dust.rs:339-460 + 462-489 for one query: masks the low-complexity intervals of bases[0..n) in
-// out[0..n) (out holds a copy of bases).  `scratch` holds DUST_PERFECT_CAP entries.  Returns false
+// out[0..n) (out holds a copy of bases); `compat` adds the multi-chunk path's extra base after
+// each interval (dust.rs:614-630).  `scratch` holds DUST_PERFECT_CAP entries.  Returns false
 // if the perfect list would have outgrown its ring (then `out` is incomplete).
-RMB_HD bool dust_query(const uint8_t* bases, uint32_t n, uint8_t* out, DustPerfect* scratch) {
+RMB_HD bool dust_query(const uint8_t* bases, uint32_t n, uint8_t* out, DustPerfect* scratch, bool compat = false) {
     if (n < 3) return true;
     DustRng rng;
     rng.init();
     DustPerfectList perfect{scratch, 0, 0, false};
-    DustMasker mk{out, n, false, 0, 0};
+    DustMasker mk{out, n, compat, false, 0, 0};
     DustTriplets w;
     uint8_t conv[8];
     uint32_t j_start = 0;

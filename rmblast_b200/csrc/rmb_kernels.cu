@@ -2073,11 +2073,11 @@ cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t
 __global__ void __launch_bounds__(32) k_dust(const uint8_t* __restrict__ q, const uint64_t* __restrict__ off,
                                              const uint32_t* __restrict__ len, uint32_t nq, uint8_t* __restrict__ qm,
                                              DustPerfect* __restrict__ scratch, uint32_t nworkers,
-                                             unsigned int* __restrict__ overflow) {
+                                             unsigned int* __restrict__ overflow, bool compat) {
     if (threadIdx.x != 0 || blockIdx.x >= nworkers) return;
     for (uint32_t i = blockIdx.x; i < nq; i += nworkers) {
         const uint64_t o = off[i] + 1;
-        if (!dust_query(q + o, len[i], qm + o, scratch + (uint64_t)blockIdx.x * DUST_PERFECT_CAP))
+        if (!dust_query(q + o, len[i], qm + o, scratch + (uint64_t)blockIdx.x * DUST_PERFECT_CAP, compat))
             atomicAdd(overflow, 1u);
     }
 }
@@ -2089,9 +2089,9 @@ uint32_t dust_threads(uint32_t nq, int sms) {
 size_t dust_scratch_bytes(uint32_t nthreads) { return (size_t)nthreads * DUST_PERFECT_CAP * sizeof(DustPerfect); }
 
 cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
-                        void* scratch, uint32_t nthreads, unsigned int* overflow, cudaStream_t st) {
+                        void* scratch, uint32_t nthreads, unsigned int* overflow, bool compat, cudaStream_t st) {
     if (!nq || !nthreads) return cudaSuccess;
-    k_dust<<<nthreads, 32, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow);
+    k_dust<<<nthreads, 32, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow, compat);
     return cudaGetLastError();
 }
 }  // namespace rmb

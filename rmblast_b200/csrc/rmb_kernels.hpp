@@ -89,9 +89,10 @@ namespace rmb {
 cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* rc,
                            cudaStream_t st);
 // DUST masking of a query batch: qm must hold a copy of q; `scratch` holds
-// dust_scratch_bytes(nthreads); overflow counts queries whose interval list overflowed.
+// dust_scratch_bytes(nthreads); overflow counts queries whose interval list overflowed; compat
+// adds the multi-chunk path's extra masked base after each interval.
 uint32_t dust_threads(uint32_t nq, int sms);
 size_t dust_scratch_bytes(uint32_t nthreads);
 cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
-                        void* scratch, uint32_t nthreads, unsigned int* overflow, cudaStream_t st);
+                        void* scratch, uint32_t nthreads, unsigned int* overflow, bool compat, cudaStream_t st);
 }  // namespace rmb

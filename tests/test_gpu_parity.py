@@ -225,10 +225,6 @@ def test_edge_cases():
     res = s.search(qs)
     assert res.n_hsps == 0
     assert s.search([]).n_hsps == 0
-    # the chunked path is refused, not silently truncated
-    with pytest.raises(api.RmbError) as e:
-        s.search([api.encode(b"A" * 1_999_800)])
-    assert e.value.code == 5
 
 
 def test_lookup_tables_match_reference_rules():
@@ -277,3 +273,23 @@ def test_traceback_stage_matches_oracle(case):
     want = O.stage_text(q, db, mt, mn, p, 4)
     assert len(want) > 0
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("scale,dust", [(21.0, 1), (26.0, 0)])
+def test_chunked_long_query_matches_oracle(scale, dust):
+    """Queries of 1,999,800 bp or more take the multi-chunk path (two and three chunks here),
+    in one call with short queries: every line against the oracle's chunked pipeline, which the
+    chr22 NCBI golden pins."""
+    qs, db, prm = synth.workload("small", scale=scale)
+    short, _, _ = synth.workload("small", scale=0.2)
+    p = dict(prm, **synth.RM_FLAGS)
+    p["dust"] = dust
+    names = [n for n, _ in short] + [n for n, _ in qs] + ["short_b"]
+    seqs = [s for _, s in short] + [s for _, s in qs] + [short[0][1][5000:15000]]
+    assert len(qs[0][1]) >= 1_999_800
+    qf = synth.to_fasta(names, seqs)
+    dbf = synth.to_fasta([n for n, _ in db], [s for _, s in db])
+    txt, res = gpu_text(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, qf, FIELDS)
+    want, _, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert txt.count("\n") > 1000
+    assert txt == want
