@@ -111,10 +111,11 @@ typedef struct rmb_results {
     rmb_counters counters;
 } rmb_results;
 
-/* main.rs:1133-1236 search_db_parallel (single-chunk path) for n_queries queries.
+/* main.rs:1133-1236 search_db_parallel for n_queries queries: the single-chunk path, and for
+ * queries of 1,999,800 bp or more the multi-chunk path (main.rs:1236-1400: 1 Mb chunks with a
+ * 100 bp overlap, whole-query DUST, cross-chunk merge, full-query traceback); both in one call.
  * query[i]: sentinel-wrapped BLASTNA (qlen[i] + 2 bytes), not CRandom-resolved (queries keep
- * N).  Queries of 1,999,800 bp or more take the reference's chunked path and are refused
- * with RMB_ELIMIT. */
+ * N).  Stage taps (rmb_debug_stage) take single-chunk queries only. */
 int rmb_search_batch(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
                      rmb_results** out, char* err, size_t errlen);
 
