@@ -217,6 +217,8 @@ void mask_queries(rmb_ctx& C, rmb_queries& QH, bool compat, rmb_counters& ctr) {
 }
 
 // One (query, subject) pair's Phase 2a output, in the reference's order (purge order).
+constexpr uint64_t MAX_RANGE_HITS = 1ull << 29;
+
 struct PairPrelims {
     uint32_t q, s;
     std::vector<Prelim> p;
@@ -356,287 +358,320 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         CK(cudaMemcpyAsync(&nh, C.offs.as<uint64_t>() + npairs, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctr.gpu_ms_scan += ev.ms();
-        if (nh >= 0xffffffffull) throw Fail(RMB_ELIMIT, "more than 2^32 word hits in one batch");
         ctr.word_hits += nh;
-        C.hits.ensure(nh * sizeof(SeedHit));
-        C.hit_pair.ensure(nh * 4);
-        ev.start(st);
-        CK(launch_scan(true, C.L, Q, P.word_size, 0, npairs, nullptr, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
-                       C.hit_pair.as<uint32_t>(), C.sms, st));
-        ev.stop(st);
-        CK(cudaStreamSynchronize(st));
-        ctr.gpu_ms_scan += ev.ms();
-        ctr.launches += 2;
-        ctr.ms_scan += ms_since(t0);
-
-        // ---- ungapped extension of every hit, then the per-pair dedup
-        t0 = std::chrono::steady_clock::now();
-        C.ub.ensure(nh * sizeof(UngBox));
-        ev.start(st);
-        CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
-                           C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st));
-        ev.stop(st);
-        CK(cudaStreamSynchronize(st));
-        ctr.gpu_ms_ungapped += ev.ms();
-        ctr.launches += nh ? 1 : 0;
-        ctr.ms_ungapped += ms_since(t0);
-        t0 = std::chrono::steady_clock::now();
-        C.flags.ensure(nh + 1);
-        C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
-        C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
-        ev.start(st);
-        CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], 0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
-                        C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
-        ev.stop(st);
-        ctr.launches += 1;
-        C.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
-        C.n_sel.ensure(16);
-        tb = 0;
-        CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb,
-                            st));
-        C.temp.ensure(tb);
-        CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p,
-                            tb, st));
-        uint32_t nu = 0;
-        CK(cudaMemcpyAsync(&nu, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        ctr.gpu_ms_dedup += ev.ms();
-        ctr.ms_dedup += ms_since(t0);
-        ctr.ungapped += nu;
-        if (taps && (taps->seeds || taps->ungapped)) {
-            std::vector<SeedHit> hh(nh);
-            std::vector<uint32_t> hp(nh);
-            std::vector<uint8_t> fl(nh);
-            std::vector<UngBox> uu(nh);
-            if (nh) {
-                CK(cudaMemcpy(hh.data(), C.hits.p, nh * sizeof(SeedHit), cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(hp.data(), C.hit_pair.p, nh * 4, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(fl.data(), C.flags.p, nh, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(uu.data(), C.ub.p, nh * sizeof(UngBox), cudaMemcpyDeviceToHost));
-            }
-            for (uint64_t i = 0; i < nh; ++i) {
-                if (!fl[i]) continue;
-                const uint32_t qi = hp[i] / ns, si = hp[i] % ns;
-                const uint32_t s_len = C.slen[si];
-                const bool minus = hh[i].qs >> 31;
-                const uint32_t qo = hh[i].qs & 0x7fffffffu, so = hh[i].s;
-                if (taps->seeds) {
-                    if (!minus) taps->seeds->insert(taps->seeds->end(), {0u, qo, so});
-                    else {
-                        const uint32_t en = (uint32_t)(P.word_size - hlw[qi]);
-                        const uint32_t sl = so + (uint32_t)hlw[qi];
-                        taps->seeds->insert(taps->seeds->end(), {1u, qo >= en ? qo - en : 0, s_len >= sl ? s_len - sl : 0});
-                    }
-                }
-            }
-            if (taps->ungapped) {
-                // per pair, in the reference's sort order (engine.rs:1280-1309)
-                std::vector<std::vector<UngSurvivor>> per(npairs);
-                for (uint64_t i = 0; i < nh; ++i) {
-                    if (fl[i] != 3) continue;
-                    UngSurvivor r{};
-                    r.q_seed = hh[i].qs & 0x7fffffffu;
-                    r.s_seed = hh[i].s;
-                    r.q_start = uu[i].q_start;
-                    r.q_end = uu[i].q_end;
-                    r.s_start = uu[i].s_start;
-                    r.s_end = uu[i].s_end;
-                    r.score = uu[i].score;
-                    r.strand = (uint8_t)(hh[i].qs >> 31);
-                    per[hp[i]].push_back(r);
-                }
-                for (uint64_t pr = 0; pr < npairs; ++pr) {
-                    auto& v = per[pr];
-                    if (v.empty()) continue;
-                    const uint32_t qa = hqlen[pr / ns], sa = C.slen[pr % ns];
-                    // sort exactly as phase2a_filter does, with every record kept
-                    for (auto& r : v) { r.p_score = INT32_MIN; }
-                    std::vector<UngSurvivor> w = v;
-                    auto ss = [&](const UngSurvivor& r) { return r.strand == 0 ? r.s_start : sa - r.s_end; };
-                    auto qk = [&](const UngSurvivor& r) -> uint64_t {
-                        return r.strand == 0 ? r.q_start : ((uint64_t)qa + 1) + ((uint64_t)qa >= r.q_end ? qa - r.q_end : 0);
-                    };
-                    auto sk = [&](const UngSurvivor& r) { return r.strand == 0 ? r.s_seed : sa - r.s_seed; };
-                    std::sort(w.begin(), w.end(), [&](const UngSurvivor& a, const UngSurvivor& b) {
-                        if (a.score != b.score) return a.score > b.score;
-                        if (ss(a) != ss(b)) return ss(a) < ss(b);
-                        const uint32_t la = a.s_end - a.s_start, lb = b.s_end - b.s_start;
-                        if (la != lb) return la > lb;
-                        if (qk(a) != qk(b)) return qk(a) < qk(b);
-                        return sk(a) < sk(b);
-                    });
-                    for (auto& r : w) {
-                        const uint32_t s0 = r.strand == 0 ? r.s_start : sa - r.s_end;
-                        const uint32_t s1 = r.strand == 0 ? r.s_end : sa - r.s_start;
-                        taps->ungapped->insert(taps->ungapped->end(),
-                                               {(uint32_t)r.strand, r.q_start, r.q_end, s0, s1, (uint32_t)r.score});
-                    }
-                }
-            }
-            if (!taps->prelims) { qb = qe; continue; }
+        // Pair ranges whose word hits fit the stage buffers: one range unless the batch is huge
+        // (an all-against-all search at word 7 makes tens of billions).  Every stage from the
+        // write pass on works per pair, so ranges run one after another; masklevel and the hit
+        // order run once over all of them.
+        std::vector<uint64_t> ranges{0, npairs};
+        std::vector<uint64_t> hoffs;
+        if (nh > MAX_RANGE_HITS) {
+            if (taps) throw Fail(RMB_ELIMIT, "stage taps take batches of at most 2^29 word hits");
+            hoffs.resize(npairs + 1);
+            CK(cudaMemcpy(hoffs.data(), C.offs.p, (npairs + 1) * 8, cudaMemcpyDeviceToHost));
+            ranges.assign(1, 0);
+            for (uint64_t pr = 0; pr < npairs; ++pr)
+                if (hoffs[pr + 1] - hoffs[ranges.back()] > MAX_RANGE_HITS && pr > ranges.back()) ranges.push_back(pr);
+            ranges.push_back(npairs);
         }
-
-        // ---- preliminary gapped DP of every ungapped record
-        t0 = std::chrono::steady_clock::now();
-        C.po.ensure(std::max<uint64_t>(nu, 1) * sizeof(PrelimOut));
-        C.wide.ensure(std::max<uint64_t>(nu, 1) * 4);
-        C.n_wide.ensure(16);
-        C.cells.ensure(16);
-        C.fails.ensure(16);
-        CK(cudaMemsetAsync(C.n_wide.p, 0, 16, st));
-        CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
-        CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
-        ev.start(st);
-        EvTimer ev_main;
-        if (C.prelim_stream) {
-            C.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
-            CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
-                                  C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p, C.sms,
+        bool tapped = false;
+        const uint64_t nh_all = nh;
+        for (size_t ri = 0; ri + 1 < ranges.size() && !tapped; ++ri) {
+            const uint64_t pair0 = ranges[ri];
+            const uint64_t npairs = ranges[ri + 1] - pair0;  // the pairs of this range
+            const uint64_t nh = ranges.size() > 2 ? hoffs[pair0 + npairs] - hoffs[pair0] : nh_all;
+            if (nh >= 0xffffffffull) throw Fail(RMB_ELIMIT, "more than 2^32 word hits in one pair range");
+            if (ranges.size() > 2) {  // offsets local to the range
+                tb = 0;
+                CK(launch_offsets(C.counts.as<uint32_t>() + pair0, npairs + 1, C.offs.as<uint64_t>(), nullptr, tb,
                                   st));
-            ctr.launches += nu ? 1 : 0;
-            ev_main.start(st);
-            CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
-                                    C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
-                                    C.cells.as<unsigned long long>(), C.sms, st));
-            ev_main.stop(st);
-        }
-        else
-            CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
-                             C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
-                             C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(),
-                             C.sms, st));
-        ev.stop(st);
-        ctr.launches += nu ? 1 : 0;
-        uint32_t nw = 0;
-        unsigned long long main_cells = 0;
-        CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&main_cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        ctr.gpu_ms_prelim += ev.ms();
-        if (C.prelim_stream) {
-            ctr.gpu_ms_prelim_main += ev_main.ms();
-            ctr.so_cells_main += main_cells;
-        }
-        DBuf* wide_list = &C.wide;
-        if (nw && C.prelim_stream) {
-            // records whose band window outgrew the thread ring: the warp kernel's 256-cell rings
-            C.wide2.ensure((uint64_t)nw * 4);
-            C.dres.ensure((uint64_t)nw * 2 * sizeof(int4));
-            CK(cudaMemsetAsync(C.n_wide.p, 0, 4, st));
-            EvTimer e2;
-            e2.start(st);
-            CK(launch_prelim_split(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(),
-                                   C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(),
-                                   C.ub.as<UngBox>(), C.dres.as<int4>(), C.po.as<PrelimOut>(), C.wide2.as<uint32_t>(),
-                                   C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(), C.sms, st));
-            e2.stop(st);
-            ctr.launches += 2;
-            CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            ctr.gpu_ms_prelim += e2.ms();
-            wide_list = &C.wide2;
-        }
-        if (nw) {
-            uint32_t qmax = 0;
-            for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
-            const uint64_t cap = (uint64_t)std::max(qmax, C.max_slen) + 2;
-            const uint32_t threads = std::min<uint32_t>(nw, (uint32_t)std::max<uint64_t>(128, (1ull << 31) / (cap * 8)));
-            C.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
-            EvTimer ew;
-            ew.start(st);
-            ctr.launches += 1;
-            CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, wide_list->as<uint32_t>(), C.ung_idx.as<uint32_t>(),
-                                  C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
-                                  C.po.as<PrelimOut>(), C.band.as<int2>(), cap, threads,
-                                  C.cells.as<unsigned long long>(), C.fails.as<unsigned int>(), st));
-            ew.stop(st);
-            ctr.gpu_ms_prelim += ew.ms();
-        }
-        unsigned long long cells = 0;
-        unsigned int fails = 0;
-        CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&fails, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (fails) throw Fail(RMB_ECUDA, "prelim DP band exceeded its storage");
-        ctr.so_cells += cells;
-        ctr.prelim_dp += nu;
-        // survivors (score >= gapped cutoff) to the host
-        C.sel.ensure(std::max<uint64_t>(nu, 1) * 4);
-        tb = 0;
-        CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb, st));
-        C.temp.ensure(tb);
-        CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p, tb, st));
-        uint32_t nsv = 0;
-        CK(cudaMemcpyAsync(&nsv, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        C.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
-        ctr.launches += nsv ? 1 : 0;
-        CK(launch_gather_survivors(nsv, C.sel.as<uint32_t>(), C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
-                                   C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
-                                   C.surv.as<SurvivorRec>(), st));
-        std::vector<SurvivorRec> sv(nsv);
-        if (nsv) CK(cudaMemcpyAsync(sv.data(), C.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        ctr.ms_prelim_dp += ms_since(t0);
-
-        // ---- host Phase 2a filter per pair
-        t0 = std::chrono::steady_clock::now();
-        std::vector<uint32_t> pair_ids;
-        std::vector<std::vector<UngSurvivor>> per_pair;
-        for (const SurvivorRec& r : sv) {
-            if (pair_ids.empty() || pair_ids.back() != r.pair) {
-                pair_ids.push_back(r.pair);
-                per_pair.emplace_back();
+                C.temp.ensure(tb);
+                CK(launch_offsets(C.counts.as<uint32_t>() + pair0, npairs + 1, C.offs.as<uint64_t>(), C.temp.p, tb,
+                                  st));
             }
-            UngSurvivor u{};
-            u.q_seed = r.hit.qs & 0x7fffffffu;
-            u.s_seed = r.hit.s;
-            u.q_start = r.ub.q_start;
-            u.q_end = r.ub.q_end;
-            u.s_start = r.ub.s_start;
-            u.s_end = r.ub.s_end;
-            u.score = r.ub.score;
-            u.strand = (uint8_t)(r.hit.qs >> 31);
-            u.p_score = r.po.score;
-            u.p_qs = r.po.q_start;
-            u.p_qe = r.po.q_end;
-            u.p_ss = r.po.s_start;
-            u.p_se = r.po.s_end;
-            u.tb_q = r.po.tb_q;
-            u.tb_s = r.po.tb_s;
-            per_pair.back().push_back(u);
-        }
-        const size_t np = pair_ids.size();
-        std::vector<std::vector<Prelim>> prelims(np);
-        parallel_for(np, [&](size_t k) {
-            const uint32_t qa = hqlen[pair_ids[k] / ns], sa = C.slen[pair_ids[k] % ns];
-            prelims[k] = phase2a_filter(per_pair[k], qa, sa);
-            if (!collect) sort_prelims_for_traceback(prelims[k], qa, sa);
-        });
-        per_pair.clear();
-        uint64_t n_pre = 0;
-        for (auto& v : prelims) n_pre += v.size();
-        ctr.prelims += n_pre;
-        if (taps && taps->prelims) {
-            // in pipeline (purge) order: re-run the purge order is not kept after the traceback
-            // sort, so report them in traceback order per pair
-            for (size_t k = 0; k < np; ++k)
-                for (const Prelim& p : prelims[k])
-                    taps->prelims->insert(taps->prelims->end(), {(uint32_t)p.strand, p.q_start, p.q_end, p.s_start,
-                                                                 p.s_end, (uint32_t)p.score, p.q_seed, p.s_seed});
-            qb = qe;
-            continue;
-        }
-        ctr.ms_host_2a += ms_since(t0);
-        if (collect) {
-            for (size_t k = 0; k < np; ++k)
-                collect->push_back(PairPrelims{qb + pair_ids[k] / ns, pair_ids[k] % ns, std::move(prelims[k])});
-            qb = qe;
-            continue;
-        }
+            C.hits.ensure(nh * sizeof(SeedHit));
+            C.hit_pair.ensure(nh * 4);
+            ev.start(st);
+            CK(launch_scan(true, C.L, Q, P.word_size, pair0, npairs, nullptr, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
+                           C.hit_pair.as<uint32_t>(), C.sms, st));
+            ev.stop(st);
+            CK(cudaStreamSynchronize(st));
+            ctr.gpu_ms_scan += ev.ms();
+            ctr.launches += 2;
+            ctr.ms_scan += ms_since(t0);
 
-        // ---- traceback DP and host Phase 2b of every prelim
-        if (traceback_2b(C, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps)) {
+            // ---- ungapped extension of every hit, then the per-pair dedup
+            t0 = std::chrono::steady_clock::now();
+            C.ub.ensure(nh * sizeof(UngBox));
+            ev.start(st);
+            CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
+                               C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st));
+            ev.stop(st);
+            CK(cudaStreamSynchronize(st));
+            ctr.gpu_ms_ungapped += ev.ms();
+            ctr.launches += nh ? 1 : 0;
+            ctr.ms_ungapped += ms_since(t0);
+            t0 = std::chrono::steady_clock::now();
+            C.flags.ensure(nh + 1);
+            C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
+            C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+            ev.start(st);
+            CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], pair0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
+                            C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
+            ev.stop(st);
+            ctr.launches += 1;
+            C.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
+            C.n_sel.ensure(16);
+            tb = 0;
+            CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb,
+                                st));
+            C.temp.ensure(tb);
+            CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p,
+                                tb, st));
+            uint32_t nu = 0;
+            CK(cudaMemcpyAsync(&nu, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ctr.gpu_ms_dedup += ev.ms();
+            ctr.ms_dedup += ms_since(t0);
+            ctr.ungapped += nu;
+            if (taps && (taps->seeds || taps->ungapped)) {
+                std::vector<SeedHit> hh(nh);
+                std::vector<uint32_t> hp(nh);
+                std::vector<uint8_t> fl(nh);
+                std::vector<UngBox> uu(nh);
+                if (nh) {
+                    CK(cudaMemcpy(hh.data(), C.hits.p, nh * sizeof(SeedHit), cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(hp.data(), C.hit_pair.p, nh * 4, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(fl.data(), C.flags.p, nh, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(uu.data(), C.ub.p, nh * sizeof(UngBox), cudaMemcpyDeviceToHost));
+                }
+                for (uint64_t i = 0; i < nh; ++i) {
+                    if (!fl[i]) continue;
+                    const uint32_t qi = hp[i] / ns, si = hp[i] % ns;
+                    const uint32_t s_len = C.slen[si];
+                    const bool minus = hh[i].qs >> 31;
+                    const uint32_t qo = hh[i].qs & 0x7fffffffu, so = hh[i].s;
+                    if (taps->seeds) {
+                        if (!minus) taps->seeds->insert(taps->seeds->end(), {0u, qo, so});
+                        else {
+                            const uint32_t en = (uint32_t)(P.word_size - hlw[qi]);
+                            const uint32_t sl = so + (uint32_t)hlw[qi];
+                            taps->seeds->insert(taps->seeds->end(), {1u, qo >= en ? qo - en : 0, s_len >= sl ? s_len - sl : 0});
+                        }
+                    }
+                }
+                if (taps->ungapped) {
+                    // per pair, in the reference's sort order (engine.rs:1280-1309)
+                    std::vector<std::vector<UngSurvivor>> per(npairs);
+                    for (uint64_t i = 0; i < nh; ++i) {
+                        if (fl[i] != 3) continue;
+                        UngSurvivor r{};
+                        r.q_seed = hh[i].qs & 0x7fffffffu;
+                        r.s_seed = hh[i].s;
+                        r.q_start = uu[i].q_start;
+                        r.q_end = uu[i].q_end;
+                        r.s_start = uu[i].s_start;
+                        r.s_end = uu[i].s_end;
+                        r.score = uu[i].score;
+                        r.strand = (uint8_t)(hh[i].qs >> 31);
+                        per[hp[i]].push_back(r);
+                    }
+                    for (uint64_t pr = 0; pr < npairs; ++pr) {
+                        auto& v = per[pr];
+                        if (v.empty()) continue;
+                        const uint32_t qa = hqlen[pr / ns], sa = C.slen[pr % ns];
+                        // sort exactly as phase2a_filter does, with every record kept
+                        for (auto& r : v) { r.p_score = INT32_MIN; }
+                        std::vector<UngSurvivor> w = v;
+                        auto ss = [&](const UngSurvivor& r) { return r.strand == 0 ? r.s_start : sa - r.s_end; };
+                        auto qk = [&](const UngSurvivor& r) -> uint64_t {
+                            return r.strand == 0 ? r.q_start : ((uint64_t)qa + 1) + ((uint64_t)qa >= r.q_end ? qa - r.q_end : 0);
+                        };
+                        auto sk = [&](const UngSurvivor& r) { return r.strand == 0 ? r.s_seed : sa - r.s_seed; };
+                        std::sort(w.begin(), w.end(), [&](const UngSurvivor& a, const UngSurvivor& b) {
+                            if (a.score != b.score) return a.score > b.score;
+                            if (ss(a) != ss(b)) return ss(a) < ss(b);
+                            const uint32_t la = a.s_end - a.s_start, lb = b.s_end - b.s_start;
+                            if (la != lb) return la > lb;
+                            if (qk(a) != qk(b)) return qk(a) < qk(b);
+                            return sk(a) < sk(b);
+                        });
+                        for (auto& r : w) {
+                            const uint32_t s0 = r.strand == 0 ? r.s_start : sa - r.s_end;
+                            const uint32_t s1 = r.strand == 0 ? r.s_end : sa - r.s_start;
+                            taps->ungapped->insert(taps->ungapped->end(),
+                                                   {(uint32_t)r.strand, r.q_start, r.q_end, s0, s1, (uint32_t)r.score});
+                        }
+                    }
+                }
+                if (!taps->prelims) { tapped = true; continue; }
+            }
+
+            // ---- preliminary gapped DP of every ungapped record
+            t0 = std::chrono::steady_clock::now();
+            C.po.ensure(std::max<uint64_t>(nu, 1) * sizeof(PrelimOut));
+            C.wide.ensure(std::max<uint64_t>(nu, 1) * 4);
+            C.n_wide.ensure(16);
+            C.cells.ensure(16);
+            C.fails.ensure(16);
+            CK(cudaMemsetAsync(C.n_wide.p, 0, 16, st));
+            CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
+            CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
+            ev.start(st);
+            EvTimer ev_main;
+            if (C.prelim_stream) {
+                C.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
+                CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
+                                      C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p, C.sms,
+                                      st));
+                ctr.launches += nu ? 1 : 0;
+                ev_main.start(st);
+                CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
+                                        C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
+                                        C.cells.as<unsigned long long>(), C.sms, st));
+                ev_main.stop(st);
+            }
+            else
+                CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
+                                 C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
+                                 C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(),
+                                 C.sms, st));
+            ev.stop(st);
+            ctr.launches += nu ? 1 : 0;
+            uint32_t nw = 0;
+            unsigned long long main_cells = 0;
+            CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&main_cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ctr.gpu_ms_prelim += ev.ms();
+            if (C.prelim_stream) {
+                ctr.gpu_ms_prelim_main += ev_main.ms();
+                ctr.so_cells_main += main_cells;
+            }
+            DBuf* wide_list = &C.wide;
+            if (nw && C.prelim_stream) {
+                // records whose band window outgrew the thread ring: the warp kernel's 256-cell rings
+                C.wide2.ensure((uint64_t)nw * 4);
+                C.dres.ensure((uint64_t)nw * 2 * sizeof(int4));
+                CK(cudaMemsetAsync(C.n_wide.p, 0, 4, st));
+                EvTimer e2;
+                e2.start(st);
+                CK(launch_prelim_split(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(),
+                                       C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(),
+                                       C.ub.as<UngBox>(), C.dres.as<int4>(), C.po.as<PrelimOut>(), C.wide2.as<uint32_t>(),
+                                       C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(), C.sms, st));
+                e2.stop(st);
+                ctr.launches += 2;
+                CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                ctr.gpu_ms_prelim += e2.ms();
+                wide_list = &C.wide2;
+            }
+            if (nw) {
+                uint32_t qmax = 0;
+                for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
+                const uint64_t cap = (uint64_t)std::max(qmax, C.max_slen) + 2;
+                const uint32_t threads = std::min<uint32_t>(nw, (uint32_t)std::max<uint64_t>(128, (1ull << 31) / (cap * 8)));
+                C.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
+                EvTimer ew;
+                ew.start(st);
+                ctr.launches += 1;
+                CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, wide_list->as<uint32_t>(), C.ung_idx.as<uint32_t>(),
+                                      C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
+                                      C.po.as<PrelimOut>(), C.band.as<int2>(), cap, threads,
+                                      C.cells.as<unsigned long long>(), C.fails.as<unsigned int>(), st));
+                ew.stop(st);
+                ctr.gpu_ms_prelim += ew.ms();
+            }
+            unsigned long long cells = 0;
+            unsigned int fails = 0;
+            CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&fails, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (fails) throw Fail(RMB_ECUDA, "prelim DP band exceeded its storage");
+            ctr.so_cells += cells;
+            ctr.prelim_dp += nu;
+            // survivors (score >= gapped cutoff) to the host
+            C.sel.ensure(std::max<uint64_t>(nu, 1) * 4);
+            tb = 0;
+            CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb, st));
+            C.temp.ensure(tb);
+            CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p, tb, st));
+            uint32_t nsv = 0;
+            CK(cudaMemcpyAsync(&nsv, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            C.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
+            ctr.launches += nsv ? 1 : 0;
+            CK(launch_gather_survivors(nsv, C.sel.as<uint32_t>(), C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
+                                       C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
+                                       C.surv.as<SurvivorRec>(), st));
+            std::vector<SurvivorRec> sv(nsv);
+            if (nsv) CK(cudaMemcpyAsync(sv.data(), C.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ctr.ms_prelim_dp += ms_since(t0);
+
+            // ---- host Phase 2a filter per pair
+            t0 = std::chrono::steady_clock::now();
+            std::vector<uint32_t> pair_ids;
+            std::vector<std::vector<UngSurvivor>> per_pair;
+            for (const SurvivorRec& r : sv) {
+                if (pair_ids.empty() || pair_ids.back() != r.pair) {
+                    pair_ids.push_back(r.pair);
+                    per_pair.emplace_back();
+                }
+                UngSurvivor u{};
+                u.q_seed = r.hit.qs & 0x7fffffffu;
+                u.s_seed = r.hit.s;
+                u.q_start = r.ub.q_start;
+                u.q_end = r.ub.q_end;
+                u.s_start = r.ub.s_start;
+                u.s_end = r.ub.s_end;
+                u.score = r.ub.score;
+                u.strand = (uint8_t)(r.hit.qs >> 31);
+                u.p_score = r.po.score;
+                u.p_qs = r.po.q_start;
+                u.p_qe = r.po.q_end;
+                u.p_ss = r.po.s_start;
+                u.p_se = r.po.s_end;
+                u.tb_q = r.po.tb_q;
+                u.tb_s = r.po.tb_s;
+                per_pair.back().push_back(u);
+            }
+            const size_t np = pair_ids.size();
+            std::vector<std::vector<Prelim>> prelims(np);
+            parallel_for(np, [&](size_t k) {
+                const uint32_t qa = hqlen[pair_ids[k] / ns], sa = C.slen[pair_ids[k] % ns];
+                prelims[k] = phase2a_filter(per_pair[k], qa, sa);
+                if (!collect) sort_prelims_for_traceback(prelims[k], qa, sa);
+            });
+            per_pair.clear();
+            uint64_t n_pre = 0;
+            for (auto& v : prelims) n_pre += v.size();
+            ctr.prelims += n_pre;
+            if (taps && taps->prelims) {
+                // in pipeline (purge) order: re-run the purge order is not kept after the traceback
+                // sort, so report them in traceback order per pair
+                for (size_t k = 0; k < np; ++k)
+                    for (const Prelim& p : prelims[k])
+                        taps->prelims->insert(taps->prelims->end(), {(uint32_t)p.strand, p.q_start, p.q_end, p.s_start,
+                                                                     p.s_end, (uint32_t)p.score, p.q_seed, p.s_seed});
+                tapped = true;
+                continue;
+            }
+            ctr.ms_host_2a += ms_since(t0);
+            if (collect) {
+                for (size_t k = 0; k < np; ++k)
+                    collect->push_back(PairPrelims{qb + pair_ids[k] / ns, pair_ids[k] % ns, std::move(prelims[k])});
+                continue;  // next range
+            }
+
+            // ---- traceback DP and host Phase 2b of every prelim
+            if (traceback_2b(C, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps)) {
+                tapped = true;
+                continue;
+            }
+        }
+        if (tapped || collect) {
             qb = qe;
             continue;
         }

@@ -1866,6 +1866,10 @@ cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevPara
 
 namespace rmb {
 
+struct U64Add {
+    __host__ __device__ __forceinline__ uint64_t operator()(uint64_t a, uint64_t b) const { return a + b; }
+};
+
 __global__ void k_gather_survivors(uint32_t n, const uint32_t* __restrict__ sel, const uint32_t* __restrict__ idx,
                                    const SeedHit* __restrict__ hits, const uint32_t* __restrict__ hit_pair,
                                    const UngBox* __restrict__ ub, const PrelimOut* __restrict__ po,
@@ -1909,7 +1913,9 @@ cudaError_t launch_select_prelim(const PrelimOut* po, uint64_t n, uint32_t* out,
 
 cudaError_t launch_offsets(const uint32_t* counts, uint64_t n, uint64_t* offs, void* temp, size_t& temp_bytes,
                            cudaStream_t st) {
-    return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offs, (int64_t)n, st);
+    // a 64-bit initial value makes the scan accumulate in 64 bits: the counts are 32-bit, their
+    // sums are not (ExclusiveSum would add them up in the counts' type)
+    return cub::DeviceScan::ExclusiveScan(temp, temp_bytes, counts, offs, U64Add{}, (uint64_t)0, (int64_t)n, st);
 }
 
 }  // namespace rmb

@@ -293,3 +293,33 @@ def test_chunked_long_query_matches_oracle(scale, dust):
     want, _, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
     assert txt.count("\n") > 1000
     assert txt == want
+
+
+@pytest.mark.parametrize("name,scale", [("batched", 0.002), ("allvsall", 0.04)])
+def test_config_workloads_match_oracle(name, scale):
+    """The other configurations' shapes: many chunks of mixed lengths (1-200 kb, three lookup
+    widths in one call) against the 2,000-consensus library, and the library searched against
+    itself (word 7, masklevel off, derived and high-divergence consensi)."""
+    qs, db, prm = synth.workload(name, scale=scale)
+    p = dict(prm, **synth.RM_FLAGS)
+    qf = synth.to_fasta([n for n, _ in qs], [s for _, s in qs])
+    dbf = synth.to_fasta([n for n, _ in db], [s for _, s in db])
+    txt, res = gpu_text(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, qf, FIELDS)
+    want, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert txt.count("\n") > 150
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"]
+
+
+def test_pair_ranges_match_oracle():
+    """A batch with more word hits than one pass holds (500 consensi against themselves at word 7:
+    ~760 M hits, two pair ranges): output and counters as in one pass, against the oracle."""
+    qs, db, prm = synth.workload("allvsall", scale=0.1)
+    p = dict(prm, **synth.RM_FLAGS)
+    qf = synth.to_fasta([n for n, _ in qs], [s for _, s in qs])
+    dbf = synth.to_fasta([n for n, _ in db], [s for _, s in db])
+    txt, res = gpu_text(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, qf, FIELDS)
+    assert res.counters["word_hits"] > (1 << 29)
+    want, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"]
