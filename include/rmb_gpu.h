@@ -45,6 +45,13 @@ typedef struct rmb_params {
     int32_t schedule;     /* 0 = FIFO (only value accepted) */
     int32_t kernels;      /* 0 = automatic; 1 = run every preliminary DP on the warp-cooperative
                              kernel (the thread-per-extension kernel's fallback), for testing */
+    /* Gapped Karlin-Altschul statistics for E-values and bit scores, as rmb_ka_resolve returns
+     * them: lambda, K, H, and the alpha/beta of the length adjustment.  ka_lambda <= 0: none
+     * (every E-value 1.0 and bit score 0.0, the reference's rendering without statistics). */
+    double ka_lambda, ka_k, ka_h, ka_alpha, ka_beta;
+    /* --evalue (main.rs:1224-1226, NCBI Blast_HSPListReapByEvalue): HSPs whose E-value is above
+     * this are dropped before masklevel; 0 = off; no effect without statistics. */
+    double evalue;
 } rmb_params;
 
 typedef struct rmb_ctx rmb_ctx;
@@ -78,6 +85,7 @@ typedef struct rmb_hsp {
     uint32_t ops_len;
     uint32_t aln_len;  /* length of the aligned strings */
     uint64_t seq_off;  /* into rmb_results.q_seq / s_seq (BLASTNA, gap = 15) */
+    double evalue, bitscore;  /* Karlin-Altschul E-value and bit score (1.0 / 0.0 without statistics) */
 } rmb_hsp;
 
 /* Stage counters of one search call (the reference's diagnostics counters,
@@ -156,6 +164,17 @@ int rmb_debug_stage(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* quer
  * rmb_resolve_subject: seq/fasta_db.rs:86-131 -- CRandom (seeded with the length) replaces each
  * ambiguity code 4..14 by a base, and n_mask (n bytes) keeps the original codes; *has_mask is
  * 0 when the subject has no ambiguity code (n_mask then stays all zero). */
+/* rmb_ka_resolve: the statistics for rmb_params.ka_* (rmblast-lib/src/ka_stats.rs:153-300, the
+ * default mode): RMBlast's built-in table by matrix file base name and exact gap costs; else the
+ * -matrix_lambda/-matrix_k/-matrix_alpha/-matrix_beta values in cli[4] (used when lambda, K and
+ * alpha are > 0; zeros otherwise; NULL for none); else a "# KARLIN lambda .. k .. h|alpha ..
+ * [beta ..]" line of matrix_text (NULL for none; matrix.rs:38-70); else none (ka[0] = -1).
+ * The reference's last resort, an ALP simulation fit of the matrix, is not provided: such a
+ * matrix gets no statistics here.  ka[5] = lambda, K, H, alpha, beta; *source = 0 none,
+ * 1 table, 2 command line, 3 matrix comment. */
+int rmb_ka_resolve(const char* matrix_name, const char* matrix_text, int32_t gap_open, int32_t gap_extend,
+                   const double cli[4], double ka[5], int32_t* source, char* err, size_t errlen);
+
 int rmb_matrix_parse(const char* text, int32_t scores[256], double freqs[16], double* lambda, char* err,
                      size_t errlen);
 void rmb_encode_iupac(const char* ascii, size_t n, uint8_t* out);

@@ -65,6 +65,8 @@ struct Matrix {
     double freqs[16];
     double lambda = 0.0;
     std::string name;
+    bool has_karlin = false;          // a "# KARLIN" comment line (matrix.rs:38-70, 100-103)
+    double karlin[5] = {0, 0, 0, 0, 0};  // lambda, K, H, alpha, beta
 };
 Matrix parse_matrix(const std::string& text, const std::string& name);  // matrix.rs:76
 Matrix load_matrix(const std::string& path);
@@ -80,6 +82,8 @@ struct Params {
     bool complexity_adjust = false;
     bool dust = true;
     uint32_t mask_level = 101;
+    double evalue = 0.0;                  // --evalue reap threshold; 0 = off
+    double cli_stats[4] = {0, 0, 0, 0};   // -matrix_lambda, -matrix_k, -matrix_alpha, -matrix_beta
     int gapped_cutoff() const { return min_raw_gapped_score > 1 ? min_raw_gapped_score : 1; }
     int cutoff_score_max() const { return min_raw_gapped_score > 0 ? min_raw_gapped_score / 2 : 1; }
 };
@@ -116,6 +120,7 @@ struct AlignResult {
     std::string query_id, subject_id;
     uint32_t oid = 0;
     AlignStats stats;
+    double evalue = 1.0, bitscore = 0.0;  // the no-statistics rendering until set
 };
 
 // ---- lookup table (blast/nalookup.rs, blast/mblookup.rs) --------------------------------
@@ -197,5 +202,19 @@ GapAlign align_ex(const uint8_t* a, const uint8_t* b, size_t m, size_t n, int go
 AlignStats compute_align_stats(const std::vector<uint8_t>& q_iupac, const std::vector<uint8_t>& s_iupac);
 std::vector<uint8_t> to_iupac(const std::vector<uint8_t>& aligned);
 std::string format_tabular(const AlignResult& r, const std::vector<std::string>& fields);
+
+// ---- E-value statistics (rmb_oracle_stats.cpp) -----------------------------------------
+struct KaStats {  // gapped Karlin block + the length adjustment's alpha/beta; lambda <= 0: none
+    double lambda = -1.0, k = -1.0, log_k = -1.0, h = -1.0, alpha = 0.0, beta = 0.0;
+    int source = 0;  // 0 none, 1 table, 2 command line, 3 matrix comment
+};
+KaStats resolve_stats(const std::string& matrix_name, int go, int ge, const double cli[4], const Matrix& m);
+int32_t length_adjustment(double k, double log_k, double alpha_d_lambda, double beta, int32_t query_length,
+                          int64_t db_length, int32_t db_num_seqs, bool* converged);
+int64_t effective_search_space(const KaStats& s, int32_t query_length, int64_t db_length, int32_t db_num_seqs);
+double evalue_of(int32_t score, const KaStats& s, int64_t searchsp);
+double bitscore_of(int32_t score, const KaStats& s);
+std::string format_evalue(double e);
+std::string format_bitscore(double b);
 
 }  // namespace rmbo

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
 #include <cstring>
 #include <sstream>
 #include <stdexcept>
@@ -17,6 +18,8 @@ extern "C" {
 struct rmbo_params {
     int32_t gap_open, gap_extend, word_size, xdrop_ungap, xdrop_gap, xdrop_gap_final;
     int32_t min_raw_gapped_score, complexity_adjust, dust, mask_level;  // mask_level < 0 = off
+    double evalue;         // --evalue; 0 = off
+    double cli_stats[4];   // -matrix_lambda, -matrix_k, -matrix_alpha, -matrix_beta; zeros = unset
 };
 
 static Params to_params(const rmbo_params* c, const std::string& mname) {
@@ -32,6 +35,8 @@ static Params to_params(const rmbo_params* c, const std::string& mname) {
     p.dust = c->dust != 0;
     p.mask_level = c->mask_level < 0 ? 101u : (uint32_t)c->mask_level;
     p.matrix_name = mname;
+    p.evalue = c->evalue;
+    for (int i = 0; i < 4; ++i) p.cli_stats[i] = c->cli_stats[i];
     return p;
 }
 
@@ -47,6 +52,40 @@ static void set_err(char* err, size_t errlen, const char* msg) {
         strncpy(err, msg, errlen - 1);
         err[errlen - 1] = 0;
     }
+}
+
+// The statistics of a matrix: out = lambda, K, H, alpha, beta, source.
+int rmbo_stats(const char* matrix_name, const char* matrix_text, int32_t go, int32_t ge, const double cli[4],
+               double out[6], char* err, size_t errlen) {
+    try {
+        Matrix m = parse_matrix(matrix_text, matrix_name);
+        const double zero[4] = {0, 0, 0, 0};
+        KaStats s = resolve_stats(matrix_name, go, ge, cli ? cli : zero, m);
+        out[0] = s.lambda; out[1] = s.k; out[2] = s.h; out[3] = s.alpha; out[4] = s.beta; out[5] = s.source;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return 1;
+    }
+}
+
+int32_t rmbo_length_adjustment(double k, double log_k, double alpha_d_lambda, double beta, int32_t qlen,
+                               int64_t db_len, int32_t db_num, int32_t* converged) {
+    bool c = false;
+    const int32_t la = length_adjustment(k, log_k, alpha_d_lambda, beta, qlen, db_len, db_num, &c);
+    if (converged) *converged = c ? 1 : 0;
+    return la;
+}
+
+// E-value and bit score of a raw score with stats ka = lambda, K, H, alpha, beta
+void rmbo_evalue(const double ka[5], int32_t score, int32_t qlen, int64_t db_len, int32_t db_num, double out[3]) {
+    KaStats s;
+    s.lambda = ka[0]; s.k = ka[1]; s.log_k = ka[1] > 0 ? std::log(ka[1]) : -1.0; s.h = ka[2];
+    s.alpha = ka[3]; s.beta = ka[4];
+    const int64_t sp = effective_search_space(s, qlen, db_len, db_num);
+    out[0] = evalue_of(score, s, sp);
+    out[1] = bitscore_of(score, s);
+    out[2] = (double)sp;
 }
 
 // Full search of every query against every subject; writes the outfmt-6 text.

@@ -52,6 +52,11 @@ int main(int argc, char** argv) {
             else if (a == "--num-threads") threads = std::stoi(val());
             else if (a == "--mt-mode") val();
             else if (a == "--stats") stats = true;
+            else if (a == "--evalue") p.evalue = std::stod(val());
+            else if (a == "--matrix-lambda") p.cli_stats[0] = std::stod(val());
+            else if (a == "--matrix-k") p.cli_stats[1] = std::stod(val());
+            else if (a == "--matrix-alpha") p.cli_stats[2] = std::stod(val());
+            else if (a == "--matrix-beta") p.cli_stats[3] = std::stod(val());
             else throw std::runtime_error("unknown option " + a);
         }
         if (matrix.empty()) throw std::runtime_error("--matrix is required");

@@ -1355,6 +1355,27 @@ static std::vector<std::vector<AlignResult>> search_chunked(const std::vector<ui
     return per;
 }
 
+// main.rs:1224-1234 + 758-763: E-values and bit scores for the query (ka_stats.rs:382
+// for_query: the query length against the database's letters and sequences), the --evalue
+// reap before masklevel, masklevel, then the hit order.
+static void finish_query(std::vector<AlignResult>& res, const Params& p, const Matrix& m, size_t qlen,
+                         uint64_t db_letters, size_t db_seqs) {
+    const KaStats ka = resolve_stats(p.matrix_name, p.gap_open, p.gap_extend, p.cli_stats, m);
+    const int64_t sp = effective_search_space(ka, (int32_t)qlen, (int64_t)db_letters, (int32_t)db_seqs);
+    for (auto& r : res) {
+        r.evalue = evalue_of(r.hsp.score, ka, sp);
+        r.bitscore = bitscore_of(r.hsp.score, ka);
+    }
+    if (p.evalue > 0.0 && ka.lambda > 0.0) {
+        std::vector<AlignResult> kept;
+        for (auto& r : res)
+            if (r.evalue <= p.evalue) kept.push_back(std::move(r));
+        res.swap(kept);
+    }
+    apply_mask_level(res, p.mask_level);
+    sort_hit_list_order(res);
+}
+
 std::vector<AlignResult> search_query(const std::vector<uint8_t>& query, const std::string& qid,
                                       const std::vector<Subject>& db, const Params& p0, const Matrix& m, int threads,
                                       Counters* counters) {
@@ -1369,8 +1390,7 @@ std::vector<AlignResult> search_query(const std::vector<uint8_t>& query, const s
         std::vector<AlignResult> res;
         for (auto& v : per)
             for (auto& r : v) res.push_back(std::move(r));
-        apply_mask_level(res, p.mask_level);
-        sort_hit_list_order(res);
+        finish_query(res, p, m, qlen, total, db.size());
         return res;
     }
     QueryLookup ql = build_query_lookup(query, p);
@@ -1403,8 +1423,7 @@ std::vector<AlignResult> search_query(const std::vector<uint8_t>& query, const s
     std::vector<AlignResult> res;
     for (auto& v : per)
         for (auto& r : v) res.push_back(std::move(r));
-    apply_mask_level(res, p.mask_level);
-    sort_hit_list_order(res);
+    finish_query(res, p, m, qlen, total, db.size());
     return res;
 }
 

@@ -125,8 +125,8 @@ std::string format_tabular(const AlignResult& r, const std::vector<std::string>&
         else if (f == "cpg_sites") out += std::to_string(st.transitions);
         else if (f == "qseq") { auto v = to_iupac(h.q_seq); out.append(v.begin(), v.end()); }
         else if (f == "sseq") { auto v = to_iupac(h.s_seq); out.append(v.begin(), v.end()); }
-        else if (f == "evalue") out += "1.0";
-        else if (f == "bitscore") out += " 0.0";
+        else if (f == "evalue") out += format_evalue(r.evalue);
+        else if (f == "bitscore") out += format_bitscore(r.bitscore);
         else throw std::runtime_error("unknown -outfmt field '" + f + "'");
     }
     return out;

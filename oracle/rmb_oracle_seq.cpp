@@ -383,6 +383,25 @@ Matrix parse_matrix(const std::string& text, const std::string& name) {
         std::string t = line.substr(a, b - a);
         if (t.empty()) continue;
         if (t[0] == '#') {
+            if (t.rfind("# KARLIN", 0) == 0 || t.rfind("#KARLIN", 0) == 0) {  // matrix.rs:100-103, 248-264
+                auto tok = split_ws(t.substr(t[1] == ' ' ? 8 : 7));
+                for (int i = 0; i < 5; ++i) m.karlin[i] = 0.0;
+                for (size_t i = 0; i + 1 < tok.size(); i += 2) {
+                    char* end = nullptr;
+                    double v = strtod(tok[i + 1].c_str(), &end);
+                    if (*end != 0 || tok[i + 1].empty()) fail("bad KARLIN value");
+                    std::string key = tok[i];
+                    for (auto& ch : key) ch = (char)tolower((unsigned char)ch);
+                    if (key == "lambda") m.karlin[0] = v;
+                    else if (key == "k") m.karlin[1] = v;
+                    else if (key == "h") m.karlin[2] = v;
+                    else if (key == "alpha") m.karlin[3] = v;
+                    else if (key == "beta") m.karlin[4] = v;
+                    else fail("unknown KARLIN key");
+                }
+                m.has_karlin = true;
+                continue;
+            }
             size_t at = t.find("FREQS");
             if (at != std::string::npos) {
                 if (have_freqs) fail("a second FREQS line");

@@ -32,7 +32,8 @@ class _Params(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "gap_open", "gap_extend", "word_size", "xdrop_ungap", "xdrop_gap", "xdrop_gap_final",
         "min_raw_gapped_score", "complexity_adjust", "dust", "mask_level", "ungapped_cutoff",
-        "device", "schedule", "kernels")]
+        "device", "schedule", "kernels")] + [(n, C.c_double) for n in (
+        "ka_lambda", "ka_k", "ka_h", "ka_alpha", "ka_beta", "evalue")]
 
 
 class _Hsp(C.Structure):
@@ -41,7 +42,7 @@ class _Hsp(C.Structure):
         "mismatches", "query_gaps", "subject_gaps", "transitions", "transversions", "cpg_sites")] + [
         ("perc_sub", C.c_float), ("perc_query_gap", C.c_float), ("perc_db_gap", C.c_float),
         ("kdiv", C.c_double), ("cpg_kdiv", C.c_double), ("ops_off", C.c_uint64), ("ops_len", C.c_uint32),
-        ("aln_len", C.c_uint32), ("seq_off", C.c_uint64)]
+        ("aln_len", C.c_uint32), ("seq_off", C.c_uint64), ("evalue", C.c_double), ("bitscore", C.c_double)]
 
 
 class _Counters(C.Structure):
@@ -150,6 +151,7 @@ class ScoreMatrix:
     freqs: np.ndarray   # float64 (16,)
     lambda_: float
     name: str
+    text: str | None = None  # the file text (its "# KARLIN" line feeds the E-value statistics)
 
     @classmethod
     def from_text(cls, text: str, name: str = "") -> "ScoreMatrix":
@@ -159,7 +161,7 @@ class ScoreMatrix:
         err = C.create_string_buffer(512)
         _check(lib().rmb_matrix_parse(text.encode(), sc, fr, C.byref(lam), err, 512), err)
         return cls(np.frombuffer(sc, dtype=np.int32).reshape(16, 16).copy(), np.frombuffer(fr).copy(),
-                   lam.value, name)
+                   lam.value, name, text)
 
     @classmethod
     def from_file(cls, path: str) -> "ScoreMatrix":
@@ -183,11 +185,18 @@ class SearchParams:
     device: int = 0
     # 0: automatic kernel choice; 1: every preliminary DP on the warp-cooperative kernel
     kernels: int = 0
+    # --evalue threshold (0: off) and the -matrix_lambda/-matrix_k/-matrix_alpha/-matrix_beta
+    # statistics overrides (zeros: unset)
+    evalue: float = 0.0
+    matrix_lambda: float = 0.0
+    matrix_k: float = 0.0
+    matrix_alpha: float = 0.0
+    matrix_beta: float = 0.0
 
-    def _c(self) -> _Params:
+    def _c(self, ka=(-1.0, -1.0, -1.0, 0.0, 0.0)) -> _Params:
         return _Params(self.gap_open, self.gap_extend, self.word_size, self.xdrop_ungap, self.xdrop_gap,
                        self.xdrop_gap_final, self.min_raw_gapped_score, int(self.complexity_adjust), int(self.dust),
-                       self.mask_level, self.ungapped_cutoff, self.device, 0, self.kernels)
+                       self.mask_level, self.ungapped_cutoff, self.device, 0, self.kernels, *ka, self.evalue)
 
 
 class SubjectDb:
@@ -278,6 +287,19 @@ class ResidentQueries:
         self.free()
 
 
+def ka_resolve(matrix_name: str, gap_open: int, gap_extend: int, matrix_text: str | None = None,
+               cli: tuple[float, float, float, float] | None = None) -> tuple[tuple[float, ...], int]:
+    """rmb_ka_resolve: (lambda, K, H, alpha, beta) and the source (0 none, 1 table, 2 command
+    line, 3 matrix comment) of the E-value statistics, as the reference's ka_stats::resolve."""
+    ka = (C.c_double * 5)()
+    src = C.c_int32()
+    err = C.create_string_buffer(512)
+    c = (C.c_double * 4)(*cli) if cli else None
+    _check(lib().rmb_ka_resolve(matrix_name.encode(), matrix_text.encode() if matrix_text is not None else None,
+                                gap_open, gap_extend, c, ka, C.byref(src), err, 512), err)
+    return tuple(ka), src.value
+
+
 class Searcher:
     """One search context on one GPU: parameters, matrix and the resident library."""
 
@@ -287,7 +309,9 @@ class Searcher:
         err = C.create_string_buffer(512)
         sc = matrix.scores.astype(np.int32).ravel()
         fr = matrix.freqs.astype(np.float64)
-        _check(lib().rmb_ctx_create(C.byref(params._c()), sc.ctypes.data_as(C.POINTER(C.c_int32)),
+        cli = (params.matrix_lambda, params.matrix_k, params.matrix_alpha, params.matrix_beta)
+        self.ka, self.ka_source = ka_resolve(matrix.name, params.gap_open, params.gap_extend, matrix.text, cli)
+        _check(lib().rmb_ctx_create(C.byref(params._c(self.ka)), sc.ctypes.data_as(C.POINTER(C.c_int32)),
                                     fr.ctypes.data_as(C.POINTER(C.c_double)), matrix.lambda_,
                                     matrix.name.encode(), C.byref(ctx), err, 512), err)
         self._ctx = ctx

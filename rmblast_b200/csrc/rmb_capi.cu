@@ -142,6 +142,7 @@ struct rmb_ctx {
     // per-batch device buffers
     DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     bool prelim_stream = false;  // thread-per-extension prelim kernel (else the warp kernel)
+    KaBlock ka;                  // E-value statistics (lambda <= 0: none)
     DBuf dust_scratch;           // per-thread DUST interval lists
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
@@ -227,6 +228,22 @@ struct PairPrelims {
 bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
                   std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps);
+
+// The per-query end of a search: E-values and bit scores (rmstats RmStats for the query's length
+// against the whole database), the --evalue reap (main.rs:1224-1226, before masklevel), then
+// masklevel (engine.rs:863) and the hit order (main.rs:1230-1234, engine.rs:998).
+void finish_query(const rmb_ctx& C, std::vector<Hit>& v, uint32_t qlen) {
+    const rmb_params& P = C.p;
+    const int64_t sp = eff_searchsp(C.ka, (int32_t)qlen, (int64_t)C.total_letters, (int32_t)C.ids.size());
+    for (Hit& h : v) {
+        h.evalue = hsp_evalue(h.score, C.ka, sp);
+        h.bitscore = hsp_bitscore(h.score, C.ka);
+    }
+    if (P.evalue > 0.0 && C.ka.lambda > 0.0)
+        v.erase(std::remove_if(v.begin(), v.end(), [&](const Hit& h) { return h.evalue > P.evalue; }), v.end());
+    apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
+    sort_hit_list_order(v, C.ids);
+}
 
 // The search of a set of single-chunk queries.  ucut_override: per-query ungapped cutoffs (the
 // chunks of a long query take their parent's).  collect: stop after Phase 2a and hand over the
@@ -676,11 +693,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             continue;
         }
         t0 = std::chrono::steady_clock::now();
-        parallel_for(nb, [&](size_t i) {
-            auto& v = out_hits[qb + i];
-            apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
-            sort_hit_list_order(v, C.ids);
-        });
+        parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
         for (uint32_t i = 0; i < nb; ++i) ctr.finals += out_hits[qb + i].size();
         ctr.ms_host_2b += ms_since(t0);
         qb = qe;
@@ -884,6 +897,17 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         dp.gapped_cutoff = C->gp.gapped_cutoff;
         for (int i = 0; i < 256; ++i) dp.matrix[i] = scores[i];
         C->prelim_stream = p.kernels == 0 && prelim_stream_eligible(dp.matrix, p.gap_open, p.gap_extend, p.xdrop_gap);
+        if (p.ka_lambda > 0.0) {
+            if (!(p.ka_k > 0.0) || !(p.ka_h > 0.0) || !(p.ka_alpha > 0.0))
+                throw Fail(RMB_EINVAL, "statistics need K, H and alpha > 0 with lambda > 0");
+            C->ka.lambda = p.ka_lambda;
+            C->ka.k = p.ka_k;
+            C->ka.log_k = std::log(p.ka_k);
+            C->ka.h = p.ka_h;
+            C->ka.alpha = p.ka_alpha;
+            C->ka.beta = p.ka_beta;
+        }
+        if (p.evalue < 0.0) throw Fail(RMB_EINVAL, "evalue must be >= 0");
         C->d_params.ensure(sizeof(DevParams));
         CK(cudaMemcpy(C->d_params.p, &dp, sizeof dp, cudaMemcpyHostToDevice));
         *out = C;
@@ -1236,8 +1260,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
     traceback_2b(C, Q, QL->len.data(), nl, qhost, pair_ids, prelims, lh.data(), ctr, nullptr);
     t0 = std::chrono::steady_clock::now();
     for (uint32_t j = 0; j < nl; ++j) {
-        apply_mask_level(lh[j], P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
-        sort_hit_list_order(lh[j], C.ids);
+        finish_query(C, lh[j], QL->len[j]);
         ctr.finals += lh[j].size();
         out_hits[longq[j]] = std::move(lh[j]);
     }
@@ -1287,6 +1310,7 @@ static rmb_results* pack_results(const std::vector<std::vector<Hit>>& hits, cons
             x.perc_sub = h.stats.perc_sub; x.perc_query_gap = h.stats.perc_query_gap;
             x.perc_db_gap = h.stats.perc_db_gap;
             x.kdiv = h.stats.kdiv; x.cpg_kdiv = h.stats.cpg_kdiv;
+            x.evalue = h.evalue; x.bitscore = h.bitscore;
             x.ops_off = o;
             x.ops_len = (uint32_t)h.script.size();
             for (auto& r : h.script) R->ops[o++] = ((uint32_t)r.op << 30) | r.n;
@@ -1418,6 +1442,7 @@ int rmb_format_tabular(const rmb_ctx* C, const rmb_results* R, const char* const
                 h.stats.perc_sub = x.perc_sub; h.stats.perc_query_gap = x.perc_query_gap;
                 h.stats.perc_db_gap = x.perc_db_gap;
                 h.stats.kdiv = x.kdiv; h.stats.cpg_kdiv = x.cpg_kdiv;
+                h.evalue = x.evalue; h.bitscore = x.bitscore;
                 h.q_seq.assign(R->q_seq + x.seq_off, R->q_seq + x.seq_off + x.aln_len);
                 h.s_seq.assign(R->s_seq + x.seq_off, R->s_seq + x.seq_off + x.aln_len);
                 if (!format_line(out, h, qid, C->ids.at(x.subject_oid), fields))

@@ -907,11 +907,168 @@ bool format_line(std::string& out, const Hit& h, const std::string& qid, const s
         else if (f == "cpg_sites") out += std::to_string(h.stats.transitions);
         else if (f == "qseq") for (uint8_t b : h.q_seq) out.push_back(b == 15 ? '-' : IUPAC[b & 15]);
         else if (f == "sseq") for (uint8_t b : h.s_seq) out.push_back(b == 15 ? '-' : IUPAC[b & 15]);
-        else if (f == "evalue") out += "1.0";
-        else if (f == "bitscore") out += " 0.0";
+        else if (f == "evalue") append_evalue(out, h.evalue);
+        else if (f == "bitscore") append_bitscore(out, h.bitscore);
         else return false;
     }
     return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// Karlin-Altschul statistics for E-values and bit scores (rmblast-lib/src/ka_stats.rs:153-300,
+// rmblast-stats/rmstats: rmblast_tables.rs, eff_lengths.rs, length_adjust.rs, evalue.rs)
+// ---------------------------------------------------------------------------------------
+namespace {
+// rmstats tables_data.rs: RMBlast's gapped (lambda, K, H) per matrix file name and gap costs,
+// with the refitted 30p53g row and comparison.matrix; kept value for value.
+struct KaStatRow { const char* name; int go, ge; double lambda, k, h; };
+const KaStatRow KA_STATS[] = {
+    {"14p35g.matrix", 29, 6, 0.1241860392, 0.2565118357, 0.3349210581}, {"14p37g.matrix", 29, 6, 0.1243509013, 0.2538327145, 0.3484386549},
+    {"14p39g.matrix", 29, 6, 0.118108197, 0.2381799563, 0.3209988017}, {"14p41g.matrix", 29, 6, 0.1209164962, 0.251696198, 0.3474870514},
+    {"14p43g.matrix", 29, 6, 0.1204338701, 0.2484920137, 0.3397421893}, {"14p45g.matrix", 29, 6, 0.1281012415, 0.2651519027, 0.3664022073},
+    {"14p47g.matrix", 29, 6, 0.116957149, 0.2334091021, 0.3226817428}, {"14p49g.matrix", 29, 6, 0.1167697593, 0.2289233061, 0.3136272703},
+    {"14p51g.matrix", 29, 6, 0.1238779017, 0.2467119379, 0.32413383}, {"14p53g.matrix", 29, 6, 0.1211022467, 0.2307304663, 0.2949314272},
+    {"18p35g.matrix", 28, 5, 0.120477663, 0.2111410357, 0.2484902185}, {"18p37g.matrix", 28, 5, 0.1213800379, 0.2057492194, 0.2637651575},
+    {"18p39g.matrix", 28, 5, 0.1228853168, 0.2111281814, 0.2802003038}, {"18p41g.matrix", 28, 5, 0.1096830298, 0.1715966796, 0.2171487218},
+    {"18p43g.matrix", 28, 5, 0.1179924113, 0.1957371364, 0.2544060456}, {"18p45g.matrix", 28, 5, 0.1184247414, 0.2068045787, 0.2641082233},
+    {"18p47g.matrix", 28, 5, 0.115878332, 0.1842046578, 0.2407688057}, {"18p49g.matrix", 28, 5, 0.1248964218, 0.2141853759, 0.2675489103},
+    {"18p51g.matrix", 28, 5, 0.1106793836, 0.1621592148, 0.1979815532}, {"18p53g.matrix", 28, 5, 0.1082347513, 0.1408677318, 0.1771724651},
+    {"20p35g.matrix", 25, 5, 0.1112832877, 0.1466667286, 0.1741696491}, {"20p37g.matrix", 25, 5, 0.1134511409, 0.1501236494, 0.193180875},
+    {"20p39g.matrix", 25, 5, 0.1233401001, 0.1853070864, 0.2324952723}, {"20p41g.matrix", 25, 5, 0.1088138918, 0.1409300313, 0.1778018484},
+    {"20p43g.matrix", 25, 5, 0.1097495426, 0.1408421343, 0.1813610542}, {"20p45g.matrix", 25, 5, 0.1101110565, 0.1402262486, 0.1803401526},
+    {"20p47g.matrix", 25, 5, 0.1198508511, 0.175230183, 0.2232474228}, {"20p49g.matrix", 25, 5, 0.1150022018, 0.1500562415, 0.1891763921},
+    {"20p51g.matrix", 25, 5, 0.1101356126, 0.1310353805, 0.1457676446}, {"20p53g.matrix", 25, 5, 0.1239625969, 0.1752022586, 0.210665934},
+    {"25p35g.matrix", 22, 5, 0.0965155465, 0.0677355511, 0.0964040436}, {"25p37g.matrix", 22, 5, 0.0989264764, 0.076371967, 0.1025772304},
+    {"25p39g.matrix", 22, 5, 0.1005843197, 0.0805691511, 0.1108913867}, {"25p41g.matrix", 22, 5, 0.1030661339, 0.0840485952, 0.1237017673},
+    {"25p43g.matrix", 22, 5, 0.115543436, 0.1226554129, 0.1495157932}, {"25p45g.matrix", 22, 5, 0.0973402625, 0.074202019, 0.1029029688},
+    {"25p47g.matrix", 22, 5, 0.0967346256, 0.0743885008, 0.0995494785}, {"25p49g.matrix", 22, 5, 0.1070577141, 0.0941947942, 0.1181023643},
+    {"25p51g.matrix", 22, 5, 0.1044972455, 0.0789036639, 0.1081508568}, {"25p53g.matrix", 22, 5, 0.0977828435, 0.0607500307, 0.0834178835},
+    {"30p53g.matrix", 22, 5, 0.1204393447, 0.1065198197, 0.1243912966}, {"comparison.matrix", 20, 5, 0.09836223, 0.0789918084, 0.1116129577},
+};
+}  // namespace
+
+int ka_resolve(const std::string& matrix_name, int go, int ge, const double cli[4], const double* karlin,
+               KaBlock& out) {
+    std::string base = matrix_name;
+    const size_t sl = base.find_last_of('/');
+    if (sl != std::string::npos) base = base.substr(sl + 1);
+    const bool cli_set = cli && cli[0] > 0.0 && cli[1] > 0.0 && cli[2] > 0.0;
+    out = KaBlock{};
+    for (const KaStatRow& r : KA_STATS) {  // the table, by base name and exact gap costs
+        if (r.go != go || r.ge != ge || strcasecmp(r.name, base.c_str()) != 0) continue;
+        out.lambda = r.lambda;
+        out.k = r.k;
+        out.log_k = std::log(r.k);
+        out.h = r.h;
+        // eff_lengths.rs: alpha/beta from the command line when given, else lambda/H and 0
+        out.alpha = cli_set ? cli[2] : r.lambda / r.h;
+        out.beta = cli_set ? cli[3] : 0.0;
+        return KA_TABLE;
+    }
+    auto cli_like = [&](double lambda, double k, double alpha, double beta) {
+        out.lambda = lambda;
+        out.k = k;
+        out.log_k = std::log(k);
+        out.h = lambda / alpha;
+        out.alpha = alpha;
+        out.beta = beta;
+    };
+    if (cli_set) {
+        cli_like(cli[0], cli[1], cli[2], cli[3]);
+        return KA_CLI;
+    }
+    if (karlin) {  // a "# KARLIN" matrix comment: lambda, K, H, alpha, beta (alpha = lambda/H if absent)
+        const double alpha = karlin[3] > 0.0 ? karlin[3] : karlin[2] > 0.0 ? karlin[0] / karlin[2] : 0.0;
+        if (karlin[0] > 0.0 && karlin[1] > 0.0 && alpha > 0.0) {
+            cli_like(karlin[0], karlin[1], alpha, karlin[4]);
+            return KA_MATRIX_COMMENT;
+        }
+    }
+    return KA_NONE;  // the sentinel: E-value 1.0, bit score 0.0, nothing reaped
+}
+
+// length_adjust.rs (BLAST_ComputeLengthAdjustment): the fixed point of
+// ell = alpha/lambda * (ln K + ln((m - ell)(n - N ell))) + beta, by bisection.
+static int32_t length_adjustment(double k, double log_k, double alpha_d_lambda, double beta, int32_t qlen,
+                                 int64_t db_len, int32_t db_num) {
+    const int kMaxIter = 20;
+    const double m = qlen, n = (double)db_len, bn = db_num;
+    double ell_min = 0.0, ell_max, ell_next = 0.0;
+    bool converged = false;
+    {
+        const double a = bn, mb = m * bn + n, c = n * m - std::max(m, n) / k;
+        if (c < 0.0) return 0;
+        ell_max = 2.0 * c / (mb + std::sqrt(mb * mb - 4.0 * a * c));
+    }
+    for (int i = 1; i <= kMaxIter; ++i) {
+        const double ell = ell_next;
+        const double ss = (m - ell) * (n - bn * ell);
+        const double ell_bar = alpha_d_lambda * (log_k + std::log(ss)) + beta;
+        if (ell_bar >= ell) {
+            ell_min = ell;
+            if (ell_bar - ell_min <= 1.0) {
+                converged = true;
+                break;
+            }
+            if (ell_min == ell_max) break;
+        } else {
+            ell_max = ell;
+        }
+        if (ell_min <= ell_bar && ell_bar <= ell_max) ell_next = ell_bar;
+        else ell_next = i == 1 ? ell_max : (ell_min + ell_max) / 2.0;
+    }
+    int32_t la = (int32_t)ell_min;
+    if (converged) {
+        const double ell = std::ceil(ell_min);
+        if (ell <= ell_max) {
+            const double ss = (m - ell) * (n - bn * ell);
+            if (alpha_d_lambda * (log_k + std::log(ss)) + beta >= ell) la = (int32_t)ell;
+        }
+    }
+    return la;
+}
+
+int64_t eff_searchsp(const KaBlock& kb, int32_t qlen, int64_t db_len, int32_t db_num) {  // eff_lengths.rs
+    if (qlen <= 0 || !(kb.lambda > 0.0)) return 0;
+    const int32_t la = length_adjustment(kb.k, kb.log_k, kb.alpha / kb.lambda, kb.beta, qlen, db_len, db_num);
+    int64_t eff_db = db_len - (int64_t)db_num * (int64_t)la;
+    if (eff_db <= 0) eff_db = 1;
+    return eff_db * (int64_t)(qlen - la);
+}
+
+double hsp_evalue(int32_t score, const KaBlock& kb, int64_t searchsp) {  // evalue.rs hsp_evalue
+    if (!(kb.lambda > 0.0)) return 1.0;
+    if (kb.lambda < 0.0 || kb.k < 0.0 || kb.h < 0.0) return -1.0;
+    return (double)searchsp * std::exp(-kb.lambda * (double)score + kb.log_k);
+}
+
+double hsp_bitscore(int32_t score, const KaBlock& kb) {  // evalue.rs hsp_bit_score
+    if (!(kb.lambda > 0.0)) return 0.0;
+    return ((double)score * kb.lambda - kb.log_k) / 0.6931471805599453;
+}
+
+// output.rs:244-289: NCBI's tabular renderings (CAlignFormatUtil::GetScoreString)
+static void c_sci(std::string& out, double v, int prec) {
+    char buf[64];
+    snprintf(buf, sizeof buf, "%.*e", prec, v);
+    out += buf;
+}
+void append_evalue(std::string& out, double e) {
+    char buf[64];
+    if (e < 1.0e-180) { out += "0.0"; return; }
+    if (e < 0.0009) { c_sci(out, e, 2); return; }
+    if (e < 0.1) snprintf(buf, sizeof buf, "%.3f", e);
+    else if (e < 1.0) snprintf(buf, sizeof buf, "%.2f", e);
+    else if (e < 10.0) snprintf(buf, sizeof buf, "%.1f", e);
+    else snprintf(buf, sizeof buf, "%.0f", e);
+    out += buf;
+}
+void append_bitscore(std::string& out, double b) {
+    char buf[64];
+    if (b > 99999.0) { c_sci(out, b, 3); return; }
+    if (b > 99.9) snprintf(buf, sizeof buf, "%3ld", (long)b);
+    else snprintf(buf, sizeof buf, "%4.1f", b);
+    out += buf;
 }
 
 int choose_lut_width(int ws, uint64_t e) {  // blast/nalookup.rs:254-291

@@ -28,6 +28,7 @@ struct Hit {  // output.rs:132 AlignResult
     Script script;
     std::vector<uint8_t> q_seq, s_seq;
     Stats stats;
+    double evalue = 1.0, bitscore = 0.0;  // the statistics sentinel until set
 };
 
 // The host views of one subject the glue reads (sentinel-wrapped BLASTNA).
@@ -92,6 +93,24 @@ bool format_line(std::string& out, const Hit& h, const std::string& qid, const s
                  const std::vector<std::string>& fields);
 
 int choose_lut_width(int word_size, uint64_t approx_entries);
+
+// Gapped Karlin-Altschul block (lambda <= 0: no statistics) with the alpha/beta of the length
+// adjustment.
+struct KaBlock {
+    double lambda = -1.0, k = -1.0, log_k = -1.0, h = -1.0, alpha = 0.0, beta = 0.0;
+};
+enum { KA_NONE = 0, KA_TABLE = 1, KA_CLI = 2, KA_MATRIX_COMMENT = 3 };
+// ka_stats.rs:153-300 default mode without the ALP fit: the built-in table (base name, exact
+// gap costs), then cli = {lambda, K, alpha, beta} (used when lambda, K, alpha > 0), then a
+// "# KARLIN" comment {lambda, K, H, alpha, beta} (or null), else none.  Returns the source.
+int ka_resolve(const std::string& matrix_name, int go, int ge, const double cli[4], const double* karlin,
+               KaBlock& out);
+// eff_lengths.rs: the effective search space of one query against the database.
+int64_t eff_searchsp(const KaBlock& kb, int32_t qlen, int64_t db_len, int32_t db_num);
+double hsp_evalue(int32_t score, const KaBlock& kb, int64_t searchsp);
+double hsp_bitscore(int32_t score, const KaBlock& kb);
+void append_evalue(std::string& out, double e);
+void append_bitscore(std::string& out, double b);
 int ungapped_cutoff_for(const std::string& matrix_name, int go, int ge, int min_raw, uint64_t qlen, uint64_t avg);
 Stats align_stats(const std::vector<uint8_t>& q, const std::vector<uint8_t>& s);
 

@@ -1,5 +1,6 @@
 // rmb_io.cpp -- input preparation entry points of include/rmb_gpu.h: matrix parsing, IUPAC
 // encoding and CRandom resolution of subject ambiguity codes.
+#include <cctype>
 #include <cerrno>
 #include <cmath>
 #include <cstdint>
@@ -11,6 +12,7 @@
 #include <vector>
 
 #include "../../include/rmb_gpu.h"
+#include "rmb_glue.hpp"
 
 namespace {
 
@@ -225,3 +227,73 @@ int rmb_matrix_parse(const char* text, int32_t scores[256], double freqs[16], do
 }
 
 }  // extern "C"
+
+// rmblast-lib/src/matrix.rs:100-103, 248-264: the key/value pairs of a "# KARLIN" comment line.
+static bool karlin_comment(const char* text, double kc[5], std::string& err) {
+    std::istringstream is(text ? text : "");
+    std::string line;
+    bool found = false;
+    while (std::getline(is, line)) {
+        const size_t a = line.find_first_not_of(" \t\r\n");
+        if (a == std::string::npos) continue;
+        std::string t = line.substr(a);
+        std::string rest;
+        if (t.rfind("# KARLIN", 0) == 0) rest = t.substr(8);
+        else if (t.rfind("#KARLIN", 0) == 0) rest = t.substr(7);
+        else continue;
+        for (int i = 0; i < 5; ++i) kc[i] = 0.0;
+        std::istringstream ts(rest);
+        std::vector<std::string> tk;
+        std::string w;
+        while (ts >> w) tk.push_back(w);
+        for (size_t i = 0; i + 1 < tk.size(); i += 2) {
+            char* e = nullptr;
+            const double v = strtod(tk[i + 1].c_str(), &e);
+            if (!e || *e || tk[i + 1].empty()) {
+                err = "bad KARLIN value '" + tk[i + 1] + "' for key '" + tk[i] + "'";
+                return false;
+            }
+            std::string key = tk[i];
+            for (auto& c : key) c = (char)std::tolower((unsigned char)c);
+            if (key == "lambda") kc[0] = v;
+            else if (key == "k") kc[1] = v;
+            else if (key == "h") kc[2] = v;
+            else if (key == "alpha") kc[3] = v;
+            else if (key == "beta") kc[4] = v;
+            else {
+                err = "unknown KARLIN key '" + tk[i] + "'";
+                return false;
+            }
+        }
+        found = true;
+    }
+    if (!found) err.clear();
+    return found;
+}
+
+int rmb_ka_resolve(const char* matrix_name, const char* matrix_text, int32_t gap_open, int32_t gap_extend,
+                   const double cli[4], double ka[5], int32_t* source, char* err, size_t errlen) {
+    try {
+        if (!ka) throw std::runtime_error("null argument");
+        double kc[5] = {0, 0, 0, 0, 0};
+        std::string kerr;
+        const bool have_kc = karlin_comment(matrix_text, kc, kerr);
+        if (!have_kc && !kerr.empty()) throw std::runtime_error(kerr);
+        rmb::KaBlock kb;
+        const int src = rmb::ka_resolve(matrix_name ? matrix_name : "", gap_open, gap_extend, cli, have_kc ? kc : nullptr,
+                                        kb);
+        ka[0] = kb.lambda;
+        ka[1] = kb.k;
+        ka[2] = kb.h;
+        ka[3] = kb.alpha;
+        ka[4] = kb.beta;
+        if (source) *source = src;
+        return RMB_OK;
+    } catch (const std::exception& e) {
+        if (err && errlen) {
+            strncpy(err, e.what(), errlen - 1);
+            err[errlen - 1] = 0;
+        }
+        return RMB_EINVAL;
+    }
+}

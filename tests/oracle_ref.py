@@ -25,7 +25,8 @@ RM_PARAMS = dict(gap_open=20, gap_extend=5, word_size=14, xdrop_ungap=400, xdrop
 class OParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "gap_open", "gap_extend", "word_size", "xdrop_ungap", "xdrop_gap", "xdrop_gap_final",
-        "min_raw_gapped_score", "complexity_adjust", "dust", "mask_level")]
+        "min_raw_gapped_score", "complexity_adjust", "dust", "mask_level")] + [
+        ("evalue", C.c_double), ("cli_stats", C.c_double * 4)]
 
 
 def build_oracle() -> None:
@@ -51,9 +52,11 @@ def lib():
 
 
 def oparams(p: dict) -> OParams:
+    cli = p.get("cli_stats", (0.0, 0.0, 0.0, 0.0))
     return OParams(p["gap_open"], p["gap_extend"], p["word_size"], p["xdrop_ungap"], p["xdrop_gap"],
                    p["xdrop_gap_final"], p["min_raw_gapped_score"], int(p.get("complexity_adjust", 0)),
-                   int(p.get("dust", 0)), int(p.get("mask_level", -1)))
+                   int(p.get("dust", 0)), int(p.get("mask_level", -1)), float(p.get("evalue", 0.0)),
+                   (C.c_double * 4)(*cli))
 
 
 def search_text(query_fasta: str, db_fasta: str, matrix_text: str, matrix_name: str, p: dict, outfmt: str,

@@ -25,7 +25,9 @@ def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str, kernels
                           xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
                           min_raw_gapped_score=p["min_raw_gapped_score"],
                           complexity_adjust=bool(p.get("complexity_adjust", 0)), dust=bool(p.get("dust", 0)),
-                          mask_level=p.get("mask_level", -1), kernels=kernels)
+                          mask_level=p.get("mask_level", -1), kernels=kernels, evalue=p.get("evalue", 0.0),
+                          **dict(zip(("matrix_lambda", "matrix_k", "matrix_alpha", "matrix_beta"),
+                                     p.get("cli_stats", (0.0, 0.0, 0.0, 0.0)))))
     return api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
 
 
@@ -323,3 +325,33 @@ def test_pair_ranges_match_oracle():
     want, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS)
     assert txt == want
     assert res.counters["ungapped"] == ctr["ungapped"]
+
+
+STATS_FIELDS = "6 score evalue bitscore qseqid qstart qend sseqid sstart send"
+
+
+@pytest.mark.parametrize("case", ["table", "command_line", "matrix_comment"])
+def test_evalues_and_reap_match_oracle(case):
+    """E-value and bit-score columns and the --evalue reap (before masklevel): statistics from the
+    built-in table (comparison.matrix at 20/5), from the command line, and from a "# KARLIN"
+    matrix comment."""
+    if case == "table":
+        p = dict(O.RM_PARAMS, mask_level=80, complexity_adjust=1, dust=1, evalue=1e-30)
+        mt, name = (G / "comparison.matrix").read_text(), "comparison.matrix"
+        qf, dbf = (G / "query.fa").read_text(), (G / "db.fa").read_text()
+    else:
+        qf, dbf, p = synthetic("small", 0.3, synth.RM_FLAGS)
+        mt, name = synth.MATRIX_TEXT, synth.MATRIX_NAME
+        if case == "command_line":
+            p.update(cli_stats=(0.11, 0.09, 0.9, -20.0), evalue=1e-12)
+        else:
+            mt = "# KARLIN lambda 0.105 k 0.08 h 0.12\n" + mt
+    txt, res = gpu_text(p, mt, name, dbf, qf, STATS_FIELDS)
+    want, _, _ = O.search_text(qf, dbf, mt, name, p, STATS_FIELDS)
+    assert txt == want
+    lines = txt.splitlines()
+    assert len(lines) > 10
+    assert all(ln.split("\t")[1] != "1.0" for ln in lines)  # statistics were applied
+    if p.get("evalue"):
+        unreaped, _, _ = O.search_text(qf, dbf, mt, name, dict(p, evalue=0.0), STATS_FIELDS)
+        assert unreaped.count("\n") > txt.count("\n")  # the cut dropped some HSPs
