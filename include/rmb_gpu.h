@@ -164,6 +164,16 @@ int rmb_debug_stage(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* quer
  * rmb_resolve_subject: seq/fasta_db.rs:86-131 -- CRandom (seeded with the length) replaces each
  * ambiguity code 4..14 by a base, and n_mask (n bytes) keeps the original codes; *has_mask is
  * 0 when the subject has no ambiguity code (n_mask then stays all zero). */
+int rmb_matrix_parse(const char* text, int32_t scores[256], double freqs[16], double* lambda, char* err,
+                     size_t errlen);
+void rmb_encode_iupac(const char* ascii, size_t n, uint8_t* out);
+void rmb_resolve_subject(const uint8_t* raw, uint32_t n, uint8_t* plus, uint8_t* n_mask, int32_t* has_mask);
+/* rmb_resolve_twobit_n: seq/twobit.rs:73-135 -- a .2bit record's N blocks (starts/sizes as in the
+ * file, clipped to n) get bases drawn from CRandom seeded with n, block by block; n_mask (n bytes,
+ * zeroed by the caller) gets 14 there.  plus is the sentinel-wrapped record (n + 2 bytes). */
+void rmb_resolve_twobit_n(uint32_t n, uint32_t n_blocks, const uint32_t* starts, const uint32_t* sizes,
+                          uint8_t* plus, uint8_t* n_mask);
+
 /* rmb_ka_resolve: the statistics for rmb_params.ka_* (rmblast-lib/src/ka_stats.rs:153-300, the
  * default mode): RMBlast's built-in table by matrix file base name and exact gap costs; else the
  * -matrix_lambda/-matrix_k/-matrix_alpha/-matrix_beta values in cli[4] (used when lambda, K and
@@ -175,10 +185,17 @@ int rmb_debug_stage(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* quer
 int rmb_ka_resolve(const char* matrix_name, const char* matrix_text, int32_t gap_open, int32_t gap_extend,
                    const double cli[4], double ka[5], int32_t* source, char* err, size_t errlen);
 
-int rmb_matrix_parse(const char* text, int32_t scores[256], double freqs[16], double* lambda, char* err,
-                     size_t errlen);
-void rmb_encode_iupac(const char* ascii, size_t n, uint8_t* out);
-void rmb_resolve_subject(const uint8_t* raw, uint32_t n, uint8_t* plus, uint8_t* n_mask, int32_t* has_mask);
+/* rmb_format_pairwise: pairwise output, outfmt 0 (rmblast-lib/src/output.rs:369-720), of the
+ * results of one search.  query[i] and qlen[i] are the searched queries (with dust = 1 their DUST
+ * intervals print in lower case; query may be NULL with dust = 0); query_deflines[i] is the full
+ * FASTA header after '>'; subject_deflines[oid] each subject's full header, or NULL for a
+ * database of ids only (.2bit).  db_name: as given to -db.  parts: bit 0 the program header,
+ * bit 1 the footer (for output split across calls).  db_mtime >= 0 (seconds since 1970, UTC)
+ * adds the footer's "Posted date" line.  The text is freed with rmb_text_free. */
+int rmb_format_pairwise(rmb_ctx* ctx, const rmb_results* res, const uint8_t* const* query, const uint32_t* qlen,
+                        const char* const* query_deflines, const char* const* subject_deflines,
+                        const char* db_name, int64_t db_mtime, int32_t parts, char** text, size_t* text_len,
+                        char* err, size_t errlen);
 
 void rmb_results_free(rmb_results* res);
 void rmb_text_free(void* p);

@@ -9,6 +9,7 @@
 // (rmblastn/tests/data/expected_*.tsv) and its chr22 stage goldens, see tests/.
 #pragma once
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 #include <utility>
@@ -202,6 +203,12 @@ GapAlign align_ex(const uint8_t* a, const uint8_t* b, size_t m, size_t n, int go
 AlignStats compute_align_stats(const std::vector<uint8_t>& q_iupac, const std::vector<uint8_t>& s_iupac);
 std::vector<uint8_t> to_iupac(const std::vector<uint8_t>& aligned);
 std::string format_tabular(const AlignResult& r, const std::vector<std::string>& fields);
+// pairwise output (outfmt 0, output.rs:369-720); query_mask: the query's DUST intervals
+std::string pairwise_program_header(const std::string& db_name, size_t n_seqs, uint64_t total);
+std::string pairwise_results(const std::vector<AlignResult>& res, const std::string& query_defline, uint32_t qlen,
+                             const std::map<std::string, std::string>* subject_deflines,
+                             const std::vector<std::pair<size_t, size_t>>& query_mask);
+std::string pairwise_footer(const std::string& db_name, size_t n_seqs, uint64_t total, int go, int ge);
 
 // ---- E-value statistics (rmb_oracle_stats.cpp) -----------------------------------------
 struct KaStats {  // gapped Karlin block + the length adjustment's alpha/beta; lambda <= 0: none

@@ -133,3 +133,212 @@ std::string format_tabular(const AlignResult& r, const std::vector<std::string>&
 }
 
 }  // namespace rmbo
+
+// ---- pairwise output (outfmt 0): rmblast-lib/src/output.rs:25-126, 369-720 ------------------
+namespace rmbo {
+
+std::string with_commas(uint64_t n) {  // output.rs:28 NStr::Int8ToString(n, fWithCommas)
+    std::string d = std::to_string(n), o;
+    for (size_t i = 0; i < d.size(); ++i) {
+        if (i > 0 && (d.size() - i) % 3 == 0) o.push_back(',');
+        o.push_back(d[i]);
+    }
+    return o;
+}
+
+// output.rs:44-106 ncbi_wrap_flat (NStr::Wrap with fWrap_FlatFile)
+std::vector<std::string> ncbi_wrap_flat(const std::string& s, size_t width) {
+    enum Score { Forced = 0, Punct = 1, Comma = 2, Space = 3, Newline = 4 };
+    const size_t len = s.size();
+    std::vector<std::string> lines;
+    size_t pos = 0;
+    while (pos < len) {
+        size_t column = 0, best_pos = SIZE_MAX;
+        int best = Forced;
+        size_t nl = s.find('\n', pos);
+        if (nl == std::string::npos) nl = len;
+        const size_t pos0 = (nl - pos <= width) ? nl : pos;
+        size_t pos2 = pos0;
+        while (pos2 < len && column <= width) {
+            const char c = s[pos2];
+            int score = Forced;
+            size_t score_pos = pos2;
+            if (c == '\n') {
+                best_pos = pos2;
+                best = Newline;
+                break;
+            } else if (isspace((unsigned char)c)) {
+                score = Space;
+            } else if (c == ',' && column < width && score_pos < len - 1) {
+                score = Comma;
+                ++score_pos;
+            } else if (c == '-' && score_pos < len - 1 && column < width) {
+                score = Punct;
+                ++score_pos;
+            }
+            if (score >= best && score_pos > pos0) {
+                best_pos = score_pos;
+                best = score;
+            }
+            ++pos2;
+            ++column;
+        }
+        if (best != Newline && column <= width) best_pos = len;
+        best_pos = std::max(std::min(best_pos, len), pos + 1);
+        lines.push_back(s.substr(pos, best_pos - pos));
+        pos = best_pos;
+        if (best == Space) {
+            while (pos < len && s[pos] == ' ') ++pos;
+            if (pos < len && s[pos] == '\n') ++pos;
+        } else if (best == Newline) {
+            ++pos;
+        }
+    }
+    if (lines.empty()) lines.push_back("");
+    return lines;
+}
+
+// output.rs:108-126 ncbi_wrap_title (s_WrapOutputLine): past every 60th character, break after
+// the next whitespace
+std::string ncbi_wrap_title(const std::string& s) {
+    if (s.size() <= 60) return s;
+    std::string o;
+    bool wrap = false;
+    for (size_t i = 0; i < s.size(); ++i) {
+        if (i > 0 && i % 60 == 0) wrap = true;
+        o.push_back(s[i]);
+        if (wrap && isspace((unsigned char)s[i])) {
+            o.push_back('\n');
+            wrap = false;
+        }
+    }
+    return o;
+}
+
+static uint32_t percent_match(uint32_t n, uint32_t d) {  // output.rs:369
+    if (d == 0) return 0;
+    if (n == d) return 100;
+    const uint32_t r = (uint32_t)(0.5 + 100.0 * n / d);
+    return std::min(r, 99u);
+}
+
+std::string pairwise_program_header(const std::string& db_name, size_t n_seqs, uint64_t total) {  // :431-455
+    std::string o = "RMBLASTN 2.17.1+\n\n\n";
+    o += "Reference: Robert M. Hubley, Arian Smit\nRMBlast - RepeatMasker Search Engine\n"
+         "2010 <http://www.repeatmasker.org>\n\n";
+    o += "Reference: Stephen F. Altschul, Thomas L. Madden, Alejandro A.\n"
+         "Schaffer, Jinghui Zhang, Zheng Zhang, Webb Miller, and David J.\n"
+         "Lipman (1997), \"Gapped BLAST and PSI-BLAST: a new generation of\n"
+         "protein database search programs\", Nucleic Acids Res. 25:3389-3402.\n\n\n\n";
+    o += "Database: ";
+    for (auto& l : ncbi_wrap_flat(db_name, 68)) o += l + "\n";
+    o += "           " + with_commas(n_seqs) + " sequences; " + with_commas(total) + " total letters\n\n\n\n";
+    return o;
+}
+
+static std::string pairwise_hsp(const AlignResult& r, const std::vector<std::pair<size_t, size_t>>& mask) {  // :509-653
+    const Hsp& h = r.hsp;
+    const AlignStats& st = r.stats;
+    const uint32_t aln_len = (uint32_t)h.q_seq.size();
+    const uint32_t n_ident = st.matches, n_gaps = st.query_gaps + st.subject_gaps;
+    char b[256];
+    std::string o;
+    o += " Score = " + std::to_string(h.score) + "\n";
+    snprintf(b, sizeof b, " Substitutions = %.2f%%, Query Gaps = %.2f%%, DB Gaps = %.2f%%\n", (double)st.perc_sub,
+             (double)st.perc_query_gap, (double)st.perc_db_gap);
+    o += b;
+    snprintf(b, sizeof b, " TransI/TransV = %u/%u,  CpG_sites = %u\n", st.transitions, st.transversions, st.cpg_sites);
+    o += b;
+    snprintf(b, sizeof b, " Kimura Div = %.2f%%, Kimura Div CpG Adjusted = %.2f%%\n", st.kdiv, st.cpg_kdiv);
+    o += b;
+    snprintf(b, sizeof b, " Identities = %u/%u (%u%%), Gaps = %u/%u (%u%%)\n", n_ident, aln_len,
+             percent_match(n_ident, aln_len), n_gaps, aln_len, percent_match(n_gaps, aln_len));
+    o += b;
+    o += std::string(" Strand=") + (h.strand == PLUS ? "Plus/Plus" : "Plus/Minus") + "\n\n";
+    std::vector<uint8_t> qi = to_iupac(h.q_seq), si = to_iupac(h.s_seq);
+    if (!mask.empty()) {
+        size_t q = h.q_start, m = 0;
+        while (m < mask.size() && mask[m].second < q) ++m;
+        for (auto& c : qi) {
+            if (c == '-') continue;
+            while (m < mask.size() && mask[m].second < q) ++m;
+            if (m < mask.size() && mask[m].first <= q) c = (uint8_t)tolower(c);
+            ++q;
+        }
+    }
+    const uint32_t maxc = std::max(h.q_end, h.s_end);
+    const int pos_w = (int)std::to_string(maxc).size();
+    uint32_t q_pos = h.q_start + 1;
+    uint32_t s_pos = h.strand == PLUS ? h.s_start + 1 : h.s_end;
+    for (size_t i = 0; i < qi.size(); i += 60) {
+        const size_t e = std::min(i + 60, qi.size());
+        uint32_t qn = 0, sn = 0;
+        std::string match;
+        for (size_t k = i; k < e; ++k) {
+            qn += qi[k] != '-';
+            sn += si[k] != '-';
+            match.push_back(qi[k] == '-' || si[k] == '-' ? ' ' : (tolower(qi[k]) == tolower(si[k]) ? '|' : ' '));
+        }
+        const uint32_t q_end_row = qn ? q_pos + qn - 1 : q_pos;
+        const uint32_t s_end_row = h.strand == PLUS ? (sn ? s_pos + sn - 1 : s_pos) : (sn ? s_pos - (sn - 1) : s_pos);
+        snprintf(b, sizeof b, "Query  %-*u  ", pos_w, q_pos);
+        o += b;
+        o.append((const char*)qi.data() + i, e - i);
+        o += "  " + std::to_string(q_end_row) + "\n";
+        o += std::string(9 + pos_w, ' ') + match + "\n";
+        snprintf(b, sizeof b, "Sbjct  %-*u  ", pos_w, s_pos);
+        o += b;
+        o.append((const char*)si.data() + i, e - i);
+        o += "  " + std::to_string(s_end_row) + "\n\n";
+        q_pos += qn;
+        if (h.strand == PLUS) s_pos += sn;
+        else s_pos = s_pos >= sn ? s_pos - sn : 0;
+    }
+    o += "\n";
+    return o;
+}
+
+// output.rs:684-720 write_pairwise_results (+ the query and subject headers, :469-505)
+std::string pairwise_results(const std::vector<AlignResult>& res, const std::string& query_defline, uint32_t qlen,
+                             const std::map<std::string, std::string>* subject_deflines,
+                             const std::vector<std::pair<size_t, size_t>>& query_mask) {
+    std::string d = query_defline;
+    while (!d.empty() && isspace((unsigned char)d.back())) d.pop_back();
+    std::string o = "Query= " + d + "\n\nLength=" + std::to_string(qlen) + "\n\n";
+    if (res.empty()) return o + "\n***** No hits found *****\n\n\n\n\n";
+    std::vector<std::string> order;
+    std::map<std::string, std::vector<const AlignResult*>> groups;
+    for (auto& r : res) {
+        auto it = groups.find(r.subject_id);
+        if (it == groups.end()) {
+            order.push_back(r.subject_id);
+            groups[r.subject_id].push_back(&r);
+        } else {
+            it->second.push_back(&r);
+        }
+    }
+    for (auto& id : order) {
+        const auto& g = groups[id];
+        std::string title;
+        if (subject_deflines) {
+            auto it = subject_deflines->find(id);
+            if (it != subject_deflines->end() && it->second.compare(0, id.size(), id) == 0 && it->second.size() > id.size())
+                title = it->second.substr(id.size() + 1);
+        }
+        o += ">" + id + " " + ncbi_wrap_title(title) + "\nLength=" + std::to_string(g[0]->hsp.s_len) + "\n\n";
+        for (auto* r : g) o += pairwise_hsp(*r, query_mask);
+    }
+    return o + "\n\n";
+}
+
+std::string pairwise_footer(const std::string& db_name, size_t n_seqs, uint64_t total, int go, int ge) {  // :666-680
+    std::string o = "  Database: ";
+    for (auto& l : ncbi_wrap_flat(db_name, 68)) o += l + "\n";
+    o += "  Number of letters in database: " + with_commas(total) + "\n";
+    o += "  Number of sequences in database:  " + with_commas(n_seqs) + "\n\n\n\n";
+    char b[128];
+    snprintf(b, sizeof b, "Matrix: blastn matrix 0 0\nGap Penalties: Existence: %d, Extension: %.2f\n", go, (double)ge);
+    return o + b;
+}
+
+}  // namespace rmbo

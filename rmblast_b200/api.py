@@ -129,6 +129,24 @@ def encode(ascii_seq: bytes | np.ndarray) -> np.ndarray:
     return out
 
 
+def read_fasta_records(text: str) -> list[tuple[str, str, bytes]]:
+    """seq/fasta.rs:83-150 FastaReader: (id, defline, sequence) per record; the defline is the
+    header after '>' with only its line ending removed."""
+    recs, head, buf = [], None, []
+    for line in text.split("\n"):
+        line = line.rstrip("\r")
+        if line.startswith(">"):
+            if head is not None:
+                recs.append((head.split()[0], head, "".join(buf).encode()))
+            head = line[1:]
+            buf = []
+        elif line.strip():
+            buf.append(line.strip())
+    if head is not None:
+        recs.append((head.split()[0], head, "".join(buf).encode()))
+    return recs
+
+
 def read_fasta(text: str) -> list[tuple[str, bytes]]:
     """seq/fasta.rs:83 FastaReader: (id, sequence) per record."""
     recs, name, buf = [], None, []
@@ -202,8 +220,10 @@ class SearchParams:
 class SubjectDb:
     """seq/mod.rs:155-291: subjects decoded once, ambiguity codes CRandom-resolved."""
 
-    def __init__(self, ids: list[str], plus: list[np.ndarray], masks: list[np.ndarray | None]):
+    def __init__(self, ids: list[str], plus: list[np.ndarray], masks: list[np.ndarray | None],
+                 deflines: list[str] | None = None):
         self.ids, self.plus, self.masks = ids, plus, masks
+        self.deflines = deflines  # full FASTA headers (None for a .2bit database: ids only)
 
     @classmethod
     def from_records(cls, recs: list[tuple[str, bytes | np.ndarray]]) -> "SubjectDb":
@@ -224,7 +244,65 @@ class SubjectDb:
 
     @classmethod
     def from_fasta(cls, text: str) -> "SubjectDb":
-        return cls.from_records(read_fasta(text))
+        recs = read_fasta_records(text)
+        db = cls.from_records([(i, s) for i, _, s in recs])
+        db.deflines = [d for _, d, _ in recs]
+        return db
+
+    @classmethod
+    def from_twobit(cls, path: str | Path) -> "SubjectDb":
+        """seq/twobit.rs: a UCSC .2bit database (either byte order), its N blocks CRandom-resolved
+        with n_mask = N, soft-mask blocks ignored."""
+        d = Path(path).read_bytes()
+        magic = int.from_bytes(d[0:4], "little")
+        order = "little" if magic == 0x1A412743 else "big" if magic == 0x4327411A else None
+        if order is None:
+            raise ValueError("not a .2bit file (bad signature)")
+        r32 = lambda p: int.from_bytes(d[p:p + 4], order)
+        count, pos = r32(8), 16
+        index = []
+        for _ in range(count):
+            nl = d[pos]
+            name = d[pos + 1:pos + 1 + nl].decode()
+            pos += 1 + nl
+            index.append((name, r32(pos)))
+            pos += 4
+        ucsc = np.array([3, 1, 0, 2], dtype=np.uint8)  # UCSC T, C, A, G -> BLASTNA
+        dt = np.dtype(np.uint32).newbyteorder("<" if order == "little" else ">")
+        ids, plus, masks = [], [], []
+        for name, off in index:
+            n, nb = r32(off), r32(off + 4)
+            starts = np.frombuffer(d, dtype=dt, count=nb, offset=off + 8).astype(np.uint32)
+            sizes = np.frombuffer(d, dtype=dt, count=nb, offset=off + 8 + 4 * nb).astype(np.uint32)
+            mb = r32(off + 8 + 8 * nb)
+            dna_off = off + 8 + 8 * nb + 4 + 8 * mb + 4
+            packed = np.frombuffer(d, dtype=np.uint8, count=(n + 3) // 4, offset=dna_off)
+            codes = np.stack([(packed >> s) & 3 for s in (6, 4, 2, 0)], axis=1).ravel()[:n]
+            p = np.full(n + 2, 15, dtype=np.uint8)
+            p[1:n + 1] = ucsc[codes]
+            m = np.zeros(max(n, 1), dtype=np.uint8)
+            if nb:
+                lib().rmb_resolve_twobit_n(n, nb, starts.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           sizes.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           p.ctypes.data_as(C.POINTER(C.c_uint8)), m.ctypes.data_as(C.POINTER(C.c_uint8)))
+            ids.append(name)
+            plus.append(p)
+            masks.append(m[:n] if nb else None)
+        return cls(ids, plus, masks)
+
+    def select(self, gilist: list[str]) -> "SubjectDb":
+        """main.rs:1444-1470: the subjects named in a gilist (a bare number also names "gi|n"),
+        in database order."""
+        keep = set()
+        for e in (x.strip() for x in gilist):
+            if not e:
+                continue
+            if e.isdigit():
+                keep.add("gi|" + e)
+            keep.add(e)
+        idx = [i for i, n in enumerate(self.ids) if n in keep]
+        return SubjectDb([self.ids[i] for i in idx], [self.plus[i] for i in idx], [self.masks[i] for i in idx],
+                         [self.deflines[i] for i in idx] if self.deflines else None)
 
     def total_letters(self) -> int:
         return sum(len(p) - 2 for p in self.plus)
@@ -255,6 +333,25 @@ class Results:
                 h = r.hsps[k]
                 out.append({f: getattr(h, f) for f, _ in _Hsp._fields_} | {"query": q})
         return out
+
+    def pairwise(self, queries: list[np.ndarray], query_deflines: list[str], db_name: str, parts: int = 3,
+                 db_mtime: int = -1) -> str:
+        """rmb_format_pairwise: outfmt 0 for these results (header and footer by `parts`)."""
+        s = self._s
+        n = len(query_deflines)
+        qp = _ptr_array(queries) if queries else None
+        ql = (C.c_uint32 * max(n, 1))(*[len(q) - 2 for q in queries]) if queries else (C.c_uint32 * max(n, 1))()
+        qd = (C.c_char_p * max(n, 1))(*[d.encode() for d in query_deflines])
+        sd = (C.c_char_p * len(s.db.ids))(*[d.encode() for d in s.db.deflines]) if s.db.deflines else None
+        txt = C.c_void_p()
+        size = C.c_size_t()
+        err = C.create_string_buffer(512)
+        _check(lib().rmb_format_pairwise(s._ctx, self._p, qp, ql, qd, sd, db_name.encode(), C.c_int64(db_mtime),
+                                         parts, C.byref(txt), C.byref(size), err, 512), err)
+        try:
+            return C.string_at(txt.value, size.value).decode()
+        finally:
+            lib().rmb_text_free(txt)
 
     def tabular(self, outfmt: str) -> str:
         ids = (C.c_char_p * max(1, len(self.query_ids)))(*[i.encode() for i in self.query_ids])

@@ -1130,6 +1130,26 @@ void merge_chunk_prelims(std::vector<Prelim>& acc, std::vector<Prelim>& add, uin
         if (!absorbed[j]) acc.push_back(add[j]);
 }
 
+// One result record back to the host hit the formatters take.
+void hit_from_record(const rmb_results* R, uint64_t k, Hit& h) {
+    const rmb_hsp& x = R->hsps[k];
+    h.score = x.score;
+    h.q_start = x.q_start; h.q_end = x.q_end; h.q_len = x.q_len;
+    h.s_start = x.s_start; h.s_end = x.s_end; h.s_len = x.s_len;
+    h.oid = x.subject_oid;
+    h.strand = (uint8_t)x.strand;
+    h.stats.matches = x.matches; h.stats.mismatches = x.mismatches;
+    h.stats.query_gaps = x.query_gaps; h.stats.subject_gaps = x.subject_gaps;
+    h.stats.transitions = x.transitions; h.stats.transversions = x.transversions;
+    h.stats.cpg_sites = x.cpg_sites;
+    h.stats.perc_sub = x.perc_sub; h.stats.perc_query_gap = x.perc_query_gap;
+    h.stats.perc_db_gap = x.perc_db_gap;
+    h.stats.kdiv = x.kdiv; h.stats.cpg_kdiv = x.cpg_kdiv;
+    h.evalue = x.evalue; h.bitscore = x.bitscore;
+    h.q_seq.assign(R->q_seq + x.seq_off, R->q_seq + x.seq_off + x.aln_len);
+    h.s_seq.assign(R->s_seq + x.seq_off, R->s_seq + x.seq_off + x.aln_len);
+}
+
 QueriesPtr subset_queries(rmb_ctx& C, const std::vector<const uint8_t*>& ptr, const std::vector<uint32_t>& len) {
     return QueriesPtr(make_queries(&C, (uint32_t)ptr.size(), ptr.data(), len.data()));
 }
@@ -1413,6 +1433,72 @@ int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const 
     }
 }
 
+int rmb_format_pairwise(rmb_ctx* C, const rmb_results* R, const uint8_t* const* query, const uint32_t* qlen,
+                        const char* const* query_deflines, const char* const* subject_deflines,
+                        const char* db_name, int64_t db_mtime, int32_t parts, char** text, size_t* text_len, char* err,
+                        size_t errlen) {
+    try {
+        if (!C || !R || !text || !db_name) throw Fail(RMB_EINVAL, "null argument");
+        if (R->n_queries && (!query_deflines || !qlen)) throw Fail(RMB_EINVAL, "query deflines and lengths are needed");
+        CK(cudaSetDevice(C->p.device));
+        // the query's DUST intervals print in lower case (main.rs:948-956): the device masker's
+        // interval bitmap over the plain (single-chunk) intervals
+        std::vector<uint32_t> bits;
+        std::vector<uint64_t> bits_off(R->n_queries + 1, 0);
+        if (C->p.dust && R->n_queries) {
+            if (!query) throw Fail(RMB_EINVAL, "with dust on, the query sequences are needed");
+            QueriesPtr QH(make_queries(C, R->n_queries, query, qlen));
+            for (uint32_t i = 0; i < R->n_queries; ++i) bits_off[i + 1] = bits_off[i] + (qlen[i] + 31) / 32;
+            DBuf d_bits, d_off;
+            d_bits.ensure(std::max<uint64_t>(bits_off.back(), 1) * 4);
+            upload(d_off, bits_off, C->st);
+            CK(cudaMemsetAsync(d_bits.p, 0, std::max<uint64_t>(bits_off.back(), 1) * 4, C->st));
+            const uint32_t nt = dust_threads(R->n_queries, C->sms);
+            C->dust_scratch.ensure(dust_scratch_bytes(nt));
+            C->fails.ensure(16);
+            CK(cudaMemsetAsync(C->fails.p, 0, 4, C->st));
+            CK(launch_dust(QH->d_q.as<uint8_t>(), QH->d_off.as<uint64_t>(), QH->d_len.as<uint32_t>(), R->n_queries,
+                           nullptr, C->dust_scratch.p, nt, C->fails.as<unsigned int>(), false, C->st,
+                           d_bits.as<uint32_t>(), d_off.as<uint64_t>()));
+            bits.resize(std::max<uint64_t>(bits_off.back(), 1));
+            unsigned int over = 0;
+            CK(cudaMemcpyAsync(bits.data(), d_bits.p, bits.size() * 4, cudaMemcpyDeviceToHost, C->st));
+            CK(cudaMemcpyAsync(&over, C->fails.p, 4, cudaMemcpyDeviceToHost, C->st));
+            CK(cudaStreamSynchronize(C->st));
+            d_bits.release();
+            d_off.release();
+            if (over) throw Fail(RMB_ELIMIT, "DUST interval list outgrew its fixed capacity");
+        }
+        std::string out;
+        if (parts & 1) out += pairwise_header(db_name, C->ids.size(), C->total_letters);
+        std::vector<Hit> hits;
+        for (uint32_t qi = 0; qi < R->n_queries; ++qi) {
+            hits.clear();
+            for (uint64_t k = R->query_off[qi]; k < R->query_off[qi + 1]; ++k) {
+                hits.emplace_back();
+                hit_from_record(R, k, hits.back());
+            }
+            pairwise_query(out, hits, query_deflines[qi], qlen[qi], C->ids, subject_deflines,
+                           bits.empty() ? nullptr : bits.data() + bits_off[qi]);
+        }
+        if (parts & 2)
+            out += pairwise_footer(db_name, C->ids.size(), C->total_letters, db_mtime, C->p.gap_open, C->p.gap_extend);
+        char* o = (char*)malloc(out.size() + 1);
+        if (!o) throw std::bad_alloc();
+        memcpy(o, out.data(), out.size());
+        o[out.size()] = 0;
+        *text = o;
+        if (text_len) *text_len = out.size();
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
 int rmb_format_tabular(const rmb_ctx* C, const rmb_results* R, const char* const* query_ids, const char* outfmt,
                        char** text, size_t* text_len, char* err, size_t errlen) {
     try {
@@ -1430,21 +1516,7 @@ int rmb_format_tabular(const rmb_ctx* C, const rmb_results* R, const char* const
             const std::string qid = query_ids ? query_ids[qi] : ("query" + std::to_string(qi));
             for (uint64_t k = R->query_off[qi]; k < R->query_off[qi + 1]; ++k) {
                 const rmb_hsp& x = R->hsps[k];
-                h.score = x.score;
-                h.q_start = x.q_start; h.q_end = x.q_end; h.q_len = x.q_len;
-                h.s_start = x.s_start; h.s_end = x.s_end; h.s_len = x.s_len;
-                h.oid = x.subject_oid;
-                h.strand = (uint8_t)x.strand;
-                h.stats.matches = x.matches; h.stats.mismatches = x.mismatches;
-                h.stats.query_gaps = x.query_gaps; h.stats.subject_gaps = x.subject_gaps;
-                h.stats.transitions = x.transitions; h.stats.transversions = x.transversions;
-                h.stats.cpg_sites = x.cpg_sites;
-                h.stats.perc_sub = x.perc_sub; h.stats.perc_query_gap = x.perc_query_gap;
-                h.stats.perc_db_gap = x.perc_db_gap;
-                h.stats.kdiv = x.kdiv; h.stats.cpg_kdiv = x.cpg_kdiv;
-                h.evalue = x.evalue; h.bitscore = x.bitscore;
-                h.q_seq.assign(R->q_seq + x.seq_off, R->q_seq + x.seq_off + x.aln_len);
-                h.s_seq.assign(R->s_seq + x.seq_off, R->s_seq + x.seq_off + x.aln_len);
+                hit_from_record(R, k, h);
                 if (!format_line(out, h, qid, C->ids.at(x.subject_oid), fields))
                     throw Fail(RMB_EINVAL, "unknown -outfmt field");
                 out.push_back('\n');

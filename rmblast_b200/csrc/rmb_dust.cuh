@@ -219,16 +219,21 @@ struct DustTriplets {
 // dust.rs:284-331 result list: only its last interval is ever extended, so an interval is final
 // (and masked) once the next one starts
 struct DustMasker {
-    uint8_t* out;  // masked copy of the query bases (no sentinel), length n
+    uint8_t* out;    // masked copy of the query bases (no sentinel), length n; or null
+    uint32_t* bits;  // or null: bit p set for every position inside an interval (the plain
+                     // intervals, which pairwise output prints in lower case)
     uint32_t n;
-    bool compat;   // the multi-chunk path's off-by-one: also mask e + 1 (dust.rs:614-630)
+    bool compat;     // the multi-chunk path's off-by-one: also mask e + 1 (dust.rs:614-630)
     bool has;
     uint32_t cs, ce;
     RMB_HD void flush() {
         if (!has) return;
         const uint32_t end = ce < n - 1 ? ce : n - 1;
-        for (uint32_t p = cs; p <= end; ++p) out[p] = 14;
-        if (compat && ce + 1 < n) out[ce + 1] = 14;
+        for (uint32_t p = cs; p <= end; ++p) {
+            if (out) out[p] = 14;
+            if (bits) bits[p >> 5] |= 1u << (p & 31);
+        }
+        if (out && compat && ce + 1 < n) out[ce + 1] = 14;
     }
     RMB_HD void save(DustPerfectList& perfect, uint32_t wstart) {
         if (perfect.size == 0) return;
@@ -252,12 +257,13 @@ struct DustMasker {
 // out[0..n) (out holds a copy of bases); `compat` adds the multi-chunk path's extra base after
 // each interval (dust.rs:614-630).  `scratch` holds DUST_PERFECT_CAP entries.  Returns false
 // if the perfect list would have outgrown its ring (then `out` is incomplete).
-RMB_HD bool dust_query(const uint8_t* bases, uint32_t n, uint8_t* out, DustPerfect* scratch, bool compat = false) {
+RMB_HD bool dust_query(const uint8_t* bases, uint32_t n, uint8_t* out, DustPerfect* scratch, bool compat = false,
+                       uint32_t* bits = nullptr) {
     if (n < 3) return true;
     DustRng rng;
     rng.init();
     DustPerfectList perfect{scratch, 0, 0, false};
-    DustMasker mk{out, n, compat, false, 0, 0};
+    DustMasker mk{out, bits, n, compat, false, 0, 0};
     DustTriplets w;
     uint8_t conv[8];
     uint32_t j_start = 0;

@@ -1071,6 +1071,225 @@ void append_bitscore(std::string& out, double b) {
     out += buf;
 }
 
+// ---------------------------------------------------------------------------------------
+// Pairwise output, outfmt 0 (rmblast-lib/src/output.rs:25-126, 369-720)
+// ---------------------------------------------------------------------------------------
+static std::string commas(uint64_t n) {  // NStr::Int8ToString(n, fWithCommas)
+    const std::string d = std::to_string(n);
+    std::string o;
+    for (size_t i = 0; i < d.size(); ++i) {
+        if (i > 0 && (d.size() - i) % 3 == 0) o.push_back(',');
+        o.push_back(d[i]);
+    }
+    return o;
+}
+
+// NStr::Wrap(fWrap_FlatFile) as output.rs:44-106: break after a space, a comma or a hyphen
+// (spaces preferred), forced at `width`
+static std::vector<std::string> wrap_flat(const std::string& s, size_t width) {
+    const size_t len = s.size();
+    std::vector<std::string> lines;
+    size_t pos = 0;
+    while (pos < len) {
+        size_t column = 0, best_pos = SIZE_MAX;
+        int best = 0;  // 0 forced, 1 hyphen, 2 comma, 3 space, 4 newline
+        size_t nl = s.find('\n', pos);
+        if (nl == std::string::npos) nl = len;
+        const size_t pos0 = nl - pos <= width ? nl : pos;
+        for (size_t p2 = pos0; p2 < len && column <= width; ++p2, ++column) {
+            const char c = s[p2];
+            int score = 0;
+            size_t sp = p2;
+            if (c == '\n') {
+                best_pos = p2;
+                best = 4;
+                break;
+            }
+            if (std::isspace((unsigned char)c)) score = 3;
+            else if (c == ',' && column < width && sp < len - 1) { score = 2; ++sp; }
+            else if (c == '-' && sp < len - 1 && column < width) { score = 1; ++sp; }
+            if (score >= best && sp > pos0) {
+                best_pos = sp;
+                best = score;
+            }
+        }
+        if (best != 4 && column <= width) best_pos = len;
+        best_pos = std::max(std::min(best_pos, len), pos + 1);
+        lines.push_back(s.substr(pos, best_pos - pos));
+        pos = best_pos;
+        if (best == 3) {
+            while (pos < len && s[pos] == ' ') ++pos;
+            if (pos < len && s[pos] == '\n') ++pos;
+        } else if (best == 4) {
+            ++pos;
+        }
+    }
+    if (lines.empty()) lines.push_back("");
+    return lines;
+}
+
+// s_WrapOutputLine as output.rs:108-126: past every 60th character, a break after the next
+// whitespace character
+static std::string wrap_title(const std::string& s) {
+    if (s.size() <= 60) return s;
+    std::string o;
+    bool wrap = false;
+    for (size_t i = 0; i < s.size(); ++i) {
+        if (i > 0 && i % 60 == 0) wrap = true;
+        o.push_back(s[i]);
+        if (wrap && std::isspace((unsigned char)s[i])) {
+            o.push_back('\n');
+            wrap = false;
+        }
+    }
+    return o;
+}
+
+static uint32_t pct(uint32_t n, uint32_t d) {  // output.rs:369 get_percent_match
+    if (d == 0) return 0;
+    if (n == d) return 100;
+    return std::min((uint32_t)(0.5 + 100.0 * n / d), 99u);
+}
+
+std::string pairwise_header(const std::string& db_name, uint64_t n_seqs, uint64_t letters) {
+    std::string o = "RMBLASTN 2.17.1+\n\n\n"
+                    "Reference: Robert M. Hubley, Arian Smit\n"
+                    "RMBlast - RepeatMasker Search Engine\n"
+                    "2010 <http://www.repeatmasker.org>\n\n"
+                    "Reference: Stephen F. Altschul, Thomas L. Madden, Alejandro A.\n"
+                    "Schaffer, Jinghui Zhang, Zheng Zhang, Webb Miller, and David J.\n"
+                    "Lipman (1997), \"Gapped BLAST and PSI-BLAST: a new generation of\n"
+                    "protein database search programs\", Nucleic Acids Res. 25:3389-3402.\n\n\n\n"
+                    "Database: ";
+    for (const auto& l : wrap_flat(db_name, 68)) o += l + "\n";
+    o += "           " + commas(n_seqs) + " sequences; " + commas(letters) + " total letters\n\n\n\n";
+    return o;
+}
+
+// One HSP (output.rs:509-653): the statistics block, then rows of 60 columns.  qmask: bit p set
+// when query position p lies in a DUST interval (printed in lower case), or null.
+static void pairwise_hsp(std::string& o, const Hit& h, const uint32_t* qmask) {
+    const Stats& st = h.stats;
+    const uint32_t aln = (uint32_t)h.q_seq.size();
+    const uint32_t ident = st.matches, gaps = st.query_gaps + st.subject_gaps;
+    char b[256];
+    o += " Score = " + std::to_string(h.score) + "\n";
+    snprintf(b, sizeof b, " Substitutions = %.2f%%, Query Gaps = %.2f%%, DB Gaps = %.2f%%\n", (double)st.perc_sub,
+             (double)st.perc_query_gap, (double)st.perc_db_gap);
+    o += b;
+    snprintf(b, sizeof b, " TransI/TransV = %u/%u,  CpG_sites = %u\n", st.transitions, st.transversions,
+             st.cpg_sites);
+    o += b;
+    snprintf(b, sizeof b, " Kimura Div = %.2f%%, Kimura Div CpG Adjusted = %.2f%%\n", st.kdiv, st.cpg_kdiv);
+    o += b;
+    snprintf(b, sizeof b, " Identities = %u/%u (%u%%), Gaps = %u/%u (%u%%)\n", ident, aln, pct(ident, aln), gaps, aln,
+             pct(gaps, aln));
+    o += b;
+    o += h.strand == 0 ? " Strand=Plus/Plus\n\n" : " Strand=Plus/Minus\n\n";
+    std::string qs(aln, ' '), ss(aln, ' ');
+    uint32_t qp = h.q_start;
+    for (uint32_t i = 0; i < aln; ++i) {
+        qs[i] = h.q_seq[i] == 15 ? '-' : IUPAC[h.q_seq[i] & 15];
+        ss[i] = h.s_seq[i] == 15 ? '-' : IUPAC[h.s_seq[i] & 15];
+        if (qs[i] != '-') {
+            if (qmask && ((qmask[qp >> 5] >> (qp & 31)) & 1u)) qs[i] = (char)std::tolower((unsigned char)qs[i]);
+            ++qp;
+        }
+    }
+    const int w = (int)std::to_string(std::max(h.q_end, h.s_end)).size();
+    uint32_t q_pos = h.q_start + 1, s_pos = h.strand == 0 ? h.s_start + 1 : h.s_end;
+    for (uint32_t i = 0; i < aln; i += 60) {
+        const uint32_t e = std::min(i + 60, aln);
+        uint32_t qn = 0, sn = 0;
+        std::string mid;
+        for (uint32_t k = i; k < e; ++k) {
+            qn += qs[k] != '-';
+            sn += ss[k] != '-';
+            const bool same = qs[k] != '-' && ss[k] != '-' &&
+                              std::tolower((unsigned char)qs[k]) == std::tolower((unsigned char)ss[k]);
+            mid.push_back(same ? '|' : ' ');
+        }
+        const uint32_t q_last = qn ? q_pos + qn - 1 : q_pos;
+        const uint32_t s_last = h.strand == 0 ? (sn ? s_pos + sn - 1 : s_pos) : (sn ? s_pos - (sn - 1) : s_pos);
+        snprintf(b, sizeof b, "Query  %-*u  ", w, q_pos);
+        o += b;
+        o.append(qs, i, e - i);
+        o += "  " + std::to_string(q_last) + "\n" + std::string(9 + w, ' ') + mid + "\n";
+        snprintf(b, sizeof b, "Sbjct  %-*u  ", w, s_pos);
+        o += b;
+        o.append(ss, i, e - i);
+        o += "  " + std::to_string(s_last) + "\n\n";
+        q_pos += qn;
+        if (h.strand == 0) s_pos += sn;
+        else s_pos = s_pos >= sn ? s_pos - sn : 0;
+    }
+    o += "\n";
+}
+
+void pairwise_query(std::string& o, const std::vector<Hit>& hits, const std::string& defline, uint32_t qlen,
+                    const std::vector<std::string>& subject_ids, const char* const* subject_deflines,
+                    const uint32_t* qmask) {
+    std::string d = defline;  // NCBI trims a query's defline, not a subject's
+    while (!d.empty() && std::isspace((unsigned char)d.back())) d.pop_back();
+    o += "Query= " + d + "\n\nLength=" + std::to_string(qlen) + "\n\n";
+    if (hits.empty()) {
+        o += "\n***** No hits found *****\n\n\n\n\n";
+        return;
+    }
+    std::vector<uint32_t> order;  // subjects in order of first appearance
+    std::map<uint32_t, std::vector<const Hit*>> groups;
+    for (const Hit& h : hits) {
+        auto& g = groups[h.oid];
+        if (g.empty()) order.push_back(h.oid);
+        g.push_back(&h);
+    }
+    for (uint32_t oid : order) {
+        const std::string& id = subject_ids.at(oid);
+        std::string title;
+        if (subject_deflines && subject_deflines[oid]) {
+            const std::string dl = subject_deflines[oid];
+            if (dl.compare(0, id.size(), id) == 0 && dl.size() > id.size()) title = dl.substr(id.size() + 1);
+        }
+        const auto& g = groups[oid];
+        o += ">" + id + " " + wrap_title(title) + "\nLength=" + std::to_string(g[0]->s_len) + "\n\n";
+        for (const Hit* h : g) pairwise_hsp(o, *h, qmask);
+    }
+    o += "\n\n";
+}
+
+// output.rs:379-411 format_ncbi_date: "Mon D, YYYY  H:MM AM/PM" (UTC), days-to-civil by the
+// published public-domain algorithm of H. Hinnant
+static std::string ncbi_date(uint64_t secs) {
+    static const char* MON[12] = {"Jan", "Feb", "Mar", "Apr", "May", "Jun", "Jul", "Aug", "Sep", "Oct", "Nov", "Dec"};
+    const uint64_t tod = secs % 86400, minute = (tod / 60) % 60, hour = tod / 3600;
+    const int64_t z = (int64_t)(secs / 86400) + 719468;
+    const int64_t era = (z >= 0 ? z : z - 146096) / 146097;
+    const int64_t doe = z - era * 146097;
+    const int64_t yoe = (doe - doe / 1460 + doe / 36524 - doe / 146096) / 365;
+    const int64_t doy = doe - (365 * yoe + yoe / 4 - yoe / 100);
+    const int64_t mp = (5 * doy + 2) / 153;
+    const int64_t d = doy - (153 * mp + 2) / 5 + 1;
+    const int64_t m = mp < 10 ? mp + 3 : mp - 9;
+    const int64_t y = yoe + era * 400 + (m <= 2 ? 1 : 0);
+    const uint64_t h12 = hour == 0 ? 12 : hour <= 12 ? hour : hour - 12;
+    char b[64];
+    snprintf(b, sizeof b, "%s %lld, %lld  %llu:%02llu %s", MON[m - 1], (long long)d, (long long)y,
+             (unsigned long long)h12, (unsigned long long)minute, hour < 12 ? "AM" : "PM");
+    return b;
+}
+
+std::string pairwise_footer(const std::string& db_name, uint64_t n_seqs, uint64_t letters, int64_t mtime, int go,
+                            int ge) {
+    std::string o = "  Database: ";
+    for (const auto& l : wrap_flat(db_name, 68)) o += l + "\n";
+    if (mtime >= 0) o += "    Posted date:  " + ncbi_date((uint64_t)mtime) + "\n";
+    o += "  Number of letters in database: " + commas(letters) + "\n";
+    o += "  Number of sequences in database:  " + commas(n_seqs) + "\n\n\n\n";
+    char b[128];
+    snprintf(b, sizeof b, "Matrix: blastn matrix 0 0\nGap Penalties: Existence: %d, Extension: %.2f\n", go, (double)ge);
+    return o + b;
+}
+
 int choose_lut_width(int ws, uint64_t e) {  // blast/nalookup.rs:254-291
     if (ws >= 4 && ws <= 6) return ws;
     switch (ws) {

@@ -110,6 +110,15 @@ int64_t eff_searchsp(const KaBlock& kb, int32_t qlen, int64_t db_len, int32_t db
 double hsp_evalue(int32_t score, const KaBlock& kb, int64_t searchsp);
 double hsp_bitscore(int32_t score, const KaBlock& kb);
 void append_evalue(std::string& out, double e);
+// pairwise output (outfmt 0): the program header, one query's block (hits in output order;
+// subject_deflines indexed by oid, or null for id-only databases; qmask: one bit per query
+// position inside a DUST interval, or null), and the footer (mtime < 0: no "Posted date")
+std::string pairwise_header(const std::string& db_name, uint64_t n_seqs, uint64_t letters);
+void pairwise_query(std::string& out, const std::vector<Hit>& hits, const std::string& defline, uint32_t qlen,
+                    const std::vector<std::string>& subject_ids, const char* const* subject_deflines,
+                    const uint32_t* qmask);
+std::string pairwise_footer(const std::string& db_name, uint64_t n_seqs, uint64_t letters, int64_t mtime, int go,
+                            int ge);
 void append_bitscore(std::string& out, double b);
 int ungapped_cutoff_for(const std::string& matrix_name, int go, int ge, int min_raw, uint64_t qlen, uint64_t avg);
 Stats align_stats(const std::vector<uint8_t>& q, const std::vector<uint8_t>& s);

@@ -1,5 +1,6 @@
 // rmb_io.cpp -- input preparation entry points of include/rmb_gpu.h: matrix parsing, IUPAC
 // encoding and CRandom resolution of subject ambiguity codes.
+#include <algorithm>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -101,6 +102,22 @@ void rmb_resolve_subject(const uint8_t* raw, uint32_t n, uint8_t* plus, uint8_t*
         plus[i] = c == 14 ? (uint8_t)(r & 3) : ALLOWED[c][1 + r % ALLOWED[c][0]];
         n_mask[i - 1] = c;
         *has_mask = 1;
+    }
+}
+
+// seq/twobit.rs:73-135 (the .2bit path of SubjectDb): the N blocks of a .2bit record, drawn from
+// CRandom seeded with the record's length, block by block in file order; n_mask gets 14 there.
+void rmb_resolve_twobit_n(uint32_t n, uint32_t n_blocks, const uint32_t* starts, const uint32_t* sizes,
+                          uint8_t* plus, uint8_t* n_mask) {
+    if (!n_blocks) return;
+    CRandom rng(n);
+    for (uint32_t b = 0; b < n_blocks; ++b) {
+        const uint64_t e64 = std::min<uint64_t>((uint64_t)starts[b] + sizes[b], n);
+        const uint32_t e = (uint32_t)e64, st = std::min(starts[b], e);
+        for (uint32_t p = st; p < e; ++p) {
+            plus[p + 1] = (uint8_t)((rng.next() >> 1) & 3u);
+            n_mask[p] = 14;
+        }
     }
 }
 

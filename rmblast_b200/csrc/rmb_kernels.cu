@@ -2079,11 +2079,13 @@ cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t
 __global__ void __launch_bounds__(32) k_dust(const uint8_t* __restrict__ q, const uint64_t* __restrict__ off,
                                              const uint32_t* __restrict__ len, uint32_t nq, uint8_t* __restrict__ qm,
                                              DustPerfect* __restrict__ scratch, uint32_t nworkers,
-                                             unsigned int* __restrict__ overflow, bool compat) {
+                                             unsigned int* __restrict__ overflow, bool compat,
+                                             uint32_t* __restrict__ bits, const uint64_t* __restrict__ bits_off) {
     if (threadIdx.x != 0 || blockIdx.x >= nworkers) return;
     for (uint32_t i = blockIdx.x; i < nq; i += nworkers) {
         const uint64_t o = off[i] + 1;
-        if (!dust_query(q + o, len[i], qm + o, scratch + (uint64_t)blockIdx.x * DUST_PERFECT_CAP, compat))
+        if (!dust_query(q + o, len[i], qm ? qm + o : nullptr, scratch + (uint64_t)blockIdx.x * DUST_PERFECT_CAP,
+                        compat, bits ? bits + bits_off[i] : nullptr))
             atomicAdd(overflow, 1u);
     }
 }
@@ -2095,9 +2097,11 @@ uint32_t dust_threads(uint32_t nq, int sms) {
 size_t dust_scratch_bytes(uint32_t nthreads) { return (size_t)nthreads * DUST_PERFECT_CAP * sizeof(DustPerfect); }
 
 cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
-                        void* scratch, uint32_t nthreads, unsigned int* overflow, bool compat, cudaStream_t st) {
+                        void* scratch, uint32_t nthreads, unsigned int* overflow, bool compat, cudaStream_t st,
+                        uint32_t* bits, const uint64_t* bits_off) {
     if (!nq || !nthreads) return cudaSuccess;
-    k_dust<<<nthreads, 32, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow, compat);
+    k_dust<<<nthreads, 32, 0, st>>>(q, off, len, nq, qm, (DustPerfect*)scratch, nthreads, overflow, compat, bits,
+                                    bits_off);
     return cudaGetLastError();
 }
 }  // namespace rmb

@@ -90,9 +90,11 @@ cudaError_t launch_revcomp(const uint8_t* q, const uint64_t* off, const uint32_t
                            cudaStream_t st);
 // DUST masking of a query batch: qm must hold a copy of q; `scratch` holds
 // dust_scratch_bytes(nthreads); overflow counts queries whose interval list overflowed; compat
-// adds the multi-chunk path's extra masked base after each interval.
+// adds the multi-chunk path's extra masked base after each interval.  qm may be null; bits
+// (zeroed, per query at word offset bits_off[i]) gets one bit per position inside an interval.
 uint32_t dust_threads(uint32_t nq, int sms);
 size_t dust_scratch_bytes(uint32_t nthreads);
 cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* len, uint32_t nq, uint8_t* qm,
-                        void* scratch, uint32_t nthreads, unsigned int* overflow, bool compat, cudaStream_t st);
+                        void* scratch, uint32_t nthreads, unsigned int* overflow, bool compat, cudaStream_t st,
+                        uint32_t* bits = nullptr, const uint64_t* bits_off = nullptr);
 }  // namespace rmb

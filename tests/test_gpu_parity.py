@@ -355,3 +355,98 @@ def test_evalues_and_reap_match_oracle(case):
     if p.get("evalue"):
         unreaped, _, _ = O.search_text(qf, dbf, mt, name, dict(p, evalue=0.0), STATS_FIELDS)
         assert unreaped.count("\n") > txt.count("\n")  # the cut dropped some HSPs
+
+
+PAIRWISE_RM = dict(O.RM_PARAMS, mask_level=80, complexity_adjust=1, dust=1)
+PAIRWISE_DEFAULTS = dict(gap_open=20, gap_extend=5, word_size=11, xdrop_ungap=20, xdrop_gap=30,
+                         xdrop_gap_final=100, min_raw_gapped_score=0, mask_level=101, dust=1)
+
+
+@pytest.mark.parametrize("name,p", [("defaults", PAIRWISE_DEFAULTS), ("rm", PAIRWISE_RM)])
+def test_pairwise_goldens_through_c_abi(name, p):
+    """Pairwise output (outfmt 0) of the device search against NCBI 2.17.1 (cli.rs:197-212): the
+    statistics blocks, alignment rows, DUST-masked query bases in lower case, headers and footer;
+    the "Posted date" line (the database file's time) is left out as in the reference's test."""
+    s = searcher(p, (G / "comparison.matrix").read_text(), "comparison.matrix", (G / "db.fa").read_text())
+    recs = api.read_fasta_records((G / "query.fa").read_text())
+    enc = [api.encode(x) for _, _, x in recs]
+    res = s.search(enc, [i for i, _, _ in recs])
+    txt = res.pairwise(enc, [d for _, d, _ in recs], "db.fa")
+    want = "".join(ln for ln in (G / f"expected_pairwise_{name}.ncbi-2.17.1.txt").read_text().splitlines(True)
+                   if not ln.startswith("    Posted date:"))
+    assert txt == want
+
+
+def test_twobit_databases_match_oracle(tmp_path):
+    """Searches against .2bit databases (seq/twobit.rs): the reference's alu.2bit, and a synthetic
+    library with N blocks, each against the oracle's own .2bit reader."""
+    from twobit_util import write_twobit
+    import re
+    qf = (G / "query.fa").read_text()
+    _, db, _ = synth.workload("small", scale=0.3)
+    rng = np.random.default_rng(9)
+    recs = []
+    for n, sq in db:
+        b = bytearray(sq.tobytes())
+        for _ in range(2):
+            a = int(rng.integers(0, len(b)))
+            b[a:a + 30] = b"N" * len(b[a:a + 30])
+        recs.append((n, bytes(b)))
+    syn = tmp_path / "lib.2bit"
+    write_twobit(syn, recs)
+    sq, _, prm = synth.workload("small", scale=0.3)
+    sqf = synth.to_fasta([n for n, _ in sq], [x for _, x in sq])
+    cases = [(G / "alu.2bit", qf, (G / "comparison.matrix").read_text(), "comparison.matrix",
+              dict(O.RM_PARAMS, mask_level=80, complexity_adjust=1, dust=1)),
+             (syn, sqf, synth.MATRIX_TEXT, synth.MATRIX_NAME, dict(prm, **synth.RM_FLAGS))]
+    for path, q, mt, mname, p in cases:
+        m = api.ScoreMatrix.from_text(mt, mname)
+        sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
+                              xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"],
+                              xdrop_gap_final=p["xdrop_gap_final"], min_raw_gapped_score=p["min_raw_gapped_score"],
+                              complexity_adjust=bool(p.get("complexity_adjust")), dust=bool(p.get("dust")),
+                              mask_level=p.get("mask_level", -1))
+        s = api.Searcher(sp, m, api.SubjectDb.from_twobit(path))
+        qr = api.read_fasta(q)
+        got = s.search([api.encode(x) for _, x in qr], [n for n, _ in qr]).tabular(FIELDS)
+        mfile = tmp_path / mname
+        mfile.write_text(mt)
+        qfile = tmp_path / "q.fa"
+        qfile.write_text(q)
+        args = ["--db", str(path), "--query", str(qfile), "--matrix", str(mfile), "--gapopen", str(p["gap_open"]),
+                "--gapextend", str(p["gap_extend"]), "--word-size", str(p["word_size"]),
+                "--xdrop-ungap", str(p["xdrop_ungap"]), "--xdrop-gap", str(p["xdrop_gap"]),
+                "--xdrop-gap-final", str(p["xdrop_gap_final"]),
+                "--min-raw-gapped-score", str(p["min_raw_gapped_score"]), "--dust", "yes" if p.get("dust") else "no",
+                "--mask-level", str(p.get("mask_level", 101)), "--outfmt", FIELDS, "--num-threads", "8"]
+        if p.get("complexity_adjust"):
+            args.append("--complexity-adjust")
+        want = O.run_cli(args)
+        assert got.count("\n") > 2
+        assert got == want
+
+
+def test_gilist_matches_oracle(tmp_path):
+    qf, dbf, p = synthetic("small", 0.3, synth.RM_FLAGS)
+    sdb = api.SubjectDb.from_fasta(dbf)
+    pick = sdb.ids[::3]
+    s = api.Searcher(api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
+                                      xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"],
+                                      xdrop_gap_final=p["xdrop_gap_final"],
+                                      min_raw_gapped_score=p["min_raw_gapped_score"],
+                                      complexity_adjust=bool(p.get("complexity_adjust")), mask_level=p["mask_level"]),
+                     api.ScoreMatrix.from_text(synth.MATRIX_TEXT, synth.MATRIX_NAME), sdb.select(pick))
+    qr = api.read_fasta(qf)
+    got = s.search([api.encode(x) for _, x in qr], [n for n, _ in qr]).tabular(FIELDS)
+    for name, text in (("db.fa", dbf), ("q.fa", qf), (synth.MATRIX_NAME, synth.MATRIX_TEXT),
+                       ("gi.txt", "\n".join(pick) + "\n")):
+        (tmp_path / name).write_text(text)
+    want = O.run_cli(["--db", str(tmp_path / "db.fa"), "--query", str(tmp_path / "q.fa"),
+                      "--matrix", str(tmp_path / synth.MATRIX_NAME), "--gilist", str(tmp_path / "gi.txt"),
+                      "--gapopen", str(p["gap_open"]), "--gapextend", str(p["gap_extend"]),
+                      "--word-size", str(p["word_size"]), "--xdrop-ungap", str(p["xdrop_ungap"]),
+                      "--xdrop-gap", str(p["xdrop_gap"]), "--xdrop-gap-final", str(p["xdrop_gap_final"]),
+                      "--min-raw-gapped-score", str(p["min_raw_gapped_score"]), "--dust", "no",
+                      "--mask-level", str(p["mask_level"]), "--complexity-adjust", "--outfmt", FIELDS])
+    assert got.count("\n") > 2
+    assert got == want

@@ -85,3 +85,22 @@ def test_oracle_chunked_path_matches_chr22_golden(tmp_path):
     want = (REF / "rmblastn/tests/data/expected_chr22_30M-33M_ws7.ncbi-2.17.1.tsv").read_text()
     assert got.count("\n") == 4236
     assert got == want
+
+
+@pytest.mark.parametrize("name,extra", [
+    ("defaults", []),
+    ("rm", ["--word-size", "14", "--mask-level", "80", "--complexity-adjust", "--min-raw-gapped-score", "200",
+            "--xdrop-ungap", "400", "--xdrop-gap-final", "200", "--xdrop-gap", "100"]),
+])
+def test_oracle_pairwise_matches_ncbi(name, extra):
+    """Pairwise output (outfmt 0, the default) against NCBI 2.17.1: rmblastn/tests/cli.rs:197-212,
+    run from the fixtures' folder so the database prints under its own name; the "Posted date"
+    line (the file's time) is left out, as the reference's test does."""
+    import subprocess
+    O.build_oracle()
+    r = subprocess.run([str(O.ORACLE_CLI), "--db", "db.fa", "--query", "query.fa", "--matrix", "comparison.matrix",
+                        "--gapopen", "20", "--gapextend", "5", "--num-threads", "2", *extra],
+                       cwd=G, check=True, capture_output=True, text=True)
+    want = "".join(ln for ln in (G / f"expected_pairwise_{name}.ncbi-2.17.1.txt").read_text().splitlines(True)
+                   if not ln.startswith("    Posted date:"))
+    assert r.stdout == want
