@@ -24,6 +24,7 @@
 #include "rmb_device.cuh"
 #include "rmb_dust.cuh"
 #include "rmb_kernels.hpp"
+#include "rmb_prelim_stream.cuh"
 
 namespace rmb {
 
@@ -860,53 +861,9 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
 }
 
 // ---------------------------------------------------------------------------------------
-// Thread-per-extension score-only X-drop DP over a flat cell stream.
-//
-// Each thread runs the two extensions of one ungapped record after another (left, reversed,
-// then right), one DP cell per loop iteration, and takes the next record from a grid-wide queue
-// when it is done.  Row ends, new rows and new records are short branches inside the one cell
-// loop, so the lanes of a warp stay together whatever the row widths and record lengths are;
-// the warp-cooperative kernel instead spends a whole 32-lane chunk and a row of fixed costs on
-// every row, while the rows here average about 22 cells.
-//
-// The cell step is the reference's (search/gapped.rs:222-296).  Storage differs in three ways,
-// none of which changes a result:
-//  - Band entries that the reference writes in a loop, the initial row (gapped.rs:187-200), the
-//    end-of-row extension cells and the MININT sentinel (gapped.rs:307-334), are not written:
-//    the next row computes them from (vlo, nvirt, ext_val) when it reads them.  Every other
-//    band entry a row reads was written by the row before.
-//  - An entry is 32 bits: cell and vertical gap as 14-bit values relative to the X-drop
-//    threshold T0 at the start of the row that wrote it, clamped below at T0 + FLOOR, and the
-//    column residue.  Live values lie in [T0, T0 + X + max score] (X <= 8000, scores <= 127,
-//    checked by the host); a value below T0 + FLOOR stays below every later threshold even after
-//    adding the best score, so the clamp only moves values that can no longer make a cell
-//    survive (MININT included).  A band index's residue is copied in (with those of up to three
-//    neighbours, one word load) the first time a row reaches it; every index at or past that
-//    frontier is a computed entry, so only its residue bits are live.
-//  - The band window of a row (b_size - first_b cells) must fit the RING-entry ring; a record
-//    whose window grows past it, or whose cell count passes the budget, is listed for the warp
-//    kernel.
+// Thread-per-extension score-only X-drop DP: the body is prelim_stream_thread
+// (rmb_prelim_stream.cuh), shared with a host build of the same code.
 // ---------------------------------------------------------------------------------------
-constexpr int STREAM_RING = 64;
-// A record whose two extensions pass `max_cells` cells is handed to the warp kernel: one thread
-// takes ~0.15 us a cell, so the few extensions thousands of rows long would hold their warp (and
-// the end of the launch) for milliseconds, while a warp does one of their rows in a few hundred
-// cycles.  The launch takes ~10 ns a record, so the host sets the budget to records / 750 (a
-// tail of ~2%), within [STREAM_MIN_CELLS, STREAM_MAX_CELLS].
-constexpr uint32_t STREAM_MIN_CELLS = 8192, STREAM_MAX_CELLS = 65536;
-constexpr int STREAM_BLOCK = 128;
-constexpr int STREAM_BLOCKS_PER_SM = 6;
-constexpr int32_t STREAM_FLOOR = -8192;
-
-// One record's DP geometry (engine.rs:1350-1372), written by k_prelim_prep so that the DP kernel
-// starts a record with one 48-byte load: query and subject sequence starts (record frame),
-// their lengths, the pivot, the traceback seed, X = max(min(xdrop_gap, ungapped score),
-// gap_open + gap_extend), and the strand with the first row residue of each extension.
-struct __align__(16) PrelimGeo {
-    uint64_t qseq, sseq;
-    uint32_t qa, sa, qp, sp;
-    uint32_t tbq, tbs, xdrop, flags;  // flags: plus | a[sp - 1] << 8 | a[sp] << 16
-};
 
 __global__ void __launch_bounds__(256) k_prelim_prep(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                       uint64_t n, const uint32_t* __restrict__ idx,
@@ -928,15 +885,19 @@ __global__ void __launch_bounds__(256) k_prelim_prep(DevLib L, DevQueries Q, con
     }
 }
 
-// Band entry: bits 0-13 cell, 14-27 vertical gap (14-bit two's complement, relative to the
-// row threshold), 28-31 the column residue b[j].  stream_pack keeps w's residue bits.
-__device__ __forceinline__ uint32_t stream_pack(int32_t ex, int32_t ey, uint32_t w) {
-    uint32_t r;
-    asm("bfi.b32 %0, %1, %2, 14, 14;" : "=r"(r) : "r"((uint32_t)ey), "r"(w));
-    asm("bfi.b32 %0, %1, %0, 0, 14;" : "+r"(r) : "r"((uint32_t)ex));
-    return r;
-}
+// The ring of a block: band entry j of thread x at ring[(j % STREAM_RING) * STREAM_BLOCK + x], so
+// the threads of a warp touch 32 consecutive words whatever their band indices.
+struct StreamDevEnv {
+    uint32_t* my;
+    unsigned int *queue, *n_wide;
+    uint32_t* wide;
+    __device__ __forceinline__ uint32_t& at(uint32_t j) { return my[(j % STREAM_RING) * STREAM_BLOCK]; }
+    __device__ __forceinline__ uint32_t take() { return atomicAdd(queue, 1u); }
+    __device__ __forceinline__ void overflow(uint32_t t) { wide[atomicAdd(n_wide, 1u)] = t; }
+    __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
+};
 
+template <int U>
 __global__ void __launch_bounds__(STREAM_BLOCK, STREAM_BLOCKS_PER_SM)
 k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __restrict__ geo,
                 PrelimOut* __restrict__ out,
@@ -952,197 +913,9 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
         for (int i = threadIdx.x; i < 256; i += blockDim.x) smat[i] = max(P->matrix[i], -(xmax + 1));
     }
     __syncthreads();
-    uint32_t* const my = ring + threadIdx.x;  // band entry j at my[(j % RING) * BLOCK]
-    const int32_t ge = P->gap_extend, goe = P->gap_open + ge;
-    // floor(num / ge) = (num * ge_magic) >> 32 for 0 <= num <= 8000 (ge <= 8000)
-    const uint64_t ge_magic = (0x100000000ull + (uint64_t)ge - 1) / (uint64_t)ge;
-    const int32_t cutoff = P->gapped_cutoff;
-
-    // record
-    uint64_t t = 0;
-    uint32_t qa = 0, sa = 0, qp = 0, sp = 0, tbq = 0, tbs = 0, rec_cells = 0;
-    bool plus = true;
-    int32_t xdrop = 0;
-    const uint8_t *qseq = nullptr, *sseq = nullptr;
-    int32_t l_score = 0;
-    uint32_t l_a = 0, l_b = 0;
-    int phase = 0;  // 0: need a record, 1: left extension, 2: right extension, 3: no right extension
-    // extension: row residue a[ai] at abase[dir * ai]; column residue b[bi] at qal[pb + dir * bi]
-    const uint8_t *abase = nullptr, *qal = nullptr;
-    int32_t dir = 1, pb = 0, r0 = 0;
-    uint32_t filled = 0;  // residues of band indices [.., filled) are in the ring
-    uint8_t a_nx = 0, a0_left = 0, a0_right = 0;
-    uint32_t m = 0, nb = 0, ai = 0, bi = 0, first_b = 0, b_size = 0, last_b = 0, best_a = 0, best_b = 0, vlo = 0,
-             nvirt = 0, srow = 0;
-    int32_t best = 0, prev_best = 0, thr = 0, sc = 0, gap_row = 0, ext_val = 0, base_prev = 0, base_cur = 0,
-            floor_cur = 0;
-    unsigned long long cells = 0;
-    // records come from one queue for the grid; the next index is fetched one record ahead
-    unsigned int next_t = atomicAdd(queue, 1u);
-    bool fetch = true;  // no extension running: finish the last one and start the next
-    bool dp_fail = false;
-
-    auto new_row = [&]() {
-        srow = (uint32_t)(a_nx & 15) * 16u;
-        if (ai + 1 < m) a_nx = abase[(ptrdiff_t)dir * (ptrdiff_t)(ai + 1)];  // next row's residue
-        sc = MININT; gap_row = MININT;
-        last_b = first_b; prev_best = best; bi = first_b;
-        base_prev = base_cur; base_cur = thr; floor_cur = thr + STREAM_FLOOR;
-        rec_cells += b_size - first_b;
-    };
-    // copy the residues of band indices filled.. (up to 4, one aligned word of the column
-    // sequence; only indices below `limit`: the ring holds RING of them) into the ring
-    auto fill_word = [&](uint32_t limit) {
-        const int32_t addr = pb + dir * (int32_t)filled;
-        const uint32_t wv = *(const uint32_t*)(qal + (ptrdiff_t)(addr & ~3));
-        const uint32_t cnt = dir > 0 ? 4u - (uint32_t)(addr & 3) : (uint32_t)(addr & 3) + 1u;
-#pragma unroll
-        for (uint32_t q = 0; q < 4; ++q) {
-            const uint32_t i = filled + q;
-            if (q < cnt && i < limit) {
-                const int32_t aq = addr + dir * (int32_t)q;
-                my[(i % STREAM_RING) * STREAM_BLOCK] = ((wv >> ((aq & 3) * 8)) & 15u) << 28;
-            }
-        }
-        filled += min(cnt, limit - filled);
-    };
-
-    // The loop ends for the whole warp at once (lanes out of records idle until then): the
-    // warp-wide vote at the top of every iteration brings the lanes back together after a row
-    // end or a record change, so the cell steps run with every busy lane.
-    bool out_of_records = false;
-    for (;;) {
-        if (!__any_sync(0xffffffffu, !out_of_records)) break;
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            if (fetch || out_of_records) continue;
-            // one cell (gapped.rs:234-262)
-            const uint32_t slot = (bi % STREAM_RING) * STREAM_BLOCK;
-            uint32_t w = my[slot];
-            if (bi >= filled) {  // first visit of this band index: bring in its residue
-                fill_word(min(nb + 1, first_b + (uint32_t)STREAM_RING));
-                w = my[slot];
-            }
-            int32_t cx = ((int32_t)(w << 18) >> 18) + base_prev, cy = ((int32_t)(w << 4) >> 18) + base_prev;
-            if (bi >= vlo) {  // extension cell or sentinel of the previous row end
-                const bool e = bi - vlo < nvirt;
-                const int32_t v = ext_val - (int32_t)(bi - vlo) * ge;
-                cx = e ? v : MININT;
-                cy = e ? v - goe : MININT;
-            }
-            const uint32_t code = w >> 28;
-            const int32_t nxt = bi < nb ? cx + smat[srow + code] : 0;
-            const int32_t cell = max(max(sc, cy), gap_row);
-            const bool alive = cell >= thr;
-            if (!alive && bi == first_b) ++first_b;
-            if (alive) last_b = bi;
-            if (cell > best) { best = cell; best_b = bi; thr = cell - xdrop; }
-            const int32_t open = cell - goe;
-            if (alive) gap_row = max(gap_row - ge, open);
-            const int32_t ex = alive ? cell - base_cur : STREAM_FLOOR;
-            const int32_t ey = max(alive ? max(cy - ge, open) : cy, floor_cur) - base_cur;
-            my[slot] = stream_pack(ex, ey, w);
-            sc = nxt;
-            if (++bi >= b_size) {
-                // end of row (gapped.rs:298-334), as straight-line code
-                if (best > prev_best) best_a = ai + 1;
-                const bool empty = first_b >= b_size;
-                const bool shrink = last_b + 1 < b_size;
-                const int32_t num = gap_row - thr;  // <= xdrop (gap_row never exceeds best)
-                uint32_t k = 0;
-                if (!shrink && b_size <= nb && num >= 0)
-                    k = min((uint32_t)(((uint64_t)(uint32_t)num * ge_magic) >> 32) + 1u, nb + 1 - b_size);
-                const uint32_t nbs = shrink ? last_b + 1 : b_size + k;
-                vlo = shrink ? nbs : b_size;
-                nvirt = nbs - vlo;
-                ext_val = gap_row;
-                b_size = nbs + (nbs <= nb ? 1u : 0u);  // + the MININT sentinel
-                ++ai;
-                const bool over = b_size - first_b > (uint32_t)STREAM_RING ||
-                                  rec_cells + (b_size - first_b) > max_cells;
-                if (empty || ai >= m || over) {
-                    dp_fail = !empty && ai < m;
-                    fetch = true;
-                } else {
-                    new_row();
-                }
-            }
-        }
-        if (fetch && !out_of_records) {
-            // the extension that just ended (best, best_a, best_b; zero for an empty one), then the
-            // next non-empty extension
-            while (fetch) {
-                if (phase != 0 && dp_fail) {
-                    wide[atomicAdd(n_wide, 1u)] = (uint32_t)t;
-                    phase = 0;
-                }
-                if (phase == 1) {
-                    l_score = best; l_a = best_a; l_b = best_b;
-                    const uint32_t rm = sa > sp ? sa - sp : 0, rn = qa > qp ? qa - qp : 0;
-                    if (rm > 0 && rn > 0) {
-                        abase = sseq + sp; pb = r0 + (int32_t)qp; m = rm; nb = rn; dir = 1;
-                        phase = 2;
-                    } else {
-                        best = 0; best_a = 0; best_b = 0;
-                        phase = 3;
-                    }
-                } else if (phase == 2 || phase == 3) {
-                    // both extensions done: engine.rs:1380-1397
-                    PrelimOut o{INT32_MIN, 0, 0, 0, 0, 0, 0};
-                    const int32_t total = l_score + best;
-                    if (total >= 0) {
-                        uint32_t q0 = qp - l_b, s0 = sp - l_a, q1 = qp + best_b, s1 = sp + best_a;
-                        if (!plus) {
-                            const uint32_t t0 = qa - q1, t1 = qa - q0, t2 = sa - s1, t3 = sa - s0;
-                            q0 = t0; q1 = t1; s0 = t2; s1 = t3;
-                        }
-                        if (total >= cutoff) o = PrelimOut{total, q0, q1, s0, s1, tbq, tbs};
-                    }
-                    out[t] = o;
-                    cells += rec_cells;
-                    phase = 0;
-                }
-                if (phase == 0) {
-                    // next record
-                    t = next_t;
-                    if (t >= n) { out_of_records = true; break; }
-                    next_t = atomicAdd(queue, 1u);
-                    const uint4* gp = reinterpret_cast<const uint4*>(geo + t);
-                    const uint4 g0 = gp[0], g1 = gp[1], g2 = gp[2];
-                    qseq = (const uint8_t*)(((uint64_t)g0.y << 32) | g0.x);
-                    sseq = (const uint8_t*)(((uint64_t)g0.w << 32) | g0.z);
-                    qa = g1.x; sa = g1.y; qp = g1.z; sp = g1.w;
-                    tbq = g2.x; tbs = g2.y; xdrop = (int32_t)g2.z;
-                    plus = g2.w & 1u;
-                    a0_left = (uint8_t)(g2.w >> 8);
-                    a0_right = (uint8_t)(g2.w >> 16);
-                    qal = (const uint8_t*)((uintptr_t)qseq & ~(uintptr_t)3);
-                    r0 = (int32_t)(qseq - qal);
-                    rec_cells = 0;
-                    abase = sseq; pb = r0; m = sp; nb = qp; dir = -1;
-                    phase = 1;
-                }
-                if (phase == 3) continue;
-                // start the extension set up above (gapped.rs:165-200)
-                dp_fail = false;
-                best = 0; best_a = 0; best_b = 0;
-                if (m == 0 || nb == 0) continue;  // empty: result 0
-                if (dir < 0) { abase += m - 1; pb += (int32_t)nb - 1; }
-                const uint32_t jmax = (uint32_t)((xdrop - goe) / ge) + 1u;
-                const uint32_t J = jmax < nb ? jmax : nb;
-                if (J + 1 > (uint32_t)STREAM_RING) { dp_fail = true; continue; }
-                // initial row, computed on read: entries 1..J
-                b_size = J + 1; vlo = 1; nvirt = J; ext_val = -goe;
-                first_b = 0; ai = 0; thr = -xdrop; base_cur = -xdrop;
-                filled = 0;
-                fill_word(min(nb + 1, (uint32_t)STREAM_RING));  // index 0 holds a written cell
-                my[0] = stream_pack(0 - base_cur, -goe - base_cur, my[0]);
-                a_nx = dir < 0 ? a0_left : a0_right;
-                new_row();
-                fetch = false;
-            }
-        }
-    }
+    StreamDevEnv env{ring + threadIdx.x, queue, n_wide, wide};
+    const StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells};
+    const unsigned long long cells = prelim_stream_thread<U>(A, env);
     if (cells) atomicAdd(cells_total, cells);
 }
 
@@ -1806,8 +1579,9 @@ cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo
     const uint64_t budget = n / 750;
     const uint32_t max_cells = (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
                                           : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
-    k_prelim_stream<<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1, cells,
-                                                   max_cells);
+    // groups of 8 cell steps: 4 and 6 lose more to row ends, 12 and 16 to idle lanes (B200 sweep)
+    k_prelim_stream<8><<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1,
+                                                      cells, max_cells);
     return cudaGetLastError();
 }
 
