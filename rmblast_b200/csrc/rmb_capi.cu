@@ -145,7 +145,7 @@ struct rmb_ctx {
     KaBlock ka;                  // E-value statistics (lambda <= 0: none)
     DBuf dust_scratch;           // per-thread DUST interval lists
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
-        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch;
+        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over;
     DevLib L{};
 };
 
@@ -357,22 +357,29 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         ctr.ms_lookup += ms_since(t0);
         auto qhost = [&](uint32_t local) { return QH.host.data() + QH.off[qb + local]; };
 
-        // ---- scan: count, offsets, write (pair ids are local to the sub-batch)
+        // ---- scan: one pass that counts and stages the hits per warp, offsets, then the hits in
+        // pair order (pair ids are local to the sub-batch)
         t0 = std::chrono::steady_clock::now();
         const uint64_t npairs = (uint64_t)nb * ns;
         C.counts.ensure((npairs + 1) * 4);
         C.offs.ensure((npairs + 1) * 8);
+        C.stage_start.ensure(npairs * 4);
+        C.stage.ensure(scan_stage_entries(npairs, C.sms) * sizeof(SeedHit));
+        C.stage_over.ensure(4);
         CK(cudaMemsetAsync(C.counts.p, 0, (npairs + 1) * 4, st));
+        CK(cudaMemsetAsync(C.stage_over.p, 0, 4, st));
         ev.start(st);
-        CK(launch_scan(false, C.L, Q, P.word_size, 0, npairs, C.counts.as<uint32_t>(), nullptr, nullptr, nullptr,
-                       C.sms, st));
+        CK(launch_scan_stage(C.L, Q, P.word_size, npairs, C.counts.as<uint32_t>(), C.stage_start.as<uint32_t>(),
+                             C.stage.as<SeedHit>(), C.stage_over.as<unsigned int>(), C.sms, st));
         size_t tb = 0;
         CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), nullptr, tb, st));
         C.temp.ensure(tb);
         CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), C.temp.p, tb, st));
         ev.stop(st);
         uint64_t nh = 0;
+        unsigned int stage_over = 0;
         CK(cudaMemcpyAsync(&nh, C.offs.as<uint64_t>() + npairs, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&stage_over, C.stage_over.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctr.gpu_ms_scan += ev.ms();
         ctr.word_hits += nh;
@@ -409,8 +416,13 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             C.hits.ensure(nh * sizeof(SeedHit));
             C.hit_pair.ensure(nh * 4);
             ev.start(st);
-            CK(launch_scan(true, C.L, Q, P.word_size, pair0, npairs, nullptr, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
-                           C.hit_pair.as<uint32_t>(), C.sms, st));
+            if (!stage_over)
+                CK(launch_scan_gather(pair0, npairs, C.counts.as<uint32_t>(), C.offs.as<uint64_t>(),
+                                      C.stage_start.as<uint32_t>(), C.stage.as<SeedHit>(), C.hits.as<SeedHit>(),
+                                      C.hit_pair.as<uint32_t>(), C.sms, st));
+            else  // a warp's stretch of the stage ran out: scan this range again, writing in place
+                CK(launch_scan(true, C.L, Q, P.word_size, pair0, npairs, nullptr, C.offs.as<uint64_t>(),
+                               C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.sms, st));
             ev.stop(st);
             CK(cudaStreamSynchronize(st));
             ctr.gpu_ms_scan += ev.ms();

@@ -100,18 +100,33 @@ __device__ __forceinline__ bool exact_extend(const PairView& v, uint32_t q0c, ui
     return true;
 }
 
-template <bool WRITE>
+// One warp per (query, subject) pair: the subject's words at the scan stride against the query's
+// lookup table (lookup.rs scan), each word hit extended exactly to word_size.  Hits leave in scan
+// order (subject position, then lookup-cell order).
+//   SCAN_COUNT: per-pair hit counts only.
+//   SCAN_WRITE: hits at the pair's offset in `hits` (offs from the counts).
+//   SCAN_STAGE: counts, and the hits appended to this warp's stretch of `hits` (stage_cap entries
+//               from warp * stage_cap), the pair's first entry in stage_start; if a stretch runs
+//               out, *stage_over is set and the batch takes the SCAN_WRITE pass instead.
+enum { SCAN_COUNT = 0, SCAN_WRITE = 1, SCAN_STAGE = 2 };
+
+template <int MODE>
 __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
                                                uint32_t* counts, const uint64_t* offs, SeedHit* hits,
-                                               uint32_t* hit_pair) {
+                                               uint32_t* hit_pair, uint32_t* stage_start, uint32_t stage_cap,
+                                               unsigned int* stage_over) {
+    constexpr bool WRITE = MODE != SCAN_COUNT;
     const int lane = threadIdx.x & 31;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t stage0 = MODE == SCAN_STAGE ? (uint32_t)warp * stage_cap : 0u;  // this warp's stretch
+    uint32_t cursor = 0;                                                            // entries of it used
+    bool fits = true;
     for (uint64_t w = warp; w < n_pairs; w += nwarps) {
         const uint64_t pair = pair0 + w;
         const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
         const uint32_t qlen = Q.len[qi], slen = L.len[si];
-        uint64_t out = WRITE ? offs[w] : 0;
+        uint64_t out = MODE == SCAN_WRITE ? offs[w] : MODE == SCAN_STAGE ? (uint64_t)(stage0 + cursor) : 0;
         uint32_t total = 0;
         if (qlen >= (uint32_t)ws && slen >= (uint32_t)ws) {
             PairView v;
@@ -150,13 +165,17 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
                     if (lane >= o) incl += t;
                 }
                 const uint32_t wsum = __shfl_sync(0xffffffffu, incl, 31);
-                if (WRITE && c) {
+                if (MODE == SCAN_STAGE && fits && cursor + total + wsum > stage_cap) {
+                    fits = false;
+                    if (lane == 0) atomicExch(stage_over, 1u);
+                }
+                if (WRITE && fits && c) {
                     uint64_t o = out + total + (incl - c);
                     for (uint32_t j = b; j < e; ++j) {
                         uint32_t qs, so;
                         if (exact_extend(v, __ldg(cq + j), p, qs, so)) {
                             hits[o] = SeedHit{qs, so};
-                            hit_pair[o] = (uint32_t)pair;
+                            if (MODE == SCAN_WRITE) hit_pair[o] = (uint32_t)pair;
                             ++o;
                         }
                     }
@@ -164,7 +183,30 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
                 total += wsum;
             }
         }
-        if (!WRITE && lane == 0) counts[w] = total;
+        if (MODE != SCAN_WRITE && lane == 0) counts[w] = total;
+        if (MODE == SCAN_STAGE) {
+            if (lane == 0) stage_start[w] = stage0 + cursor;
+            cursor += total;
+        }
+    }
+}
+
+// The staged hits of each pair into pair order: hits[offs[w] ..] = stage[stage_start[w] ..], with
+// the pair id; one warp per pair.
+__global__ void __launch_bounds__(256) k_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t* counts,
+                                                      const uint64_t* offs, const uint32_t* stage_start,
+                                                      const SeedHit* __restrict__ stage, SeedHit* __restrict__ hits,
+                                                      uint32_t* __restrict__ hit_pair) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_pairs; w += nwarps) {
+        const uint32_t c = counts[pair0 + w];
+        const uint64_t o = offs[w];
+        const SeedHit* src = stage + stage_start[pair0 + w];
+        for (uint32_t i = lane; i < c; i += 32) {
+            hits[o + i] = src[i];
+            hit_pair[o + i] = (uint32_t)(pair0 + w);
+        }
     }
 }
 
@@ -1505,8 +1547,35 @@ cudaError_t launch_scan(bool write, const DevLib& L, const DevQueries& Q, int32_
                         cudaStream_t st) {
     const int block = 256;
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
-    if (write) k_scan<true><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair);
-    else k_scan<false><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair);
+    if (write)
+        k_scan<SCAN_WRITE><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair, nullptr,
+                                                   0, nullptr);
+    else
+        k_scan<SCAN_COUNT><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair, nullptr,
+                                                   0, nullptr);
+    return cudaGetLastError();
+}
+
+uint64_t scan_stage_entries(uint64_t n_pairs, int sms) {
+    return (uint64_t)grid_for(n_pairs * 32, 256, 8, sms) * (256 / 32) * SCAN_STAGE_PER_WARP;
+}
+
+cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t n_pairs, uint32_t* counts,
+                              uint32_t* stage_start, SeedHit* stage, unsigned int* stage_over, int sms,
+                              cudaStream_t st) {
+    const int block = 256;
+    const int grid = grid_for(n_pairs * 32, block, 8, sms);
+    k_scan<SCAN_STAGE><<<grid, block, 0, st>>>(L, Q, ws, 0, n_pairs, counts, nullptr, stage, nullptr, stage_start,
+                                               SCAN_STAGE_PER_WARP, stage_over);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t* counts, const uint64_t* offs,
+                               const uint32_t* stage_start, const SeedHit* stage, SeedHit* hits, uint32_t* hit_pair,
+                               int sms, cudaStream_t st) {
+    if (!n_pairs) return cudaSuccess;
+    k_scan_gather<<<grid_for(n_pairs * 32, 256, 8, sms), 256, 0, st>>>(pair0, n_pairs, counts, offs, stage_start,
+                                                                       stage, hits, hit_pair);
     return cudaGetLastError();
 }
 
@@ -1576,7 +1645,7 @@ cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo
     const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
     const int grid = (int)(want < cap ? want : cap);
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
-    const uint64_t budget = n / 750;
+    const uint64_t budget = n / 128;
     const uint32_t max_cells = (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
                                           : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
     // groups of 8 cell steps: 4 and 6 lose more to row ends, 12 and 16 to idle lanes (B200 sweep)

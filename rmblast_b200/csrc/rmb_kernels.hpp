@@ -10,6 +10,18 @@ namespace rmb {
 cudaError_t launch_scan(bool write, const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
                         uint32_t* counts, const uint64_t* offs, SeedHit* hits, uint32_t* hit_pair, int sms,
                         cudaStream_t st);
+// Single-pass scan: counts plus the hits staged per warp (scan_stage_entries(n_pairs, sms)
+// SeedHits of stage), then k_scan_gather puts a range of pairs' hits in pair order at their offsets.  A set
+// *stage_over (a warp's stretch of SCAN_STAGE_PER_WARP entries ran out) means the staged hits are
+// incomplete: the caller runs launch_scan(write) instead.
+constexpr uint32_t SCAN_STAGE_PER_WARP = 32768;
+uint64_t scan_stage_entries(uint64_t n_pairs, int sms);
+cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t n_pairs, uint32_t* counts,
+                              uint32_t* stage_start, SeedHit* stage, unsigned int* stage_over, int sms,
+                              cudaStream_t st);
+cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t* counts, const uint64_t* offs,
+                               const uint32_t* stage_start, const SeedHit* stage, SeedHit* hits, uint32_t* hit_pair,
+                               int sms, cudaStream_t st);
 cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut, uint64_t n,
                             const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st);
 uint64_t dedup_threads(int sms);

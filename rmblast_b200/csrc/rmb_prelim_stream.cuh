@@ -41,12 +41,13 @@ constexpr int STREAM_RING = 64;
 // The band window of a row may span at most this many indices: whole-word residue fills run up
 // to 3 indices past its end, which must stay inside the ring.
 constexpr int STREAM_WINDOW = 60;
-// A record whose two extensions pass `max_cells` cells is handed to the warp kernel: one thread
-// takes ~0.1 us a cell, so the few extensions thousands of rows long would hold their warp (and
-// the end of the launch) for milliseconds, while a warp does one of their rows in a few hundred
-// cycles.  The launch takes ~10 ns a record, so the host sets the budget to records / 750 (a
-// tail of ~2%), within [STREAM_MIN_CELLS, STREAM_MAX_CELLS].
-constexpr uint32_t STREAM_MIN_CELLS = 8192, STREAM_MAX_CELLS = 65536;
+// A record whose two extensions pass `max_cells` cells is handed to the warp kernel, so that a few
+// extensions millions of cells long cannot hold their thread (and the end of the launch) for a
+// large part of the launch.  The host sets the budget to records / 128 within
+// [STREAM_MIN_CELLS, STREAM_MAX_CELLS]: on 132 M records of the plain workload the 2^20 budget
+// lengthens the launch by ~40 ms of tail while the warp kernel's share drops from 11 G cells
+// (~130 ms) to 0.06 G.
+constexpr uint32_t STREAM_MIN_CELLS = 65536, STREAM_MAX_CELLS = 1u << 20;
 constexpr int STREAM_BLOCK = 128;
 constexpr int STREAM_BLOCKS_PER_SM = 6;
 constexpr int32_t STREAM_FLOOR = -8192;
