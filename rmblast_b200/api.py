@@ -320,6 +320,7 @@ class Results:
 
     def __init__(self, searcher: "Searcher", ptr, query_ids: list[str]):
         self._s, self._p, self.query_ids = searcher, ptr, query_ids
+        self._lib = lib()  # held for __del__, which can run after the module's globals are gone
         r = ptr.contents
         self.n_hsps = int(r.n_hsps)
         c = r.counters
@@ -367,17 +368,18 @@ class Results:
 
     def __del__(self):
         if getattr(self, "_p", None):
-            lib().rmb_results_free(self._p)
+            self._lib.rmb_results_free(self._p)
             self._p = None
 
 
 class ResidentQueries:
     def __init__(self, h: C.c_void_p, n: int):
         self._h, self.n = h, n
+        self._lib = lib()
 
     def free(self):
         if getattr(self, "_h", None):
-            lib().rmb_queries_free(self._h)
+            self._lib.rmb_queries_free(self._h)
             self._h = None
 
     def __del__(self):
@@ -412,6 +414,7 @@ class Searcher:
                                     fr.ctypes.data_as(C.POINTER(C.c_double)), matrix.lambda_,
                                     matrix.name.encode(), C.byref(ctx), err, 512), err)
         self._ctx = ctx
+        self._lib = lib()
         n = len(db.ids)
         lens = (C.c_uint32 * n)(*[len(p) - 2 for p in db.plus])
         ids = (C.c_char_p * n)(*[i.encode() for i in db.ids])
@@ -457,7 +460,7 @@ class Searcher:
 
     def close(self):
         if getattr(self, "_ctx", None):
-            lib().rmb_ctx_destroy(self._ctx)
+            self._lib.rmb_ctx_destroy(self._ctx)
             self._ctx = None
 
     def __del__(self):

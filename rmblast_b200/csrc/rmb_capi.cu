@@ -60,6 +60,32 @@ struct DBuf {  // growable device buffer
     }
 };
 
+struct HostBuf {  // growable pinned host buffer (contents undefined after a resize)
+    uint8_t* p = nullptr;
+    size_t n = 0, cap = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void resize(size_t m) {
+        if (m > cap) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            cap = 0;
+            CK(cudaMallocHost(&p, m));
+            cap = m;
+        }
+        n = m;
+    }
+    uint8_t* data() { return p; }
+    const uint8_t* data() const { return p; }
+    size_t size() const { return n; }
+    const uint8_t* begin() const { return p; }
+    const uint8_t* end() const { return p + n; }
+};
+
 template <class T>
 void upload(DBuf& b, const std::vector<T>& v, cudaStream_t st) {
     b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
@@ -147,13 +173,14 @@ struct rmb_ctx {
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over;
     DevLib L{};
+    rmb_queries* batch = nullptr;  // the query set of rmb_search_batch, reused from call to call
 };
 
 // Queries resident on the device (rmb_queries_upload); the host copy feeds the host steps.
 struct rmb_queries {
     uint32_t n = 0;
     int device = 0;
-    std::vector<uint8_t> host;     // concatenated sentinel-wrapped queries
+    HostBuf host;                  // concatenated sentinel-wrapped queries (pinned)
     std::vector<uint64_t> off;     // offset of query i in host / d_q / d_qrc
     std::vector<uint32_t> len;
     DBuf d_q, d_qrc, d_off, d_len;
@@ -1020,10 +1047,14 @@ static void check_queries(uint32_t nq, const uint8_t* const* query, const uint32
             throw Fail(RMB_EINVAL, "query is not sentinel-wrapped BLASTNA");
 }
 
-static rmb_queries* make_queries(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen) {
+// The queries on the device (and a pinned host copy), in a new object or, for `into`, in one whose
+// buffers are reused (rmb_search_batch keeps one per context).
+static rmb_queries* make_queries(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen,
+                                 rmb_queries* into = nullptr) {
     check_queries(nq, query, qlen);
-    rmb_queries* H = new rmb_queries();
+    rmb_queries* H = into ? into : new rmb_queries();
     try {
+        H->dusted = false;
         H->n = nq;
         H->device = C->p.device;
         H->len.assign(qlen, qlen + nq);
@@ -1046,8 +1077,10 @@ static rmb_queries* make_queries(rmb_ctx* C, uint32_t nq, const uint8_t* const* 
         CK(cudaStreamSynchronize(st));
         return H;
     } catch (...) {
-        H->release();
-        delete H;
+        if (!into) {
+            H->release();
+            delete H;
+        }
         throw;
     }
 }
@@ -1200,7 +1233,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
     for (uint32_t i : longq) { lptr.push_back(hostq(i)); llen.push_back(QH.len[i]); }
     QueriesPtr QL = subset_queries(C, lptr, llen);
     const uint32_t nl = QL->n;
-    std::vector<uint8_t> lmask = QL->host;
+    std::vector<uint8_t> lmask(QL->host.begin(), QL->host.end());
     if (P.dust) {
         mask_queries(C, *QL, true, ctr);
         CK(cudaMemcpy(lmask.data(), QL->d_qm.p, lmask.size(), cudaMemcpyDeviceToHost));
@@ -1403,12 +1436,20 @@ void rmb_queries_free(rmb_queries* H) {
 
 int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, rmb_results** out,
                      char* err, size_t errlen) {
-    rmb_queries* H = nullptr;
-    int rc = rmb_queries_upload(C, nq, query, qlen, &H, err, errlen);
-    if (rc != RMB_OK) return rc;
-    rc = rmb_search_resident(C, H, out, err, errlen);
-    rmb_queries_free(H);
-    return rc;
+    // the context's own query set: device and pinned host buffers kept from call to call
+    try {
+        if (!C || !out) throw Fail(RMB_EINVAL, "null argument");
+        CK(cudaSetDevice(C->p.device));
+        if (!C->batch) C->batch = new rmb_queries();
+        make_queries(C, nq, query, qlen, C->batch);
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+    return rmb_search_resident(C, C->batch, out, err, errlen);
 }
 
 int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, int32_t stage,
@@ -1569,8 +1610,12 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
                    &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->geo, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
-                   &C->tb_scratch, &C->dust_scratch};
+                   &C->tb_scratch, &C->dust_scratch, &C->stage, &C->stage_start, &C->stage_over};
     for (DBuf* b : all) b->release();
+    if (C->batch) {
+        C->batch->release();
+        delete C->batch;
+    }
     if (C->st) cudaStreamDestroy(C->st);
     delete C;
 }
