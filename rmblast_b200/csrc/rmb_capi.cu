@@ -171,7 +171,7 @@ struct rmb_ctx {
     KaBlock ka;                  // E-value statistics (lambda <= 0: none)
     DBuf dust_scratch;           // per-thread DUST interval lists
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
-        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over;
+        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over, tb_ooff, tb_ops2;
     DevLib L{};
     rmb_queries* batch = nullptr;  // the query set of rmb_search_batch, reused from call to call
 };
@@ -796,12 +796,24 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
                                     per_thread, band_cells, rows_cap, threads, C.cells.as<unsigned long long>(), st));
                 et.stop(st);
                 std::vector<TbOut> to(todo.size());
-                std::vector<uint32_t> ops((uint64_t)todo.size() * ops_cap);
                 CK(cudaMemcpyAsync(to.data(), C.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(ops.data(), C.tb_ops.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 ctr.gpu_ms_traceback += et.ms();
+                // only the ops of the finished items come back, packed
+                std::vector<uint64_t> ooff(todo.size() + 1, 0);
+                for (size_t i = 0; i < todo.size(); ++i)
+                    ooff[i + 1] = ooff[i] + (to[i].status == 2 ? 0 : to[i].n_ops);
+                std::vector<uint32_t> ops(ooff.back());
+                if (!ops.empty()) {
+                    upload(C.tb_ooff, ooff, st);
+                    C.tb_ops2.ensure(ops.size() * 4);
+                    CK(launch_gather_ops((uint32_t)todo.size(), C.tb_ops.as<uint32_t>(), ops_cap, C.tb_out.as<TbOut>(),
+                                         C.tb_ooff.as<uint64_t>(), C.tb_ops2.as<uint32_t>(), C.sms, st));
+                    CK(cudaMemcpyAsync(ops.data(), C.tb_ops2.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    ctr.launches += 1;
+                }
                 std::vector<uint32_t> again;
                 for (size_t i = 0; i < todo.size(); ++i) {
                     const TbOut& o = to[i];
@@ -816,7 +828,7 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
                     r.s1 = o.s1;
                     r.script.clear();
                     for (uint32_t k = 0; k < o.n_ops; ++k) {
-                        const uint32_t v = ops[(uint64_t)i * ops_cap + k];
+                        const uint32_t v = ops[ooff[i] + k];
                         r.script.push_back(RunOp{(uint8_t)(v >> 30), v & 0x3fffffffu});
                     }
                 }
@@ -853,10 +865,17 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
         // ---- host Phase 2b per pair, then per query
         t0 = std::chrono::steady_clock::now();
         std::vector<std::vector<Hit>> pair_hits(np);
+        // the reverse complement of each query with prelims, once
+        std::vector<uint32_t> uq;
+        for (size_t k = 0; k < np; ++k) uq.push_back(pair_ids[k] / ns);
+        std::sort(uq.begin(), uq.end());
+        uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
+        std::vector<std::vector<uint8_t>> qrcs(uq.size());
+        parallel_for(uq.size(), [&](size_t j) { qrcs[j] = revcomp_full(qhost(uq[j]), hqlen[uq[j]] + 2); });
         parallel_for(np, [&](size_t k) {
             const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
             const uint8_t* qs = qhost(qi);
-            std::vector<uint8_t> qrc = revcomp_full(qs, hqlen[qi] + 2);
+            const std::vector<uint8_t>& qrc = qrcs[std::lower_bound(uq.begin(), uq.end(), qi) - uq.begin()];
             SubjectView v;
             v.align = C.h_align.data() + C.plus_off[si];
             v.align_rc = C.h_align_rc.data() + C.plus_off[si];
@@ -1610,7 +1629,8 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
                    &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->geo, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
-                   &C->tb_scratch, &C->dust_scratch, &C->stage, &C->stage_start, &C->stage_over};
+                   &C->tb_scratch, &C->dust_scratch, &C->stage, &C->stage_start, &C->stage_over, &C->tb_ooff,
+                   &C->tb_ops2};
     for (DBuf* b : all) b->release();
     if (C->batch) {
         C->batch->release();

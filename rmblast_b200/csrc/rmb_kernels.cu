@@ -1542,6 +1542,27 @@ static int grid_for(uint64_t work, int block, int per_sm_blocks, int sms) {
     return (int)g;
 }
 
+// The run-length ops of the finished traceback items (status 0/1), packed back to back:
+// dst[off[i] ..] = ops[i * ops_cap ..][0 .. n_ops); one warp per item.
+__global__ void __launch_bounds__(256) k_gather_ops(uint32_t n, const uint32_t* __restrict__ ops, uint32_t ops_cap,
+                                                     const TbOut* __restrict__ out, const uint64_t* __restrict__ off,
+                                                     uint32_t* __restrict__ dst) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+        if (out[i].status == 2) continue;
+        const uint32_t c = out[i].n_ops;
+        for (uint32_t k = lane; k < c; k += 32) dst[off[i] + k] = ops[(uint64_t)i * ops_cap + k];
+    }
+}
+
+cudaError_t launch_gather_ops(uint32_t n, const uint32_t* ops, uint32_t ops_cap, const TbOut* out, const uint64_t* off,
+                              uint32_t* dst, int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    k_gather_ops<<<grid_for((uint64_t)n * 32, 256, 8, sms), 256, 0, st>>>(n, ops, ops_cap, out, off, dst);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_scan(bool write, const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
                         uint32_t* counts, const uint64_t* offs, SeedHit* hits, uint32_t* hit_pair, int sms,
                         cudaStream_t st) {
