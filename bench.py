@@ -35,10 +35,12 @@ sys.path.insert(0, str(ROOT))
 FIELDS = "6 score perc_sub qseqid qstart qend sseqid sstart send"
 OPS_PER_CELL = 11  # int32 add/sub/max/compare per DP cell in search/gapped.rs:234-262
 # DRAM bytes (read + write) per ungapped record of k_prelim_stream, from one ncu capture of
-# `bench.py --scale 0.01` (profiles/k_prelim_stream_plain.md); the traffic is per record (the
+# `bench.py --scale 0.01` (1.31 M records, 80.7 MB); the traffic is per record (the
 # 48-byte geometry read, the 28-byte result write, sequence words), so a launch's traffic is
 # this times its records
-PRELIM_STREAM_DRAM_BYTES_PER_RECORD = 61.6
+PRELIM_STREAM_DRAM_BYTES_PER_RECORD = 61.4
+# copy bandwidth of this pool's B200s measured earlier, used when MEASURED_PEAKS.json is absent
+HBM_FALLBACK_GBS = 6650.0
 
 
 def parse():
@@ -247,10 +249,10 @@ def main():
     traffic = (PRELIM_STREAM_DRAM_BYTES_PER_RECORD * c["prelim_dp"]
                if PRELIM_STREAM_DRAM_BYTES_PER_RECORD and c["gpu_ms_prelim_main"] > 0 else None)
     value = bases * world / (ms_step * 1e-3) / 1e6
-    peaks = {}
+    peaks, peak_source = {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
-        peaks = json.loads(pk.read_text())
+        peaks, peak_source = json.loads(pk.read_text()), "measured"
     line = {
         "metric": "query Mbp/s", "value": value, "unit": "Mbp/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -277,7 +279,7 @@ def main():
                      "peak": peak_int, "unit": "Tops/s", "frac": achieved / peak_int if peak_int else None,
                      "traffic": traffic, "kernel_ms": main_ms, "cells": main_cells,
                      "hbm": {"achieved_gbs": traffic / (main_ms * 1e-3) / 1e9 if traffic else None,
-                             "peak_gbs": peaks.get("hbm_gbs"),
+                             "peak_gbs": peaks.get("hbm_gbs"), "peak_source": peak_source,
                              "frac": (traffic / (main_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]
                                       if traffic and peaks.get("hbm_gbs") else None)},
                      "note": f"{OPS_PER_CELL} int32 ops per DP cell (the reference's cell step) x cells of the "

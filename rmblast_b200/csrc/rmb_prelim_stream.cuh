@@ -43,11 +43,12 @@ constexpr int STREAM_RING = 64;
 constexpr int STREAM_WINDOW = 60;
 // A record whose two extensions pass `max_cells` cells is handed to the warp kernel, so that a few
 // extensions millions of cells long cannot hold their thread (and the end of the launch) for a
-// large part of the launch.  The host sets the budget to records / 128 within
-// [STREAM_MIN_CELLS, STREAM_MAX_CELLS]: on 132 M records of the plain workload the 2^20 budget
-// lengthens the launch by ~40 ms of tail while the warp kernel's share drops from 11 G cells
-// (~130 ms) to 0.06 G.
-constexpr uint32_t STREAM_MIN_CELLS = 65536, STREAM_MAX_CELLS = 1u << 20;
+// large part of the launch.  A thread does ~3 M cells/s, so the budget sets the worst tail; the
+// host makes it records / 128 within [STREAM_MIN_CELLS, STREAM_MAX_CELLS].  On the 132 M records
+// of the plain workload the 2^20 budget adds ~13 ms of tail to an ~830 ms launch while the warp
+// kernel's share drops from 11 G cells (~130 ms) to 0.06 G; a launch of 1.3 M records keeps a
+// ~3 ms tail with its 10 k budget (a 65 k budget there made a 20 ms launch of a 9 ms one).
+constexpr uint32_t STREAM_MIN_CELLS = 8192, STREAM_MAX_CELLS = 1u << 20;
 constexpr int STREAM_BLOCK = 128;
 constexpr int STREAM_BLOCKS_PER_SM = 6;
 constexpr int32_t STREAM_FLOOR = -8192;
