@@ -937,6 +937,23 @@ struct StreamDevEnv {
     __device__ __forceinline__ uint32_t take() { return atomicAdd(queue, 1u); }
     __device__ __forceinline__ void overflow(uint32_t t) { wide[atomicAdd(n_wide, 1u)] = t; }
     __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
+    // the initial-row residues of every lane that started an extension: lane k copies index k
+    // (and k + 32) into that lane's ring, so the byte loads of one row go out together
+    __device__ __forceinline__ void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n) {
+        unsigned need = __ballot_sync(0xffffffffu, pending);
+        if (!need) return;
+        const int lane = threadIdx.x & 31;
+        while (need) {
+            const int L = __ffs(need) - 1;
+            need &= need - 1;
+            const uint8_t* q = (const uint8_t*)__shfl_sync(0xffffffffu, (unsigned long long)qal, L);
+            const int32_t p = __shfl_sync(0xffffffffu, pb, L), d = __shfl_sync(0xffffffffu, dir, L);
+            const uint32_t c = __shfl_sync(0xffffffffu, n, L);
+            uint32_t* ringL = my - lane + L;
+            for (uint32_t k = lane; k < c; k += 32) ringL[(k % STREAM_RING) * STREAM_BLOCK] = q[p + d * (int32_t)k] & 15u;
+        }
+        __syncwarp();
+    }
 };
 
 template <int U>

@@ -103,8 +103,10 @@ struct StreamDiv {
 
 // The work of one thread until the record queue is empty; returns the DP cells of the records
 // it completed.  Env supplies the thread's ring (`uint32_t& at(j)`: the entry of band index j,
-// slot j % STREAM_RING), the queue (`uint32_t take()`), the overflow list (`overflow(t)`) and a
-// warp-wide vote (`bool any(bool)`).
+// slot j % STREAM_RING), the queue (`uint32_t take()`), the overflow list (`overflow(t)`), a
+// warp-wide vote (`bool any(bool)`) and `fill_rows(pending, qal, pb, dir, n)`: called by every
+// lane of the warp together, it sets entry k (k < n) of each pending lane's ring to the residue
+// qal[pb + dir * k] & 15.
 template <int U, class Env>
 __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(const StreamArgs& A, Env& env) {
     const int32_t ge = A.ge, goe = A.goe;
@@ -138,6 +140,7 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
     bool fetch = true;  // no extension running: finish the last one and start the next
     bool dp_fail = false;
     bool out_of_records = false;
+    bool init_pending = false;  // an extension started whose initial residues are not in yet
 
     auto new_row = [&]() {
         srow = A.smat + (uint32_t)(a_nx & 15) * 16u;
@@ -147,10 +150,9 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
         rec_cells += b_size - first_b;
     };
     // The residues of the band indices of one aligned word of the column sequence, from the
-    // word holding index `filled`'s residue (the other entry bits cleared).  Past the first word
-    // of an extension, `filled` sits on a word boundary, so the word's indices are filled.. +3:
-    // below the window's end + 3 < first_b + RING (the window is at most STREAM_WINDOW).  The
-    // first word may start up to 3 indices before 0: slots of indices not yet live.
+    // word holding index `filled`'s residue (the other entry bits cleared).  `filled` sits on a
+    // word boundary (the initial fill stops on one), so the word's indices are filled .. +3:
+    // below the window's end + 3 < first_b + RING (the window is at most STREAM_WINDOW).
     auto fill_word = [&]() {
         const int32_t addr = pb + dir * (int32_t)filled;
         uint32_t wv = *(const uint32_t*)(qal + (ptrdiff_t)(addr & ~3));
@@ -239,7 +241,9 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                 while (filled < b_size) fill_word();
                 nvirt = k;
                 ext_val = gap_row;
-                if (nbs <= nb) {
+                {
+                    // the sentinel; with nbs = nb + 1 (no sentinel) the store lands past the band,
+                    // on a slot no live index shares (window <= STREAM_WINDOW), and is never read
                     uint32_t& e = env.at(nbs);
                     e = stream_pack(STREAM_FLOOR, STREAM_FLOOR, e);
                 }
@@ -312,13 +316,22 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                 // initial row: cell 0 written, the J gap cells -goe - (i - 1) * ge computed on read
                 b_size = J + 1; vlo = 1; nvirt = J; ext_val = -goe;
                 first_b = 0; ai = 0; thr = -xdrop;
-                filled = 0;
-                while (filled < b_size) fill_word();
-                env.at(0) = stream_pack(0, -goe, env.at(0));
+                // residues of indices 0 .. filled - 1 come in below, with the warp's help: up to
+                // the next word boundary of the column sequence, so later whole-word fills start
+                // on one (at most 3 past b_size <= STREAM_WINDOW: inside the ring)
+                filled = b_size + (uint32_t)(dir > 0 ? -(pb + (int32_t)b_size) & 3 : (pb - (int32_t)b_size + 1) & 3);
+                init_pending = true;
                 a_nx = dir < 0 ? a0_left : a0_right;
                 new_row();
                 fetch = false;
             }
+        }
+        // the initial rows of the extensions started above: all lanes copy residues into the
+        // rings of the lanes that started one, one band index a lane at a time
+        env.fill_rows(init_pending, qal, pb, dir, filled);
+        if (init_pending) {
+            env.at(0) = stream_pack(0, -goe, env.at(0));
+            init_pending = false;
         }
     }
     return cells;
