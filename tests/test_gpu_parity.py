@@ -112,6 +112,29 @@ def test_dust_on_synthetic_matches_oracle(ws):
     assert unmasked.shape != want.shape or not np.array_equal(unmasked, want)
 
 
+def test_scan_long_lookup_cells_match_oracle():
+    """Low-complexity runs in queries and library with DUST off: the runs' words fill lookup cells
+    far past 32 entries, so the scan's write loop takes its path for long cells; seeds and
+    ungapped hits against the oracle."""
+    qs, db, prm = synth.workload("small", scale=0.3)
+    p = dict(prm, **synth.RM_FLAGS)
+    p.update(dust=0, word_size=11)
+    qseqs = with_low_complexity([s for _, s in qs], 5)
+    dseqs = with_low_complexity([s for _, s in db], 6)
+    qf = synth.to_fasta([n for n, _ in qs], qseqs)
+    dbf = synth.to_fasta([n for n, _ in db], dseqs)
+    s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf)
+    enc = [api.encode(x) for _, x in api.read_fasta(qf)]
+    for stage in (0, 1):
+        got = s.stage(enc, stage)
+        want = O.stage_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, stage)
+        assert got.shape == want.shape, (stage, got.shape, want.shape)
+        assert np.array_equal(got, want), stage
+    # some query has a word more than 32 times (a cell past the write loop's 32-entry mask)
+    from collections import Counter
+    assert max(max(Counter(bytes(q[i:i + 8]) for i in range(len(q) - 8)).values()) for q in qseqs) > 32
+
+
 def test_golden_db_dash_subjects_nomask():
     # '-' in subjects is N: CRandom-resolved for the scan, restored for the traceback
     p = dict(O.RM_PARAMS, mask_level=101)
