@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dust", action="store_true", help="mask the queries with DUST (the reference's default)")
+    ap.add_argument("--schedule", choices=["fifo", "learned"], default="fifo",
+                    help="prelim DP record order: FIFO, or the learned cost order (rmblast_b200/sched_mlp.json)")
+    ap.add_argument("--sched-model", default=None, help="schedule network JSON (default: the committed one)")
     return ap.parse_args()
 
 
@@ -183,9 +186,14 @@ def main():
     sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
                           xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
                           min_raw_gapped_score=p["min_raw_gapped_score"], complexity_adjust=bool(p["complexity_adjust"]),
-                          mask_level=p["mask_level"], dust=bool(p.get("dust", 0)), device=local)
+                          mask_level=p["mask_level"], dust=bool(p.get("dust", 0)), device=local,
+                          schedule=1 if args.schedule == "learned" else 0)
     sdb = api.SubjectDb.from_records(db)
     s = api.Searcher(sp, m, sdb)
+    if args.schedule == "learned":
+        from rmblast_b200 import train_sched
+        s.set_schedule_model(train_sched.load_model(Path(args.sched_model) if args.sched_model else
+                                                    train_sched.MODEL_PATH))
     enc = [api.encode(x) for _, x in qs]
     ids = [n for n, _ in qs]
     bases = sum(len(x) for _, x in qs)
@@ -265,7 +273,8 @@ def main():
                             f"min_raw_gapped_score {p['min_raw_gapped_score']} xdrop_ungap {p['xdrop_ungap']} "
                             f"xdrop_gap {p['xdrop_gap']} xdrop_gap_final {p['xdrop_gap_final']}",
                    "l2": "inputs larger than L2 (lookup tables and hit arrays are GBs per step)",
-                   "parallelism": f"{world} independent ranks, queries sharded by rank"},
+                   "parallelism": f"{world} independent ranks, queries sharded by rank",
+                   "schedule": args.schedule},
         "gcups": so_cells / (prelim_ms * 1e-3) / 1e9 if prelim_ms > 0 else None,
         "stage_ms": dict({k: round(c[k], 3) for k in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped",
                                                       "gpu_ms_dedup", "gpu_ms_prelim", "gpu_ms_traceback",

@@ -42,7 +42,7 @@ typedef struct rmb_params {
     int32_t complexity_adjust, dust, mask_level;
     int32_t ungapped_cutoff;
     int32_t device;       /* CUDA device ordinal */
-    int32_t schedule;     /* 0 = FIFO (only value accepted) */
+    int32_t schedule;     /* 0 = FIFO record queue; 1 = learned cost order (rmb_sched_set_model) */
     int32_t kernels;      /* 0 = automatic; 1 = run every preliminary DP on the warp-cooperative
                              kernel (the thread-per-extension kernel's fallback), for testing */
     /* Gapped Karlin-Altschul statistics for E-values and bit scores, as rmb_ka_resolve returns
@@ -55,6 +55,42 @@ typedef struct rmb_params {
 } rmb_params;
 
 typedef struct rmb_ctx rmb_ctx;
+
+/* Learned schedule of the preliminary DP (no counterpart in the reference, whose records run in
+ * a fixed order; the order changes no result).  A 12 -> 64 -> 64 -> 1 ReLU network with BF16
+ * weights predicts each ungapped record's DP cells (log1p), and with params.schedule = 1 the
+ * records leave the DP queue in descending predicted cost, so long extensions start first.
+ * Parameters: RMB_SCHED_NPARAM floats, W1[12][64] (W1[k*64+n]), b1[64], W2[64][64], b2[64],
+ * w3[64], b3, then the features' mean[12] and 1/std[12].  Features of a record: ungapped score /
+ * 100, log1p ungapped extent, log1p of the room left and right of the pivot on query and
+ * subject, X / 100, strand, GC of ~32 subject bases at the pivot, score per base, log1p of the
+ * pair's word hits, log1p of the diagonal room.
+ *
+ * rmb_sched_set_model: the network for this context's searches with schedule 1 (a search with
+ * schedule 1 and no model fails with RMB_ESTATE).
+ * rmb_sched_log: one FIFO search of the queries, returning for every record the thread kernel
+ * completed its raw features (n x 12, malloc'd) and DP cells (n, malloc'd); free both with
+ * rmb_text_free.  Training pairs for rmb_sched_train.
+ * rmb_sched_train: Adam on the GPU (hand-written kernels, FP32 with BF16-rounded weights; the
+ * rate lr falls linearly to lr / 10 over the run) from
+ * params_io (initial weights and the normalisation) over (features, targets = log1p cells);
+ * params_io gets the trained BF16-rounded weights; stats_out[epochs + 1]: each epoch's training
+ * mean squared error, then the held-out RMSE (log-cells) on val_fraction of the rows.
+ * rmb_sched_grad: mean squared error and its gradient (RMB_SCHED_NET floats, in the parameter
+ * layout) on n rows, by the training kernels.
+ * rmb_sched_predict: the inference kernel (BF16 mma, FP32 accumulation) on n rows of raw features. */
+#define RMB_SCHED_NET 5057
+#define RMB_SCHED_NPARAM 5081
+int rmb_sched_set_model(rmb_ctx* ctx, const float* params, uint32_t n_params, char* err, size_t errlen);
+int rmb_sched_log(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
+                  float** features, uint32_t** cells, uint64_t* n_records, char* err, size_t errlen);
+int rmb_sched_train(int32_t device, const float* features, const float* targets, uint64_t n, uint32_t epochs,
+                    uint32_t batch, float lr, uint64_t seed, float val_fraction, float* params_io, float* stats_out,
+                    char* err, size_t errlen);
+int rmb_sched_grad(int32_t device, const float* params, const float* features, const float* targets, uint32_t n,
+                   float* grad_out, float* loss_out, char* err, size_t errlen);
+int rmb_sched_predict(int32_t device, const float* params, const float* features, uint64_t n, float* pred_out,
+                      char* err, size_t errlen);
 
 /* rmblast-lib/src/matrix.rs:62-214 ScoreMatrix: scores[q][s] in BLASTNA order
  * (A C G T R Y M K W S B D H V N GAP), 16x16 row-major; freqs in BLASTNA order; lambda as

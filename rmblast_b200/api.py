@@ -95,6 +95,14 @@ def load_library(path: Path = LIB_PATH) -> C.CDLL:
     lib.rmb_queries_free.argtypes = [C.c_void_p]
     lib.rmb_queries_free.restype = None
     lib.rmb_probe_int32_peak.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_char_p, C.c_size_t]
+    fp = C.POINTER(C.c_float)
+    lib.rmb_sched_set_model.argtypes = [C.c_void_p, fp, C.c_uint32, C.c_char_p, C.c_size_t]
+    lib.rmb_sched_log.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32), C.POINTER(fp),
+                                  C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
+    lib.rmb_sched_train.argtypes = [C.c_int32, fp, fp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64,
+                                    C.c_float, fp, fp, C.c_char_p, C.c_size_t]
+    lib.rmb_sched_grad.argtypes = [C.c_int32, fp, fp, fp, C.c_uint32, fp, fp, C.c_char_p, C.c_size_t]
+    lib.rmb_sched_predict.argtypes = [C.c_int32, fp, fp, C.c_uint64, fp, C.c_char_p, C.c_size_t]
     return lib
 
 
@@ -203,6 +211,8 @@ class SearchParams:
     device: int = 0
     # 0: automatic kernel choice; 1: every preliminary DP on the warp-cooperative kernel
     kernels: int = 0
+    # 0: FIFO record queue; 1: learned cost order (Searcher.set_schedule_model)
+    schedule: int = 0
     # --evalue threshold (0: off) and the -matrix_lambda/-matrix_k/-matrix_alpha/-matrix_beta
     # statistics overrides (zeros: unset)
     evalue: float = 0.0
@@ -214,7 +224,8 @@ class SearchParams:
     def _c(self, ka=(-1.0, -1.0, -1.0, 0.0, 0.0)) -> _Params:
         return _Params(self.gap_open, self.gap_extend, self.word_size, self.xdrop_ungap, self.xdrop_gap,
                        self.xdrop_gap_final, self.min_raw_gapped_score, int(self.complexity_adjust), int(self.dust),
-                       self.mask_level, self.ungapped_cutoff, self.device, 0, self.kernels, *ka, self.evalue)
+                       self.mask_level, self.ungapped_cutoff, self.device, self.schedule, self.kernels, *ka,
+                       self.evalue)
 
 
 class SubjectDb:
@@ -386,6 +397,69 @@ class ResidentQueries:
         self.free()
 
 
+SCHED_NF, SCHED_H, SCHED_NET, SCHED_NPARAM = 12, 64, 5057, 5081
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def sched_init(features: np.ndarray, seed: int = 0, targets: np.ndarray | None = None) -> np.ndarray:
+    """Initial parameters of the schedule network (He-normal weights, zero hidden biases, the
+    output bias at the targets' mean when given) and the normalisation of the given raw features
+    (mean, 1/std), in the rmb_sched layout."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(SCHED_NPARAM, dtype=np.float32)
+    o = 0
+    p[o:o + SCHED_NF * SCHED_H] = rng.normal(0, np.sqrt(2.0 / SCHED_NF), SCHED_NF * SCHED_H)
+    o += SCHED_NF * SCHED_H + SCHED_H
+    p[o:o + SCHED_H * SCHED_H] = rng.normal(0, np.sqrt(2.0 / SCHED_H), SCHED_H * SCHED_H)
+    o += SCHED_H * SCHED_H + SCHED_H
+    p[o:o + SCHED_H] = rng.normal(0, np.sqrt(1.0 / SCHED_H), SCHED_H)
+    if targets is not None and len(targets):
+        p[o + SCHED_H] = float(np.mean(targets))
+    f = np.asarray(features, dtype=np.float64)
+    sd = f.std(axis=0)
+    p[SCHED_NET:SCHED_NET + SCHED_NF] = f.mean(axis=0)
+    p[SCHED_NET + SCHED_NF:] = np.where(sd > 1e-6, 1.0 / np.maximum(sd, 1e-6), 1.0)
+    return p
+
+
+def sched_train(features: np.ndarray, targets: np.ndarray, params: np.ndarray, epochs: int = 4, batch: int = 8192,
+                lr: float = 2e-3, seed: int = 0, val_fraction: float = 0.1, device: int = 0):
+    """rmb_sched_train: returns (trained parameters, per-epoch training MSE, held-out RMSE)."""
+    f = np.ascontiguousarray(features, dtype=np.float32)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    p = np.ascontiguousarray(params, dtype=np.float32).copy()
+    stats = np.zeros(epochs + 1, dtype=np.float32)
+    err = C.create_string_buffer(512)
+    _check(lib().rmb_sched_train(device, _fptr(f), _fptr(t), len(t), epochs, batch, lr, seed, val_fraction, _fptr(p),
+                                 _fptr(stats), err, 512), err)
+    return p, stats[:epochs].copy(), float(stats[epochs])
+
+
+def sched_grad(params: np.ndarray, features: np.ndarray, targets: np.ndarray, device: int = 0):
+    """rmb_sched_grad: (MSE, gradient in the parameter layout) on the given rows."""
+    f = np.ascontiguousarray(features, dtype=np.float32)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    g = np.zeros(SCHED_NET, dtype=np.float32)
+    loss = C.c_float()
+    err = C.create_string_buffer(512)
+    _check(lib().rmb_sched_grad(device, _fptr(p), _fptr(f), _fptr(t), len(t), _fptr(g), C.byref(loss), err, 512), err)
+    return float(loss.value), g
+
+
+def sched_predict(params: np.ndarray, features: np.ndarray, device: int = 0) -> np.ndarray:
+    """rmb_sched_predict: the inference kernel's predicted log1p cells for raw features."""
+    f = np.ascontiguousarray(features, dtype=np.float32)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    y = np.zeros(len(f), dtype=np.float32)
+    err = C.create_string_buffer(512)
+    _check(lib().rmb_sched_predict(device, _fptr(p), _fptr(f), len(f), _fptr(y), err, 512), err)
+    return y
+
+
 def ka_resolve(matrix_name: str, gap_open: int, gap_extend: int, matrix_text: str | None = None,
                cli: tuple[float, float, float, float] | None = None) -> tuple[tuple[float, ...], int]:
     """rmb_ka_resolve: (lambda, K, H, alpha, beta) and the source (0 none, 1 table, 2 command
@@ -430,6 +504,29 @@ class Searcher:
         err = C.create_string_buffer(1024)
         _check(lib().rmb_search_batch(self._ctx, n, qp, ql, C.byref(res), err, 1024), err)
         return Results(self, res, query_ids or [f"query{i}" for i in range(n)])
+
+    def set_schedule_model(self, params: np.ndarray) -> None:
+        """rmb_sched_set_model: the cost network for searches with schedule=1."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        err = C.create_string_buffer(512)
+        _check(lib().rmb_sched_set_model(self._ctx, _fptr(p), p.size, err, 512), err)
+
+    def schedule_log(self, queries: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray]:
+        """rmb_sched_log: (raw features n x 12, DP cells n) of the records of one FIFO search."""
+        n, qp, ql = self._queries(queries)
+        f = C.POINTER(C.c_float)()
+        c = C.POINTER(C.c_uint32)()
+        m = C.c_uint64()
+        err = C.create_string_buffer(1024)
+        _check(lib().rmb_sched_log(self._ctx, n, qp, ql, C.byref(f), C.byref(c), C.byref(m), err, 1024), err)
+        try:
+            k = m.value
+            feats = np.ctypeslib.as_array(f, shape=(max(k, 1) * SCHED_NF,))[:k * SCHED_NF].reshape(k, SCHED_NF).copy()
+            cells = np.ctypeslib.as_array(c, shape=(max(k, 1),))[:k].copy()
+        finally:
+            lib().rmb_text_free(C.cast(f, C.c_void_p))
+            lib().rmb_text_free(C.cast(c, C.c_void_p))
+        return feats, cells
 
     def upload(self, queries: list[np.ndarray]) -> "ResidentQueries":
         """rmb_queries_upload: the queries copied into device memory once."""

@@ -1,6 +1,7 @@
 // rmb_capi.cu -- the C ABI of include/rmb_gpu.h: context, library upload, the batched search
 // pipeline (GPU stages + host order-dependent filters) and result packing.
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -174,6 +175,14 @@ struct rmb_ctx {
         surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over, tb_ooff, tb_ops2;
     DevLib L{};
     rmb_queries* batch = nullptr;  // the query set of rmb_search_batch, reused from call to call
+    // learned schedule: the network's parameters (rmb_sched_set_model) and its per-batch buffers;
+    // sched_log, while rmb_sched_log runs, collects (features, cells) of the FIFO run
+    DBuf sched_params, sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
+    bool sched_ready = false;
+    struct SchedLog {
+        std::vector<float> feats;
+        std::vector<uint32_t> cells;
+    }* sched_log = nullptr;
 };
 
 // Queries resident on the device (rmb_queries_upload); the host copy feeds the host steps.
@@ -246,6 +255,7 @@ void mask_queries(rmb_ctx& C, rmb_queries& QH, bool compat, rmb_counters& ctr) {
 
 // One (query, subject) pair's Phase 2a output, in the reference's order (purge order).
 constexpr uint64_t MAX_RANGE_HITS = 1ull << 29;
+constexpr uint64_t SCHED_NF_HOST = 12;  // features per record of the learned schedule (rmb_sched.cuh)
 
 struct PairPrelims {
     uint32_t q, s;
@@ -581,11 +591,48 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                                       C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p, C.sms,
                                       st));
                 ctr.launches += nu ? 1 : 0;
+                const uint32_t* order = nullptr;
+                uint32_t* cells_out = nullptr;
+                if (C.sched_log && nu) {
+                    // training pairs: each record's features, and its cells from the DP below
+                    C.sched_feat.ensure(nu * SCHED_NF_HOST * 4);
+                    C.sched_cells.ensure(nu * 4);
+                    CK(launch_sched_features(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
+                                             C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
+                                             C.counts.as<uint32_t>(), C.sched_feat.as<float>(), C.sms, st));
+                    cells_out = C.sched_cells.as<uint32_t>();
+                    ctr.launches += 1;
+                } else if (C.p.schedule == 1 && nu) {
+                    // the records in descending predicted cost
+                    C.sched_pred.ensure(nu * 4);
+                    C.sched_order.ensure(nu * 4);
+                    C.sched_scratch.ensure(sched_order_scratch_bytes());
+                    CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
+                                          C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
+                                          C.counts.as<uint32_t>(), C.sched_params.as<float>(),
+                                          C.sched_pred.as<float>(), C.sched_scratch.p, C.sched_order.as<uint32_t>(),
+                                          C.sms, st));
+                    order = C.sched_order.as<uint32_t>();
+                    ctr.launches += 3;
+                }
                 ev_main.start(st);
                 CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
                                         C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
-                                        C.cells.as<unsigned long long>(), C.sms, st));
+                                        C.cells.as<unsigned long long>(), C.sms, st, order, cells_out));
                 ev_main.stop(st);
+                if (cells_out) {
+                    std::vector<float> f(nu * SCHED_NF_HOST);
+                    std::vector<uint32_t> c(nu);
+                    CK(cudaMemcpyAsync(f.data(), C.sched_feat.p, f.size() * 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(c.data(), C.sched_cells.p, c.size() * 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    for (uint64_t r = 0; r < nu; ++r) {
+                        if (c[r] == 0xFFFFFFFFu) continue;  // passed on to the warp kernel
+                        C.sched_log->feats.insert(C.sched_log->feats.end(), f.begin() + r * SCHED_NF_HOST,
+                                                  f.begin() + (r + 1) * SCHED_NF_HOST);
+                        C.sched_log->cells.push_back(c[r]);
+                    }
+                }
             }
             else
                 CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
@@ -923,7 +970,8 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         if (p.gap_open < 0 || p.gap_extend < 1) throw Fail(RMB_EINVAL, "gap costs out of range");
         if (p.xdrop_ungap < 0 || p.xdrop_gap < 0 || p.xdrop_gap_final < 0 || p.min_raw_gapped_score < 0)
             throw Fail(RMB_EINVAL, "negative X-drop or cutoff");
-        if (p.schedule != 0) throw Fail(RMB_EINVAL, "only the FIFO schedule (0) is supported");
+        if (p.schedule != 0 && p.schedule != 1)
+            throw Fail(RMB_EINVAL, "schedule must be 0 (FIFO) or 1 (learned cost order)");
         if (p.kernels != 0 && p.kernels != 1) throw Fail(RMB_EINVAL, "kernels must be 0 (automatic) or 1 (warp prelim)");
         C = new rmb_ctx();
         C->p = p;
@@ -1431,6 +1479,8 @@ int rmb_search_resident(rmb_ctx* C, rmb_queries* H, rmb_results** out, char* err
         if (!C || !H || !out) throw Fail(RMB_EINVAL, "null argument");
         if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before the search");
         if (H->device != C->p.device) throw Fail(RMB_EINVAL, "queries were uploaded to another device");
+        if (C->p.schedule == 1 && !C->sched_ready)
+            throw Fail(RMB_ESTATE, "schedule 1 needs the network: call rmb_sched_set_model first");
         CK(cudaSetDevice(C->p.device));
         std::vector<std::vector<Hit>> hits;
         rmb_counters ctr{};
@@ -1469,6 +1519,67 @@ int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const
         return fail_out(e, err, errlen, RMB_EINVAL);
     }
     return rmb_search_resident(C, C->batch, out, err, errlen);
+}
+
+int rmb_sched_set_model(rmb_ctx* C, const float* params, uint32_t n_params, char* err, size_t errlen) {
+    try {
+        if (!C || !params) throw Fail(RMB_EINVAL, "null argument");
+        if (n_params != RMB_SCHED_NPARAM)
+            throw Fail(RMB_EINVAL, "the schedule network takes " + std::to_string(RMB_SCHED_NPARAM) + " parameters");
+        for (uint32_t i = 0; i < n_params; ++i)
+            if (!std::isfinite(params[i])) throw Fail(RMB_EINVAL, "schedule network parameters must be finite");
+        CK(cudaSetDevice(C->p.device));
+        C->sched_params.ensure(n_params * 4);
+        CK(cudaMemcpy(C->sched_params.p, params, n_params * 4, cudaMemcpyHostToDevice));
+        C->sched_ready = true;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
+}
+
+int rmb_sched_log(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, float** features,
+                  uint32_t** cells, uint64_t* n_records, char* err, size_t errlen) {
+    rmb_ctx::SchedLog log;
+    try {
+        if (!C || !features || !cells || !n_records) throw Fail(RMB_EINVAL, "null argument");
+        if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_sched_log");
+        if (!C->prelim_stream) throw Fail(RMB_EINVAL, "cell logging needs the thread-per-extension prelim kernel");
+        CK(cudaSetDevice(C->p.device));
+        std::unique_ptr<rmb_queries, void (*)(rmb_queries*)> H(make_queries(C, nq, query, qlen), rmb_queries_free);
+        std::vector<std::vector<Hit>> hits;
+        rmb_counters ctr{};
+        C->sched_log = &log;
+        run_search(*C, *H, hits, ctr, nullptr);
+        C->sched_log = nullptr;
+        const uint64_t n = log.cells.size();
+        float* f = (float*)malloc(std::max<uint64_t>(n, 1) * SCHED_NF_HOST * 4);
+        uint32_t* c = (uint32_t*)malloc(std::max<uint64_t>(n, 1) * 4);
+        if (!f || !c) {
+            free(f);
+            free(c);
+            throw std::bad_alloc();
+        }
+        if (n) {
+            memcpy(f, log.feats.data(), n * SCHED_NF_HOST * 4);
+            memcpy(c, log.cells.data(), n * 4);
+        }
+        *features = f;
+        *cells = c;
+        *n_records = n;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        if (C) C->sched_log = nullptr;
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        if (C) C->sched_log = nullptr;
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        if (C) C->sched_log = nullptr;
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
 }
 
 int rmb_debug_stage(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, int32_t stage,
@@ -1630,7 +1741,8 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->geo, &C->n_wide, &C->band,
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
                    &C->tb_scratch, &C->dust_scratch, &C->stage, &C->stage_start, &C->stage_over, &C->tb_ooff,
-                   &C->tb_ops2};
+                   &C->tb_ops2, &C->sched_params, &C->sched_pred, &C->sched_order, &C->sched_scratch,
+                   &C->sched_feat, &C->sched_cells};
     for (DBuf* b : all) b->release();
     if (C->batch) {
         C->batch->release();

@@ -25,6 +25,7 @@
 #include "rmb_dust.cuh"
 #include "rmb_kernels.hpp"
 #include "rmb_prelim_stream.cuh"
+#include "rmb_sched.cuh"
 
 namespace rmb {
 
@@ -903,6 +904,153 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
 }
 
 // ---------------------------------------------------------------------------------------
+// Learned schedule (rmb_sched.cuh): the features of an ungapped record, the network's cost
+// prediction for every record, and the records in descending predicted cost.
+// ---------------------------------------------------------------------------------------
+// The 12 raw features of record i (a hit index): ungapped score / 100, log1p ungapped extent,
+// log1p of the room left and right of the pivot on each sequence, X / 100, strand, GC fraction of
+// ~32 subject bases at the pivot (packed bytes), ungapped score per base, log1p of the pair's word
+// hits, log1p of the diagonal room (min of the two sides' rooms, left plus right).
+__device__ __forceinline__ void sched_features(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t i,
+                                               const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                                               const uint32_t* pair_hits, float f[SCHED_NF]) {
+    const RecGeom g = rec_geom(L, Q, P, i, hits, hit_pair, ub);
+    const UngBox u = ub[i];
+    const uint32_t ext = u.s_end - u.s_start;
+    f[0] = (float)u.score * 0.01f;
+    f[1] = log1pf((float)ext);
+    f[2] = log1pf((float)g.qp);
+    f[3] = log1pf((float)g.sp);
+    f[4] = log1pf((float)(g.qa - g.qp));
+    f[5] = log1pf((float)(g.sa - g.sp));
+    f[6] = (float)g.xd * 0.01f;
+    f[7] = g.plus ? 1.0f : 0.0f;
+    {
+        const uint32_t si = hit_pair[i] % L.n;
+        const uint8_t* pk = L.packed + L.packed_off[si];
+        const uint32_t nbytes = (g.sa + 3) / 4;
+        const uint32_t b1 = min(nbytes, g.sp / 4 + 4), b0 = b1 > 8 ? b1 - 8 : 0;
+        uint32_t gc = 0;
+        for (uint32_t b = b0; b < b1; ++b) {
+            const uint32_t x = pk[b];
+            gc += __popc((x ^ (x >> 1)) & 0x55u);  // 2-bit codes 1 (C) and 2 (G)
+        }
+        f[8] = b1 > b0 ? (float)gc / (float)(4 * (b1 - b0)) : 0.5f;
+    }
+    f[9] = (float)u.score / (float)(ext > 0 ? ext : 1);
+    f[10] = log1pf((float)pair_hits[hit_pair[i]]);
+    f[11] = log1pf((float)(min(g.qp, g.sp) + min(g.qa - g.qp, g.sa - g.sp)));
+}
+
+__global__ void __launch_bounds__(256) k_sched_features(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                         uint64_t n, const uint32_t* __restrict__ idx,
+                                                         const SeedHit* __restrict__ hits,
+                                                         const uint32_t* __restrict__ hit_pair,
+                                                         const UngBox* __restrict__ ub,
+                                                         const uint32_t* __restrict__ pair_hits, float* __restrict__ out) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        float f[SCHED_NF];
+        sched_features(L, Q, P, idx[t], hits, hit_pair, ub, pair_hits, f);
+#pragma unroll
+        for (int k = 0; k < SCHED_NF; ++k) out[t * SCHED_NF + k] = f[k];
+    }
+}
+
+// Predictions for records 0..n): from the records themselves (feats null) or from given raw
+// features (n x 12); the histogram of cost bins is added to hist[SCHED_BINS] when hist is set.
+// Warps take 32 consecutive records at a time, so every lane reaches the warp-wide network.
+constexpr int SCHED_BLOCK = 128;
+__global__ void __launch_bounds__(SCHED_BLOCK) k_sched_predict(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
+                                                                uint64_t n, const uint32_t* __restrict__ idx,
+                                                                const SeedHit* __restrict__ hits,
+                                                                const uint32_t* __restrict__ hit_pair,
+                                                                const UngBox* __restrict__ ub,
+                                                                const uint32_t* __restrict__ pair_hits,
+                                                                const float* __restrict__ feats,
+                                                                const float* __restrict__ params,
+                                                                float* __restrict__ pred, unsigned int* __restrict__ hist) {
+    __shared__ SchedSmem S;
+    __shared__ __align__(16) uint16_t xs[SCHED_BLOCK / 32][32][16];
+    __shared__ float ys[SCHED_BLOCK / 32][32];
+    __shared__ unsigned int h[SCHED_BINS];
+    sched_load(S, params);
+    for (int i = threadIdx.x; i < SCHED_BINS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (SCHED_BLOCK / 32);
+    for (uint64_t base = ((uint64_t)blockIdx.x * (SCHED_BLOCK / 32) + warp) * 32; base < n; base += nwarps * 32) {
+        const uint64_t t = base + lane;
+        float f[SCHED_NF];
+        if (t < n) {
+            if (feats) {
+#pragma unroll
+                for (int k = 0; k < SCHED_NF; ++k) f[k] = feats[t * SCHED_NF + k];
+            } else {
+                sched_features(L, Q, P, idx[t], hits, hit_pair, ub, pair_hits, f);
+            }
+#pragma unroll
+            for (int k = 0; k < SCHED_NF; ++k) f[k] = (f[k] - S.mean[k]) * S.istd[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < SCHED_NF; ++k) f[k] = 0.0f;
+        }
+        const float y = sched_mlp_warp(S, xs[warp], ys[warp], f);
+        if (t < n) {
+            pred[t] = y;
+            if (hist) atomicAdd(&h[sched_bin(y)], 1u);
+        }
+    }
+    if (hist) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < SCHED_BINS; i += blockDim.x)
+            if (h[i]) atomicAdd(&hist[i], h[i]);
+    }
+}
+
+// Start of each cost bin in the order, costliest bin first; fill[] zeroed for the scatter.
+__global__ void k_sched_binstart(const unsigned int* __restrict__ hist, unsigned int* __restrict__ start,
+                                 unsigned int* __restrict__ fill) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned int acc = 0;
+    for (int b = SCHED_BINS - 1; b >= 0; --b) {
+        start[b] = acc;
+        acc += hist[b];
+        fill[b] = 0;
+    }
+}
+
+// order[start[bin] + k] = record: each block ranks a tile of records per bin in shared memory and
+// takes its stretch of every bin with one global atomic (order within a bin is arbitrary).
+constexpr int SCHED_TILE_PER_THREAD = 16;
+__global__ void __launch_bounds__(256) k_sched_scatter(uint64_t n, const float* __restrict__ pred,
+                                                        const unsigned int* __restrict__ start,
+                                                        unsigned int* __restrict__ fill, uint32_t* __restrict__ order) {
+    __shared__ unsigned int cnt[SCHED_BINS], base[SCHED_BINS];
+    const uint64_t tile = (uint64_t)blockDim.x * SCHED_TILE_PER_THREAD;
+    for (uint64_t t0 = (uint64_t)blockIdx.x * tile; t0 < n; t0 += (uint64_t)gridDim.x * tile) {
+        for (int i = threadIdx.x; i < SCHED_BINS; i += blockDim.x) cnt[i] = 0;
+        __syncthreads();
+        uint32_t bin[SCHED_TILE_PER_THREAD], rank[SCHED_TILE_PER_THREAD];
+#pragma unroll
+        for (int j = 0; j < SCHED_TILE_PER_THREAD; ++j) {
+            const uint64_t t = t0 + (uint64_t)j * blockDim.x + threadIdx.x;
+            bin[j] = t < n ? sched_bin(pred[t]) : 0u;
+            rank[j] = t < n ? atomicAdd(&cnt[bin[j]], 1u) : 0u;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < SCHED_BINS; i += blockDim.x)
+            base[i] = cnt[i] ? start[i] + atomicAdd(&fill[i], cnt[i]) : 0u;
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < SCHED_TILE_PER_THREAD; ++j) {
+            const uint64_t t = t0 + (uint64_t)j * blockDim.x + threadIdx.x;
+            if (t < n) order[base[bin[j]] + rank[j]] = (uint32_t)t;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Thread-per-extension score-only X-drop DP: the body is prelim_stream_thread
 // (rmb_prelim_stream.cuh), shared with a host build of the same code.
 // ---------------------------------------------------------------------------------------
@@ -961,7 +1109,8 @@ __global__ void __launch_bounds__(STREAM_BLOCK, STREAM_BLOCKS_PER_SM)
 k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __restrict__ geo,
                 PrelimOut* __restrict__ out,
                 uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide, unsigned int* __restrict__ queue,
-                unsigned long long* __restrict__ cells_total, uint32_t max_cells) {
+                unsigned long long* __restrict__ cells_total, uint32_t max_cells,
+                const uint32_t* __restrict__ order, uint32_t* __restrict__ cells_out) {
     __shared__ uint32_t ring[STREAM_RING * STREAM_BLOCK];
     __shared__ int32_t smat[256];
     {
@@ -973,7 +1122,8 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
     }
     __syncthreads();
     StreamDevEnv env{ring + threadIdx.x, queue, n_wide, wide};
-    const StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells};
+    const StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells,
+                       order, cells_out};
     const unsigned long long cells = prelim_stream_thread<U>(A, env);
     if (cells) atomicAdd(cells_total, cells);
 }
@@ -1677,18 +1827,60 @@ cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevPa
 }
 
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
-                                 unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st) {
+                                 unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
+                                 const uint32_t* order, uint32_t* cells_out) {
     if (!n) return cudaSuccess;
     const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
     const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
     const int grid = (int)(want < cap ? want : cap);
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
     const uint64_t budget = n / 128;
-    const uint32_t max_cells = (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
-                                          : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
+    // with the records in descending predicted cost the long ones start first: the full budget
+    const uint32_t max_cells = order ? STREAM_MAX_CELLS
+                                     : (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
+                                                  : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
     // groups of 8 cell steps: 4 and 6 lose more to row ends, 12 and 16 to idle lanes (B200 sweep)
     k_prelim_stream<8><<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1,
-                                                      cells, max_cells);
+                                                      cells, max_cells, order, cells_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sched_features(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                                  const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                                  const uint32_t* pair_hits, float* out, int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    k_sched_features<<<grid_for(n, 256, 8, sms), 256, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, pair_hits, out);
+    return cudaGetLastError();
+}
+
+size_t sched_order_scratch_bytes() { return 3 * SCHED_BINS * sizeof(unsigned int); }
+
+cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                               const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                               const uint32_t* pair_hits, const float* params, float* pred, void* scratch,
+                               uint32_t* order, int sms, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    unsigned int* hist = (unsigned int*)scratch;
+    cudaError_t e = cudaMemsetAsync(hist, 0, SCHED_BINS * sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    const uint64_t warps = (n + 31) / 32;
+    const int grid = (int)std::min<uint64_t>((warps + SCHED_BLOCK / 32 - 1) / (SCHED_BLOCK / 32), (uint64_t)sms * 8);
+    k_sched_predict<<<grid, SCHED_BLOCK, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, pair_hits, nullptr, params, pred,
+                                                  hist);
+    k_sched_binstart<<<1, 1, 0, st>>>(hist, hist + SCHED_BINS, hist + 2 * SCHED_BINS);
+    const uint64_t tile = 256ull * SCHED_TILE_PER_THREAD;
+    const int g2 = (int)std::min<uint64_t>((n + tile - 1) / tile, (uint64_t)sms * 8);
+    k_sched_scatter<<<g2, 256, 0, st>>>(n, pred, hist + SCHED_BINS, hist + 2 * SCHED_BINS, order);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sched_predict_features(uint64_t n, const float* feats, const float* params, float* pred, int sms,
+                                          cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    const uint64_t warps = (n + 31) / 32;
+    const int grid = (int)std::min<uint64_t>((warps + SCHED_BLOCK / 32 - 1) / (SCHED_BLOCK / 32), (uint64_t)sms * 8);
+    k_sched_predict<<<grid, SCHED_BLOCK, 0, st>>>(DevLib{}, DevQueries{}, nullptr, n, nullptr, nullptr, nullptr, nullptr,
+                                                  nullptr, feats, params, pred, nullptr);
     return cudaGetLastError();
 }
 

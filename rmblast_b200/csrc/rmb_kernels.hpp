@@ -43,7 +43,22 @@ cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevPa
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                void* geo, int sms, cudaStream_t st);
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
-                                 unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st);
+                                 unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
+                                 const uint32_t* order = nullptr, uint32_t* cells_out = nullptr);
+// Learned schedule (rmb_sched.cuh).  Raw features of each record (n x SCHED_NF floats); the
+// network's predicted log1p cells of every record and the records in descending predicted cost
+// (order, for launch_prelim_stream; scratch: sched_order_scratch_bytes()); the network on given
+// raw features.  params: SCHED_NPARAM floats on the device.
+cudaError_t launch_sched_features(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                                  const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                                  const uint32_t* pair_hits, float* out, int sms, cudaStream_t st);
+size_t sched_order_scratch_bytes();
+cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
+                               const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
+                               const uint32_t* pair_hits, const float* params, float* pred, void* scratch,
+                               uint32_t* order, int sms, cudaStream_t st);
+cudaError_t launch_sched_predict_features(uint64_t n, const float* feats, const float* params, float* pred, int sms,
+                                          cudaStream_t st);
 // Records `list` (the thread kernel's overflow), one warp per extension; dres holds 2 x n_list
 // int4.  Records that overflow the warp rings go to `wide` (count in n_wide[0]).
 cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_list,

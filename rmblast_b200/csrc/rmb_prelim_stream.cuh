@@ -85,6 +85,8 @@ struct StreamArgs {
     const PrelimGeo* geo;
     PrelimOut* out;
     uint32_t max_cells;
+    const uint32_t* order = nullptr;  // queue position -> record (a cost order); null: FIFO
+    uint32_t* cells_out = nullptr;    // per-record DP cells (UINT32_MAX: passed on), or null
 };
 
 // floor(num / d) for 0 <= num <= 8000 and 1 <= d <= 8000: num * ceil(2^32 / d) >> 32 (exact for
@@ -256,6 +258,7 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
             while (fetch) {
                 if (phase != 0 && dp_fail) {
                     env.overflow((uint32_t)t);
+                    if (A.cells_out) A.cells_out[t] = 0xFFFFFFFFu;
                     phase = 0;
                 }
                 if (phase == 1) {
@@ -281,13 +284,14 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                         if (total >= A.cutoff) o = PrelimOut{total, q0, q1, s0, s1, tbq, tbs};
                     }
                     A.out[t] = o;
+                    if (A.cells_out) A.cells_out[t] = rec_cells;
                     cells += rec_cells;
                     phase = 0;
                 }
                 if (phase == 0) {
                     // next record
-                    t = next_t;
-                    if (t >= A.n) { out_of_records = true; break; }
+                    if (next_t >= A.n) { out_of_records = true; break; }
+                    t = A.order ? A.order[next_t] : next_t;
                     next_t = env.take();
                     const uint4* gp = reinterpret_cast<const uint4*>(A.geo + t);
                     const uint4 g0 = gp[0], g1 = gp[1], g2 = gp[2];
