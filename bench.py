@@ -35,10 +35,10 @@ sys.path.insert(0, str(ROOT))
 FIELDS = "6 score perc_sub qseqid qstart qend sseqid sstart send"
 OPS_PER_CELL = 11  # int32 add/sub/max/compare per DP cell in search/gapped.rs:234-262
 # DRAM bytes (read + write) per ungapped record of k_prelim_stream, from one ncu capture of
-# `bench.py --scale 0.01` (1.31 M records, 80.7 MB); the traffic is per record (the
+# `bench.py --scale 0.01` (1.31 M records, 80.1 MB); the traffic is per record (the
 # 48-byte geometry read, the 28-byte result write, sequence words), so a launch's traffic is
 # this times its records
-PRELIM_STREAM_DRAM_BYTES_PER_RECORD = 61.4
+PRELIM_STREAM_DRAM_BYTES_PER_RECORD = 61.0
 # copy bandwidth of this pool's B200s measured earlier, used when MEASURED_PEAKS.json is absent
 HBM_FALLBACK_GBS = 6650.0
 
