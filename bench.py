@@ -117,6 +117,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(qs, db, p, budget_s: float):
     """The C++ restatement of the reference CPU path (oracle) on all host cores, over the first
     queries of the same workload until the time budget is spent (at least two queries)."""
@@ -134,7 +144,7 @@ def cpu_baseline(qs, db, p, budget_s: float):
         n += 1
         if secs >= budget_s and n >= 2:
             break
-    return {"value": bases / secs / 1e6, "unit": "Mbp/s", "cores": threads, "kind": "port",
+    return {"value": bases / secs / 1e6, "unit": "Mbp/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
             "sample": f"{n} of {len(qs)} queries ({bases} bp) vs the full library, {secs:.1f} s, C++ restatement "
                       f"of the reference CPU path (mt-mode 0 split by subject, {threads} threads)"}
 
@@ -161,6 +171,20 @@ def reference_arm(args, rank, world):
             "cpu_baseline": dict(cb, value=v), "e2e": {"value": v, "unit": "Mbp/s", "h2d_bytes_per_step": 0,
                                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def scan_roofline(n_queries: int, sdb, c: dict, peaks: dict) -> dict:
+    """The seed scan against HBM: algorithmic bytes = every query reads the whole packed library
+    (a byte per 4 bases) and every word hit writes 8 bytes; the library (~1.2 MB packed) stays
+    in L2, so DRAM carries far less and the stage is bound by its random probes into the query
+    tables, not by bandwidth."""
+    packed = sum((len(p) - 2 + 3) // 4 for p in sdb.plus)
+    algo = n_queries * packed + 8 * c["word_hits"]
+    ms = c["gpu_ms_scan"]
+    gbs = algo / (ms * 1e-3) / 1e9 if ms > 0 else None
+    peak = peaks.get("hbm_gbs")
+    return {"kernel": "k_scan (one staged pass) + k_scan_gather", "bound": "L2 probes", "algorithmic_bytes": algo,
+            "ms": ms, "achieved_gbs": gbs, "hbm_peak_gbs": peak, "frac_of_hbm": gbs / peak if gbs and peak else None}
 
 
 def main():
@@ -276,6 +300,8 @@ def main():
                    "parallelism": f"{world} independent ranks, queries sharded by rank",
                    "schedule": args.schedule},
         "gcups": so_cells / (prelim_ms * 1e-3) / 1e9 if prelim_ms > 0 else None,
+        "traceback_gcups": c["tb_cells"] / (c["gpu_ms_traceback"] * 1e-3) / 1e9 if c["gpu_ms_traceback"] > 0 else None,
+        "scan_roofline": scan_roofline(len(qs), sdb, c, peaks),
         "stage_ms": dict({k: round(c[k], 3) for k in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped",
                                                       "gpu_ms_dedup", "gpu_ms_prelim", "gpu_ms_traceback",
                                                       "ms_host_2a", "ms_host_2b")},

@@ -814,8 +814,14 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
         if (!tin.empty()) {
             uint32_t qmax = 0;
             for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
+            // largest prelim boxes first: warps take items round-robin, so the long alignments
+            // start in the first wave instead of stretching the end of the launch
             std::vector<uint32_t> todo(tin.size());
             for (uint32_t i = 0; i < todo.size(); ++i) todo[i] = i;
+            auto box = [&](uint32_t i) {
+                return (uint64_t)(tin[i].q_end - tin[i].q_start) + (uint64_t)(tin[i].s_end - tin[i].s_start);
+            };
+            std::stable_sort(todo.begin(), todo.end(), [&](uint32_t x, uint32_t y) { return box(x) > box(y); });
             uint64_t trace_cap = 1ull << 20;
             uint32_t ops_cap = 1024;
             int rounds = 0;
