@@ -1699,18 +1699,28 @@ int rmb_format_tabular(const rmb_ctx* C, const rmb_results* R, const char* const
         if (t != "6") throw Fail(RMB_EINVAL, "output format '" + t + "' is not supported; use 6 <fields>");
         while (is >> t) fields.push_back(t);
         if (fields.empty()) throw Fail(RMB_EINVAL, "-outfmt 6 needs a field list");
-        std::string out;
-        Hit h;
-        for (uint32_t qi = 0; qi < R->n_queries; ++qi) {
+        // queries formatted in parallel, each into its own string, then joined in query order
+        for (uint32_t qi = 0; qi < R->n_queries; ++qi)
+            for (uint64_t k = R->query_off[qi]; k < R->query_off[qi + 1]; ++k)
+                if (R->hsps[k].subject_oid >= C->ids.size()) throw Fail(RMB_EINVAL, "HSP subject out of range");
+        std::vector<std::string> parts(R->n_queries);
+        std::atomic<bool> unknown{false};
+        parallel_for(R->n_queries, [&](size_t qi) {
             const std::string qid = query_ids ? query_ids[qi] : ("query" + std::to_string(qi));
-            for (uint64_t k = R->query_off[qi]; k < R->query_off[qi + 1]; ++k) {
-                const rmb_hsp& x = R->hsps[k];
+            std::string& o = parts[qi];
+            Hit h;
+            for (uint64_t k = R->query_off[qi]; k < R->query_off[qi + 1] && !unknown; ++k) {
                 hit_from_record(R, k, h);
-                if (!format_line(out, h, qid, C->ids.at(x.subject_oid), fields))
-                    throw Fail(RMB_EINVAL, "unknown -outfmt field");
-                out.push_back('\n');
+                if (!format_line(o, h, qid, C->ids[R->hsps[k].subject_oid], fields)) unknown = true;
+                o.push_back('\n');
             }
-        }
+        });
+        if (unknown) throw Fail(RMB_EINVAL, "unknown -outfmt field");
+        size_t total = 0;
+        for (const auto& x : parts) total += x.size();
+        std::string out;
+        out.reserve(total);
+        for (const auto& x : parts) out += x;
         char* o = (char*)malloc(out.size() + 1);
         if (!o) throw std::bad_alloc();
         memcpy(o, out.data(), out.size());
