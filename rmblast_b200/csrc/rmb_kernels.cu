@@ -117,7 +117,9 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
                                                uint32_t* hit_pair, uint32_t* stage_start, uint32_t stage_cap,
                                                unsigned int* stage_over) {
     constexpr bool WRITE = MODE != SCAN_COUNT;
-    const int lane = threadIdx.x & 31;
+    // per warp: each lane's first candidate index, lookup-cell start and scan position
+    __shared__ uint32_t s_first[8][32], s_cell[8][32], s_pos[8][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const uint32_t stage0 = MODE == SCAN_STAGE ? (uint32_t)warp * stage_cap : 0u;  // this warp's stretch
@@ -145,43 +147,57 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
             const uint32_t* cs = Q.cell_start + Q.cs_off[qi];
             const uint32_t* cq = Q.cell_q + Q.cq_off[qi];
             for (uint32_t k0 = 0; k0 < npos; k0 += 32) {
+                // lane l looks up position k0 + l; its lookup cell's entries b .. b + cnt are
+                // then spread over the warp, one entry a lane, in (position, entry) order
                 const uint32_t k = k0 + lane;
-                uint32_t c = 0, b = 0, e = 0, p = 0;
+                uint32_t cnt = 0, b = 0, p = 0;
                 if (k < npos) {
                     p = k * step;
                     const uint32_t idx = kmer_at(pk, p, v.lw);
                     if (__ldg(pv + (idx >> 5)) & (1u << (idx & 31))) {
                         b = __ldg(cs + idx);
-                        e = __ldg(cs + idx + 1);
-                        for (uint32_t j = b; j < e; ++j) {
-                            uint32_t qs, so;
-                            if (exact_extend(v, __ldg(cq + j), p, qs, so)) ++c;
-                        }
+                        cnt = __ldg(cs + idx + 1) - b;
                     }
                 }
-                uint32_t incl = c;
+                uint32_t incl = cnt;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
                     if (lane >= o) incl += t;
                 }
-                const uint32_t wsum = __shfl_sync(0xffffffffu, incl, 31);
-                if (MODE == SCAN_STAGE && fits && cursor + total + wsum > stage_cap) {
-                    fits = false;
-                    if (lane == 0) atomicExch(stage_over, 1u);
-                }
-                if (WRITE && fits && c) {
-                    uint64_t o = out + total + (incl - c);
-                    for (uint32_t j = b; j < e; ++j) {
-                        uint32_t qs, so;
-                        if (exact_extend(v, __ldg(cq + j), p, qs, so)) {
-                            hits[o] = SeedHit{qs, so};
-                            if (MODE == SCAN_WRITE) hit_pair[o] = (uint32_t)pair;
-                            ++o;
-                        }
+                const uint32_t n_cand = __shfl_sync(0xffffffffu, incl, 31);
+                s_first[wib][lane] = incl - cnt;
+                s_cell[wib][lane] = b;
+                s_pos[wib][lane] = p;
+                __syncwarp();
+                uint32_t chunk = 0;  // hits of this chunk so far
+                for (uint32_t r0 = 0; r0 < n_cand; r0 += 32) {
+                    const uint32_t t = r0 + lane;
+                    bool ok = false;
+                    uint32_t qs = 0, so = 0;
+                    if (t < n_cand) {
+                        int owner = 0;  // the last lane whose first entry is <= t
+#pragma unroll
+                        for (int st = 16; st; st >>= 1)
+                            if (s_first[wib][owner + st] <= t) owner += st;
+                        ok = exact_extend(v, __ldg(cq + s_cell[wib][owner] + (t - s_first[wib][owner])),
+                                          s_pos[wib][owner], qs, so);
                     }
+                    const unsigned m = __ballot_sync(0xffffffffu, ok);
+                    const uint32_t nm = (uint32_t)__popc(m);
+                    if (MODE == SCAN_STAGE && fits && cursor + total + chunk + nm > stage_cap) {
+                        fits = false;
+                        if (lane == 0) atomicExch(stage_over, 1u);
+                    }
+                    if (WRITE && fits && ok) {
+                        const uint64_t o = out + total + chunk + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                        hits[o] = SeedHit{qs, so};
+                        if (MODE == SCAN_WRITE) hit_pair[o] = (uint32_t)pair;
+                    }
+                    chunk += nm;
                 }
-                total += wsum;
+                __syncwarp();
+                total += chunk;
             }
         }
         if (MODE != SCAN_WRITE && lane == 0) counts[w] = total;
