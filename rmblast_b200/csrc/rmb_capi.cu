@@ -172,7 +172,8 @@ struct rmb_ctx {
     KaBlock ka;                  // E-value statistics (lambda <= 0: none)
     DBuf dust_scratch;           // per-thread DUST interval lists
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
-        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over, tb_ooff, tb_ops2;
+        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over, tb_ooff, tb_ops2,
+        ung_queue;
     DevLib L{};
     rmb_queries* batch = nullptr;  // the query set of rmb_search_batch, reused from call to call
     // learned schedule: the network's parameters (rmb_sched_set_model) and its per-batch buffers;
@@ -470,8 +471,10 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             t0 = std::chrono::steady_clock::now();
             C.ub.ensure(nh * sizeof(UngBox));
             ev.start(st);
+            C.ung_queue.ensure(16);
             CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
-                               C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st));
+                               C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st,
+                               C.ung_queue.as<unsigned long long>()));
             ev.stop(st);
             CK(cudaStreamSynchronize(st));
             ctr.gpu_ms_ungapped += ev.ms();
@@ -1758,7 +1761,7 @@ void rmb_ctx_destroy(rmb_ctx* C) {
                    &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
                    &C->tb_scratch, &C->dust_scratch, &C->stage, &C->stage_start, &C->stage_over, &C->tb_ooff,
                    &C->tb_ops2, &C->sched_params, &C->sched_pred, &C->sched_order, &C->sched_scratch,
-                   &C->sched_feat, &C->sched_cells};
+                   &C->sched_feat, &C->sched_cells, &C->ung_queue};
     for (DBuf* b : all) b->release();
     if (C->batch) {
         C->batch->release();

@@ -285,43 +285,117 @@ __device__ __forceinline__ void extend_ungapped(const uint8_t* query, int64_t q_
 
 // engine.rs:1165-1170 (plus) and 1244-1261 (minus): the extension in NCBI's frame, its box in
 // the record frame, and the value the diagonal hash stores for the seed.
+// One word hit per lane at a time: the two walks of extend_ungapped (left, then right, in the
+// strand's frame) as one resumable walk of UNG_GROUP steps per round; a lane whose hit is done
+// takes the next hit index from the grid-wide queue (one atomic per warp and round), so lanes do
+// not wait for the longest walk of the warp.  Same arithmetic as extend_ungapped + the box of
+// engine.rs:1165-1170 / 1244-1261.
+constexpr int UNG_GROUP = 8;
 __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                    int32_t ucut, uint64_t n, const SeedHit* __restrict__ hits,
-                                                   const uint32_t* __restrict__ hit_pair, UngBox* __restrict__ out) {
+                                                   const uint32_t* __restrict__ hit_pair, UngBox* __restrict__ out,
+                                                   unsigned long long* __restrict__ queue) {
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
     __syncthreads();
-    const int32_t ws = P->word_size, xd = P->xdrop_ungap;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const SeedHit h = hits[i];
-        const uint32_t pair = hit_pair[i];
-        const uint32_t qi = pair / L.n, si = pair % L.n;
-        const uint32_t qlen = Q.len[qi], slen = L.len[si];
-        const uint8_t* sp = L.plus + L.plus_off[si];
-        const uint32_t qo = h.qs & 0x7fffffffu, so = h.s;
-        UngBox u;
-        int32_t sc;
-        uint32_t a, b, c, d;
-        if (!(h.qs >> 31)) {
-            extend_ungapped(Q.q + Q.off[qi], qlen, sp, slen, qo, so, mat, xd, sc, a, b, c, d);
-            u.score = sc;
-            u.q_start = a;
-            u.q_end = b;
-            u.s_start = c;
-            u.s_end = d;
-            u.store = sc >= ucut ? d : so + (uint32_t)ws;
-        } else {
-            const uint32_t qn = qlen - 1 - qo, sn = slen - 1 - so;
-            extend_ungapped(Q.qrc + Q.off[qi], qlen, sp, slen, qn, sn, mat, xd, sc, a, b, c, d);
-            u.score = sc;
-            u.q_start = qlen - b;
-            u.q_end = qlen - a;
-            u.s_start = slen - d;
-            u.s_end = slen - c;
-            const uint32_t key = slen - so - (uint32_t)Q.lw[qi];
-            u.store = sc >= ucut ? d : key + (uint32_t)ws;
+    const int32_t ws = P->word_size, x = -P->xdrop_ungap;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int phase = 0;  // 0 needs a hit, 1 left walk, 2 right walk, 3 queue empty
+    uint64_t i = 0;
+    const uint8_t *qb_ = nullptr, *sb_ = nullptr;
+    int32_t q = 0, s = 0, qlim = 0, slim = 0, dir = -1, sum = 0, score = 0, xc = 0, best = 0, q_beg = 0;
+    int32_t wq = 0, wsx = 0, qlen = 0, slen = 0;
+    SeedHit h{0, 0};
+    uint32_t lw = 0;
+    for (;;) {
+        const unsigned need = __ballot_sync(FULL, phase == 0);
+        if (need) {
+            const int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(need));
+            base = __shfl_sync(FULL, base, leader);
+            if (phase == 0) {
+                i = base + (uint64_t)__popc(need & ((1u << lane) - 1u));
+                if (i >= n) {
+                    phase = 3;
+                } else {
+                    h = hits[i];
+                    const uint32_t pair = hit_pair[i];
+                    const uint32_t qi = pair / L.n, si = pair % L.n;
+                    qlen = (int32_t)Q.len[qi];
+                    slen = (int32_t)L.len[si];
+                    sb_ = L.plus + L.plus_off[si];
+                    lw = (uint32_t)Q.lw[qi];
+                    const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
+                    if (!(h.qs >> 31)) {
+                        qb_ = Q.q + Q.off[qi];
+                        wq = qo;
+                        wsx = so;
+                    } else {
+                        qb_ = Q.qrc + Q.off[qi];
+                        wq = qlen - 1 - qo;
+                        wsx = slen - 1 - so;
+                    }
+                    q = wq - 1; s = wsx - 1; dir = -1; qlim = -1; slim = -1;
+                    sum = 0; score = 0; xc = x; best = wq;
+                    phase = 1;
+                }
+            }
         }
-        out[i] = u;
+        if (!__any_sync(FULL, phase == 1 || phase == 2)) break;
+#pragma unroll
+        for (int g = 0; g < UNG_GROUP; ++g) {
+            if (phase == 1 || phase == 2) {
+                bool stop = q == qlim || s == slim;
+                if (!stop) {
+                    const uint8_t a = qb_[1 + q], c = sb_[1 + s];
+                    if (a == 15 || c == 15) {
+                        stop = true;
+                    } else {
+                        sum += mat[((a & 15) << 4) | (c & 15)];
+                        if (sum > 0) {
+                            best = dir < 0 ? q : q + 1;
+                            score += sum;
+                            if (dir > 0) xc = -score > x ? -score : x;
+                            sum = 0;
+                        } else if (sum < xc) {
+                            stop = true;
+                        }
+                    }
+                }
+                if (!stop) {
+                    q += dir;
+                    s += dir;
+                } else if (phase == 1) {  // the right walk, from the seed
+                    q_beg = best;
+                    q = wq; s = wsx; dir = 1; qlim = qlen; slim = slen;
+                    sum = 0; xc = x; best = wq;
+                    phase = 2;
+                } else {  // the box in the record frame, and the value the diagonal hash stores
+                    const int32_t q_end = best;
+                    const uint32_t ss = (uint32_t)(wsx - (wq - q_beg)), se = (uint32_t)(wsx + (q_end - wq));
+                    UngBox u;
+                    u.score = score;
+                    if (!(h.qs >> 31)) {
+                        u.q_start = (uint32_t)q_beg;
+                        u.q_end = (uint32_t)q_end;
+                        u.s_start = ss;
+                        u.s_end = se;
+                        u.store = score >= ucut ? se : h.s + (uint32_t)ws;
+                    } else {
+                        u.q_start = (uint32_t)(qlen - q_end);
+                        u.q_end = (uint32_t)(qlen - q_beg);
+                        u.s_start = (uint32_t)slen - se;
+                        u.s_end = (uint32_t)slen - ss;
+                        const uint32_t key = (uint32_t)slen - h.s - lw;
+                        u.store = score >= ucut ? se : key + (uint32_t)ws;
+                    }
+                    out[i] = u;
+                    phase = 0;
+                }
+            }
+        }
     }
 }
 
@@ -1784,10 +1858,13 @@ cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t*
 }
 
 cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut, uint64_t n,
-                            const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st) {
+                            const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st,
+                            unsigned long long* queue) {
     if (!n) return cudaSuccess;
     const int block = 256;
-    k_ungapped<<<grid_for(n, block, 8, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out);
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    k_ungapped<<<grid_for(n, block, 8, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out, queue);
     return cudaGetLastError();
 }
 

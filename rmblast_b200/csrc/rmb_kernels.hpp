@@ -22,8 +22,10 @@ cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, 
 cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t* counts, const uint64_t* offs,
                                const uint32_t* stage_start, const SeedHit* stage, SeedHit* hits, uint32_t* hit_pair,
                                int sms, cudaStream_t st);
+// queue: 8 bytes of device scratch (the hit queue counter; zeroed here)
 cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut, uint64_t n,
-                            const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st);
+                            const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st,
+                            unsigned long long* queue);
 uint64_t dedup_threads(int sms);
 size_t diag_cell_bytes();
 cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32_t ucut, uint64_t pair0,
