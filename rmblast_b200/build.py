@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "librmb_b200.so"
 SOURCES = ["rmb_kernels.cu", "rmb_capi.cu", "rmb_glue.cpp", "rmb_io.cpp", "rmb_probe.cu", "rmb_sched.cu"]
-HEADERS = ["rmb_device.cuh", "rmb_dust.cuh", "rmb_prelim_stream.cuh", "rmb_sched.cuh", "rmb_kernels.hpp", "rmb_glue.hpp"]
+HEADERS = ["rmb_device.cuh", "rmb_dust.cuh", "rmb_prelim_stream.cuh", "rmb_sched.cuh", "rmb_ungapped.cuh", "rmb_kernels.hpp", "rmb_glue.hpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -26,6 +26,7 @@
 #include "rmb_kernels.hpp"
 #include "rmb_prelim_stream.cuh"
 #include "rmb_sched.cuh"
+#include "rmb_ungapped.cuh"
 
 namespace rmb {
 
@@ -298,14 +299,12 @@ __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const 
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
     __syncthreads();
-    const int32_t ws = P->word_size, x = -P->xdrop_ungap;
+    const int32_t ws = P->word_size, xdrop = P->xdrop_ungap;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    int phase = 0;  // 0 needs a hit, 1 left walk, 2 right walk, 3 queue empty
+    int phase = 0;  // 0 needs a hit, 1 walking, 3 queue empty
     uint64_t i = 0;
-    const uint8_t *qb_ = nullptr, *sb_ = nullptr;
-    int32_t q = 0, s = 0, qlim = 0, slim = 0, dir = -1, sum = 0, score = 0, xc = 0, best = 0, q_beg = 0;
-    int32_t wq = 0, wsx = 0, qlen = 0, slen = 0;
+    UngWalk walk;
     SeedHit h{0, 0};
     uint32_t lw = 0;
     for (;;) {
@@ -323,77 +322,45 @@ __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const 
                     h = hits[i];
                     const uint32_t pair = hit_pair[i];
                     const uint32_t qi = pair / L.n, si = pair % L.n;
-                    qlen = (int32_t)Q.len[qi];
-                    slen = (int32_t)L.len[si];
-                    sb_ = L.plus + L.plus_off[si];
+                    const int32_t qlen = (int32_t)Q.len[qi], slen = (int32_t)L.len[si];
                     lw = (uint32_t)Q.lw[qi];
                     const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
-                    if (!(h.qs >> 31)) {
-                        qb_ = Q.q + Q.off[qi];
-                        wq = qo;
-                        wsx = so;
-                    } else {
-                        qb_ = Q.qrc + Q.off[qi];
-                        wq = qlen - 1 - qo;
-                        wsx = slen - 1 - so;
-                    }
-                    q = wq - 1; s = wsx - 1; dir = -1; qlim = -1; slim = -1;
-                    sum = 0; score = 0; xc = x; best = wq;
+                    if (!(h.qs >> 31))
+                        walk.start(Q.q + Q.off[qi], L.plus + L.plus_off[si], qlen, slen, qo, so, xdrop);
+                    else
+                        walk.start(Q.qrc + Q.off[qi], L.plus + L.plus_off[si], qlen, slen, qlen - 1 - qo, slen - 1 - so,
+                                   xdrop);
                     phase = 1;
                 }
             }
         }
-        if (!__any_sync(FULL, phase == 1 || phase == 2)) break;
+        if (!__any_sync(FULL, phase == 1)) break;
 #pragma unroll
         for (int g = 0; g < UNG_GROUP; ++g) {
-            if (phase == 1 || phase == 2) {
-                bool stop = q == qlim || s == slim;
-                if (!stop) {
-                    const uint8_t a = qb_[1 + q], c = sb_[1 + s];
-                    if (a == 15 || c == 15) {
-                        stop = true;
-                    } else {
-                        sum += mat[((a & 15) << 4) | (c & 15)];
-                        if (sum > 0) {
-                            best = dir < 0 ? q : q + 1;
-                            score += sum;
-                            if (dir > 0) xc = -score > x ? -score : x;
-                            sum = 0;
-                        } else if (sum < xc) {
-                            stop = true;
-                        }
-                    }
+            if (phase == 1 && walk.step(mat) == 2) {
+                // the box in the record frame, and the value the diagonal hash stores
+                int32_t sc;
+                uint32_t a, b, c, d;
+                walk.result(sc, a, b, c, d);
+                UngBox u;
+                u.score = sc;
+                if (!(h.qs >> 31)) {
+                    u.q_start = a;
+                    u.q_end = b;
+                    u.s_start = c;
+                    u.s_end = d;
+                    u.store = sc >= ucut ? d : h.s + (uint32_t)ws;
+                } else {
+                    const uint32_t qlen = (uint32_t)walk.qlen, slen = (uint32_t)walk.slen;
+                    u.q_start = qlen - b;
+                    u.q_end = qlen - a;
+                    u.s_start = slen - d;
+                    u.s_end = slen - c;
+                    const uint32_t key = slen - h.s - lw;
+                    u.store = sc >= ucut ? d : key + (uint32_t)ws;
                 }
-                if (!stop) {
-                    q += dir;
-                    s += dir;
-                } else if (phase == 1) {  // the right walk, from the seed
-                    q_beg = best;
-                    q = wq; s = wsx; dir = 1; qlim = qlen; slim = slen;
-                    sum = 0; xc = x; best = wq;
-                    phase = 2;
-                } else {  // the box in the record frame, and the value the diagonal hash stores
-                    const int32_t q_end = best;
-                    const uint32_t ss = (uint32_t)(wsx - (wq - q_beg)), se = (uint32_t)(wsx + (q_end - wq));
-                    UngBox u;
-                    u.score = score;
-                    if (!(h.qs >> 31)) {
-                        u.q_start = (uint32_t)q_beg;
-                        u.q_end = (uint32_t)q_end;
-                        u.s_start = ss;
-                        u.s_end = se;
-                        u.store = score >= ucut ? se : h.s + (uint32_t)ws;
-                    } else {
-                        u.q_start = (uint32_t)(qlen - q_end);
-                        u.q_end = (uint32_t)(qlen - q_beg);
-                        u.s_start = (uint32_t)slen - se;
-                        u.s_end = (uint32_t)slen - ss;
-                        const uint32_t key = (uint32_t)slen - h.s - lw;
-                        u.store = score >= ucut ? se : key + (uint32_t)ws;
-                    }
-                    out[i] = u;
-                    phase = 0;
-                }
+                out[i] = u;
+                phase = 0;
             }
         }
     }
