@@ -40,17 +40,18 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale():
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
-    objs = []
-    for s in SOURCES:
+    objs, procs = [], []
+    for s in SOURCES:  # the sources compile concurrently
         o = LIB_DIR / (Path(s).stem + ".o")
         cmd = [nvcc(), *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
                "-I", str(PKG.parent / "include"), "-c", str(CSRC / s), "-o", str(o)]
-        if s.endswith(".cpp"):
-            cmd[1:1] = ["-x", "cu"] if False else []
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(str(o))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     cmd = [nvcc(), *GENCODE, "-shared", "-o", str(LIB), *objs, "-lcudart", "-Xcompiler", "-pthread"]
     if verbose:
         print(" ".join(cmd))

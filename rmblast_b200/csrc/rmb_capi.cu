@@ -81,7 +81,6 @@ struct HostBuf {  // growable pinned host buffer (contents undefined after a res
         n = m;
     }
     uint8_t* data() { return p; }
-    const uint8_t* data() const { return p; }
     size_t size() const { return n; }
     const uint8_t* begin() const { return p; }
     const uint8_t* end() const { return p + n; }
