@@ -99,3 +99,33 @@ def test_crandom_subject_decode_is_deterministic_and_masks():
     assert p[9] in (0, 2) and p[10] in (1, 3)
     db2 = api.SubjectDb.from_records([("s1", b"ACGTNNNNRYACGT")])
     assert np.array_equal(db2.plus[0], p)
+
+
+def test_python_mirror_matches_header_struct_layout(tmp_path):
+    """The ctypes structs of rmblast_b200.api against the C header, compiled by gcc: size and
+    the offset of every field."""
+    import ctypes as C
+    import shutil
+    import subprocess
+    from rmblast_b200 import api
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"rmb_params": api._Params, "rmb_hsp": api._Hsp, "rmb_counters": api._Counters,
+               "rmb_results": api._Results}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rmb_gpu.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'printf("{cname}.{f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                   check=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for f in py._fields_:
+            assert int(got[f"{cname}.{f[0]}"]) == getattr(py, f[0]).offset, (cname, f[0])
