@@ -291,7 +291,9 @@ __device__ __forceinline__ void extend_ungapped(const uint8_t* query, int64_t q_
 // takes the next hit index from the grid-wide queue (one atomic per warp and round), so lanes do
 // not wait for the longest walk of the warp.  Same arithmetic as extend_ungapped + the box of
 // engine.rs:1165-1170 / 1244-1261.
-constexpr int UNG_GROUP = 8;
+// 16 steps a round: the walks at the default size run hundreds of bases, so fewer refills pay
+// for the idle steps after a walk ends (8 measured 49-50 ms, 16 47 ms a step)
+constexpr int UNG_GROUP = 16;
 __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                    int32_t ucut, uint64_t n, const SeedHit* __restrict__ hits,
                                                    const uint32_t* __restrict__ hit_pair, UngBox* __restrict__ out,
