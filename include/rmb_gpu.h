@@ -45,6 +45,11 @@ typedef struct rmb_params {
     int32_t schedule;     /* 0 = FIFO record queue; 1 = learned cost order (rmb_sched_set_model) */
     int32_t kernels;      /* 0 = automatic; 1 = run every preliminary DP on the warp-cooperative
                              kernel (the thread-per-extension kernel's fallback), for testing */
+    int32_t pipeline;     /* 0 = batched: the ungapped extension and the preliminary DP run as
+                             persistent kernels fed by device work queues, the traceback takes
+                             the largest alignments first; 1 = plain: one launch per stage with
+                             one work item per thread (per warp for the traceback) in arrival
+                             order, no queues.  Same results either way; schedule = 1 needs 0. */
     /* Gapped Karlin-Altschul statistics for E-values and bit scores, as rmb_ka_resolve returns
      * them: lambda, K, H, and the alpha/beta of the length adjustment.  ka_lambda <= 0: none
      * (every E-value 1.0 and bit score 0.0, the reference's rendering without statistics). */
@@ -244,12 +249,19 @@ void rmb_ctx_destroy(rmb_ctx* ctx);
  * an allocation could fail or stall.  All pointers are device memory the caller owns:
  * query/query_rc and subject/subject_rc are sentinel-wrapped BLASTNA (the subject with its
  * ambiguity codes restored), prelims n x 8 uint32 in the stage-2 record layout, out n x 9 uint32
- * in the stage-4 layout (status 2 = did not fit the scratch), ops n x ops_cap edit runs.
+ * in the stage-4 layout, ops n x ops_cap edit runs.  Record status (out word 1): 0 aligned,
+ * 1 negative score, 2 did not fit the scratch, 3 the trace walk did not reach the seed (an
+ * internal error), 4 the record's box or seed lies outside the sequences (skipped, no sequence
+ * byte read), 5 the edit script is longer than ops_cap.
  * The scratch is a fixed 32 MiB array in the library that every GPU loading the library holds
  * until the process exits; query + subject must satisfy 8 (subject + 2) + 8 (query + 2) + 64 KiB
- * <= 32 MiB or the call fails with RMB_ELIMIT.  The first call on a device looks the array up
- * (cudaGetSymbolAddress); make that first call before any stream capture.  Calls share the
- * array: two calls whose work overlaps on the GPU race.  The call waits for its stream. */
+ * <= 32 MiB or the call fails with RMB_ELIMIT before any launch.  The array is shared out among
+ * up to 256 threads; records whose trace outgrows a share run again on a quarter of the threads,
+ * down to one thread holding all of it, and only a record that fails there too leaves status 2
+ * (the call then returns RMB_ELIMIT, as it does for status 5).  The first call on a device looks
+ * the array up (cudaGetSymbolAddress); make that first call before any stream capture.  Calls
+ * share the array: two calls whose work overlaps on the GPU race.  The call waits for its
+ * stream, and the caller's current device is the same on return. */
 int rmb_traceback_noalloc(int32_t device, const uint8_t* query, const uint8_t* query_rc, uint32_t qlen,
                           const uint8_t* subject, const uint8_t* subject_rc, uint32_t slen, const uint32_t* prelims,
                           uint32_t n, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap_final,

@@ -32,7 +32,7 @@ class _Params(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "gap_open", "gap_extend", "word_size", "xdrop_ungap", "xdrop_gap", "xdrop_gap_final",
         "min_raw_gapped_score", "complexity_adjust", "dust", "mask_level", "ungapped_cutoff",
-        "device", "schedule", "kernels")] + [(n, C.c_double) for n in (
+        "device", "schedule", "kernels", "pipeline")] + [(n, C.c_double) for n in (
         "ka_lambda", "ka_k", "ka_h", "ka_alpha", "ka_beta", "evalue")]
 
 
@@ -213,6 +213,9 @@ class SearchParams:
     kernels: int = 0
     # 0: FIFO record queue; 1: learned cost order (Searcher.set_schedule_model)
     schedule: int = 0
+    # 0: batched (persistent kernels with device work queues); 1: plain (one launch per stage,
+    # one work item per thread in arrival order)
+    pipeline: int = 0
     # --evalue threshold (0: off) and the -matrix_lambda/-matrix_k/-matrix_alpha/-matrix_beta
     # statistics overrides (zeros: unset)
     evalue: float = 0.0
@@ -224,7 +227,8 @@ class SearchParams:
     def _c(self, ka=(-1.0, -1.0, -1.0, 0.0, 0.0)) -> _Params:
         return _Params(self.gap_open, self.gap_extend, self.word_size, self.xdrop_ungap, self.xdrop_gap,
                        self.xdrop_gap_final, self.min_raw_gapped_score, int(self.complexity_adjust), int(self.dust),
-                       self.mask_level, self.ungapped_cutoff, self.device, self.schedule, self.kernels, *ka,
+                       self.mask_level, self.ungapped_cutoff, self.device, self.schedule, self.kernels,
+                       self.pipeline, *ka,
                        self.evalue)
 
 

@@ -473,7 +473,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             C.ung_queue.ensure(16);
             CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
                                C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st,
-                               C.ung_queue.as<unsigned long long>()));
+                               P.pipeline == 1 ? nullptr : C.ung_queue.as<unsigned long long>()));
             ev.stop(st);
             CK(cudaStreamSynchronize(st));
             ctr.gpu_ms_ungapped += ev.ms();
@@ -620,7 +620,8 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 ev_main.start(st);
                 CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
                                         C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
-                                        C.cells.as<unsigned long long>(), C.sms, st, order, cells_out));
+                                        C.cells.as<unsigned long long>(), C.sms, st, order, cells_out,
+                                        P.pipeline == 1));
                 ev_main.stop(st);
                 if (cells_out) {
                     std::vector<float> f(nu * SCHED_NF_HOST);
@@ -816,14 +817,16 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
         if (!tin.empty()) {
             uint32_t qmax = 0;
             for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
-            // largest prelim boxes first: warps take items round-robin, so the long alignments
-            // start in the first wave instead of stretching the end of the launch
+            // batched: largest prelim boxes first (warps take items round-robin, so the long
+            // alignments start in the first wave instead of stretching the end of the launch);
+            // plain: in arrival order
             std::vector<uint32_t> todo(tin.size());
             for (uint32_t i = 0; i < todo.size(); ++i) todo[i] = i;
             auto box = [&](uint32_t i) {
                 return (uint64_t)(tin[i].q_end - tin[i].q_start) + (uint64_t)(tin[i].s_end - tin[i].s_start);
             };
-            std::stable_sort(todo.begin(), todo.end(), [&](uint32_t x, uint32_t y) { return box(x) > box(y); });
+            if (C.p.pipeline != 1)
+                std::stable_sort(todo.begin(), todo.end(), [&](uint32_t x, uint32_t y) { return box(x) > box(y); });
             uint64_t trace_cap = 1ull << 20;
             uint32_t ops_cap = 1024;
             int rounds = 0;
@@ -981,6 +984,9 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         if (p.schedule != 0 && p.schedule != 1)
             throw Fail(RMB_EINVAL, "schedule must be 0 (FIFO) or 1 (learned cost order)");
         if (p.kernels != 0 && p.kernels != 1) throw Fail(RMB_EINVAL, "kernels must be 0 (automatic) or 1 (warp prelim)");
+        if (p.pipeline != 0 && p.pipeline != 1) throw Fail(RMB_EINVAL, "pipeline must be 0 (batched) or 1 (plain)");
+        if (p.pipeline == 1 && p.schedule == 1)
+            throw Fail(RMB_EINVAL, "the learned order feeds the batched pipeline's record queue (pipeline 0)");
         C = new rmb_ctx();
         C->p = p;
         C->matrix_name = matrix_name ? matrix_name : "";

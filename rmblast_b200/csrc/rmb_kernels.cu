@@ -294,6 +294,9 @@ __device__ __forceinline__ void extend_ungapped(const uint8_t* query, int64_t q_
 // 16 steps a round: the walks at the default size run hundreds of bases, so fewer refills pay
 // for the idle steps after a walk ends (8 measured 49-50 ms, 16 47 ms a step)
 constexpr int UNG_GROUP = 16;
+// QUEUE: a persistent grid whose lanes take hits from a grid-wide queue as their walks end (the
+// batched pipeline); otherwise one hit per thread, thread i taking hit i (the plain pipeline).
+template <bool QUEUE>
 __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                    int32_t ucut, uint64_t n, const SeedHit* __restrict__ hits,
                                                    const uint32_t* __restrict__ hit_pair, UngBox* __restrict__ out,
@@ -309,15 +312,23 @@ __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const 
     UngWalk walk;
     SeedHit h{0, 0};
     uint32_t lw = 0;
+    bool taken = false;
     for (;;) {
         const unsigned need = __ballot_sync(FULL, phase == 0);
         if (need) {
-            const int leader = __ffs(need) - 1;
             unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(need));
-            base = __shfl_sync(FULL, base, leader);
+            if (QUEUE) {
+                const int leader = __ffs(need) - 1;
+                if (lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(need));
+                base = __shfl_sync(FULL, base, leader);
+            }
             if (phase == 0) {
-                i = base + (uint64_t)__popc(need & ((1u << lane) - 1u));
+                if (QUEUE) {
+                    i = base + (uint64_t)__popc(need & ((1u << lane) - 1u));
+                } else {
+                    i = taken ? n : (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                    taken = true;
+                }
                 if (i >= n) {
                     phase = 3;
                 } else {
@@ -1135,13 +1146,22 @@ __global__ void __launch_bounds__(256) k_prelim_prep(DevLib L, DevQueries Q, con
 }
 
 // The ring of a block: band entry j of thread x at ring[(j % STREAM_RING) * STREAM_BLOCK + x], so
-// the threads of a warp touch 32 consecutive words whatever their band indices.
+// the threads of a warp touch 32 consecutive words whatever their band indices.  QUEUE: records
+// come from a grid-wide queue (the batched pipeline's persistent grid); otherwise thread i runs
+// record i alone (the plain pipeline's one record per thread).
+template <bool QUEUE>
 struct StreamDevEnv {
     uint32_t* my;
     unsigned int *queue, *n_wide;
     uint32_t* wide;
+    bool taken = false;
     __device__ __forceinline__ uint32_t& at(uint32_t j) { return my[(j % STREAM_RING) * STREAM_BLOCK]; }
-    __device__ __forceinline__ uint32_t take() { return atomicAdd(queue, 1u); }
+    __device__ __forceinline__ uint32_t take() {
+        if (QUEUE) return atomicAdd(queue, 1u);
+        const uint32_t t = taken ? 0xFFFFFFFFu : blockIdx.x * STREAM_BLOCK + threadIdx.x;
+        taken = true;
+        return t;
+    }
     __device__ __forceinline__ void overflow(uint32_t t) { wide[atomicAdd(n_wide, 1u)] = t; }
     __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
     // the initial-row residues of every lane that started an extension: lane k copies index k
@@ -1163,7 +1183,7 @@ struct StreamDevEnv {
     }
 };
 
-template <int U>
+template <int U, bool QUEUE>
 __global__ void __launch_bounds__(STREAM_BLOCK, STREAM_BLOCKS_PER_SM)
 k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __restrict__ geo,
                 PrelimOut* __restrict__ out,
@@ -1180,7 +1200,7 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
         for (int i = threadIdx.x; i < 256; i += blockDim.x) smat[i] = max(P->matrix[i], -(xmax + 1));
     }
     __syncthreads();
-    StreamDevEnv env{ring + threadIdx.x, queue, n_wide, wide};
+    StreamDevEnv<QUEUE> env{ring + threadIdx.x, queue, n_wide, wide};
     const StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells,
                        order, cells_out};
     const unsigned long long cells = prelim_stream_thread<U>(A, env);
@@ -1831,9 +1851,14 @@ cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParam
                             unsigned long long* queue) {
     if (!n) return cudaSuccess;
     const int block = 256;
+    if (!queue) {  // plain: one hit per thread
+        k_ungapped<false><<<(unsigned)((n + block - 1) / block), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair,
+                                                                                 out, nullptr);
+        return cudaGetLastError();
+    }
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    k_ungapped<<<grid_for(n, block, 8, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out, queue);
+    k_ungapped<true><<<grid_for(n, block, 8, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out, queue);
     return cudaGetLastError();
 }
 
@@ -1890,7 +1915,7 @@ cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevPa
 
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
                                  unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
-                                 const uint32_t* order, uint32_t* cells_out) {
+                                 const uint32_t* order, uint32_t* cells_out, bool plain) {
     if (!n) return cudaSuccess;
     const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
     const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
@@ -1902,8 +1927,13 @@ cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo
                                      : (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
                                                   : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
     // groups of 8 cell steps: 4 and 6 lose more to row ends, 12 and 16 to idle lanes (B200 sweep)
-    k_prelim_stream<8><<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide, n_wide + 1,
-                                                      cells, max_cells, order, cells_out);
+    if (plain)  // one record per thread, the whole grid at once
+        k_prelim_stream<8, false><<<(unsigned)want, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide,
+                                                                            n_wide, n_wide + 1, cells, max_cells,
+                                                                            order, cells_out);
+    else
+        k_prelim_stream<8, true><<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide,
+                                                                n_wide + 1, cells, max_cells, order, cells_out);
     return cudaGetLastError();
 }
 
@@ -2246,9 +2276,9 @@ cudaError_t launch_dust(const uint8_t* q, const uint64_t* off, const uint32_t* l
 //
 // For callers that may not call cudaMalloc: a library embedded in a process whose device memory
 // is owned by another allocator (a caching allocator that must see every byte, a stream-ordered
-// pool, a CUDA graph being captured), or code running where an allocation could fail or stall.
-// The per-thread scratch of the traceback (DP band, row table, trace bytes) comes from this
-// fixed array, which every GPU that loads the library holds until the process exits.
+// pool), or code running where an allocation could fail or stall.  The per-thread scratch of the
+// traceback (DP band, row table, trace bytes) comes from this fixed array, which every GPU that
+// loads the library holds until the process exits.
 // ---------------------------------------------------------------------------------------
 #include <mutex>
 
@@ -2260,7 +2290,9 @@ constexpr uint64_t NOALLOC_SCRATCH_BYTES = 32ull << 20;  // 32 MiB
 constexpr uint32_t NOALLOC_MAX_THREADS = 256;
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
-static __device__ unsigned int g_noalloc_overflow;
+// [0] records that did not fit their share of the scratch (status 2), [1] records whose edit
+// script did not fit ops_cap (status 5)
+static __device__ unsigned int g_noalloc_overflow[2];
 
 struct NoallocSeqs {
     const uint8_t* q;      // query, sentinel-wrapped
@@ -2271,13 +2303,17 @@ struct NoallocSeqs {
 };
 
 // k_traceback for one (query, subject) pair: the same improve_seed + bidirectional traceback +
-// gap pruning, the scratch taken from `scratch` (the address of g_noalloc_scratch).
+// gap pruning, the scratch taken from `scratch` (the address of g_noalloc_scratch).  With
+// `retry` set, only the records whose status is 2 (scratch too small) from an earlier launch
+// with more threads run again, each thread now holding a larger share of the array.
+// Record status: 0 aligned, 1 negative score, 2 scratch too small, 3 the trace walk did not
+// reach the seed, 4 record outside the sequences (skipped), 5 edit script longer than ops_cap.
 __global__ void __launch_bounds__(128) k_traceback_noalloc(NoallocSeqs S, DevParams P, uint32_t n,
                                                             const uint32_t* __restrict__ pre,
                                                             uint32_t* __restrict__ out, uint32_t* __restrict__ ops_out,
                                                             uint32_t ops_cap, uint8_t* __restrict__ scratch,
                                                             uint64_t per_thread, uint64_t band_cells,
-                                                            uint32_t rows_cap, unsigned int* overflow) {
+                                                            uint32_t rows_cap, unsigned int* overflow, bool retry) {
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P.matrix[i];
     __syncthreads();
@@ -2293,14 +2329,26 @@ __global__ void __launch_bounds__(128) k_traceback_noalloc(NoallocSeqs S, DevPar
     for (uint64_t t = tid; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
         // record: strand, q_start, q_end, s_start, s_end, score, q_seed, s_seed
         const uint32_t* r = pre + t * 8;
+        uint32_t* o = out + t * 9;
+        if (retry && o[1] != 2u) continue;
+        // the caller's records are checked before any sequence byte is read: the box inside both
+        // sequences and the seed inside both (improve_seed and the DPs index from them)
+        const bool in_range = r[0] <= 1u && r[1] <= r[2] && r[2] <= qa && r[3] <= r[4] && r[4] <= sa &&
+                              r[6] < qa && r[7] < sa;
+        uint32_t nq = 0, ns = 0;
         const bool plus = r[0] == 0;
-        uint32_t nq, ns;
-        improve_seed(S.q + 1, qa, (plus ? S.s : S.src) + 1, sa, r[6], r[7], r[1], r[2], r[3], r[4], !plus, nq, ns);
+        if (in_range)
+            improve_seed(S.q + 1, qa, (plus ? S.s : S.src) + 1, sa, r[6], r[7], r[1], r[2], r[3], r[4], !plus, nq, ns);
+        if (!in_range || nq >= qa || ns >= sa) {
+            o[0] = r[0];
+            o[1] = 4u;  // outside the sequences: skipped
+            for (int k = 2; k < 9; ++k) o[k] = 0;
+            continue;
+        }
         const uint32_t tq = plus ? nq : qa - 1 - nq, ts = plus ? ns : sa - 1 - ns;
         const uint8_t* qa_ = (plus ? S.q : S.qrc) + 1;
         const uint8_t* sa_ = S.s + 1;
         uint32_t* ops = ops_out + t * (uint64_t)ops_cap;
-        uint32_t* o = out + t * 9;
         uint64_t cells = 0, need = 0;
         int32_t ls, rs = 0;
         uint32_t la, lb, ra = 0, rb = 0, nl = 0, nr = 0;
@@ -2314,9 +2362,13 @@ __global__ void __launch_bounds__(128) k_traceback_noalloc(NoallocSeqs S, DevPar
                                         T, rs, ra, rb, ops + nl, ops_cap - nl, nr, cells, need);
         }
         if (st != 0) {
-            atomicAdd(overflow, 1u);
+            // align_ex_tb: 3 = the walk did not reach the seed; 2 with need > 0 = the trace did not
+            // fit the thread's scratch; 2 with need = 0 = the script did not fit ops_cap
+            const uint32_t code = st == 3 ? 3u : need > 0 ? 2u : 5u;
+            if (code == 2u) atomicAdd(overflow, 1u);
+            if (code == 5u) atomicAdd(overflow + 1, 1u);
             o[0] = r[0];
-            o[1] = 2u;  // did not fit the scratch
+            o[1] = code;
             for (int k = 2; k < 9; ++k) o[k] = 0;
             continue;
         }
@@ -2424,34 +2476,53 @@ extern "C" int rmb_traceback_noalloc(int32_t device, const uint8_t* query, const
     if (min_thread > NOALLOC_SCRATCH_BYTES)
         return fail(RMB_ELIMIT, "query and subject too long for the 32 MiB scratch of rmb_traceback_noalloc "
                                 "(8 bytes x (subject + 2) + 8 bytes x (query + 2) + 64 KiB must fit)");
-    cudaError_t e = cudaSetDevice(device);
+    // the caller's current device is put back on every return
+    int caller_device = -1;
+    cudaError_t e = cudaGetDevice(&caller_device);
     if (e != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+    struct RestoreDevice {
+        int d;
+        ~RestoreDevice() { cudaSetDevice(d); }
+    } restore{caller_device};
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
     uint8_t* scratch = nullptr;
     unsigned int* flag = nullptr;
     if ((e = noalloc_setup(device, &scratch, &flag)) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
-    cudaStream_t st = (cudaStream_t)stream;
-    if ((e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), st)) != cudaSuccess)
-        return fail(RMB_ECUDA, cudaGetErrorString(e));
     if (n == 0) return RMB_OK;
-    uint32_t threads = (uint32_t)(NOALLOC_SCRATCH_BYTES / min_thread);
-    if (threads > NOALLOC_MAX_THREADS) threads = NOALLOC_MAX_THREADS;
-    if (threads > n) threads = n;
-    const uint32_t block = threads >= 128 ? 128 : threads;
-    const uint32_t grid = threads / block;
-    const uint64_t per_thread = (NOALLOC_SCRATCH_BYTES / ((uint64_t)grid * block)) & ~255ull;  // >= min_thread
+    cudaStream_t st = (cudaStream_t)stream;
     DevParams P{};
     P.gap_open = gap_open;
     P.gap_extend = gap_extend;
     P.xdrop_gap_final = xdrop_gap_final;
     for (int i = 0; i < 256; ++i) P.matrix[i] = scores[i];
     NoallocSeqs S{query, query_rc, subject, subject_rc, qlen, slen};
-    k_traceback_noalloc<<<grid, block, 0, st>>>(S, P, n, prelims, out, ops, ops_cap, scratch, per_thread, band_cells,
-                                                 rows_cap, flag);
-    if ((e = cudaGetLastError()) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
-    unsigned int over = 0;
-    if ((e = cudaMemcpyAsync(&over, flag, sizeof over, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-        return fail(RMB_ECUDA, cudaGetErrorString(e));
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
-    if (over) return fail(RMB_ELIMIT, "some alignments did not fit the fixed scratch (status 2 in their records)");
+    uint32_t threads = (uint32_t)(NOALLOC_SCRATCH_BYTES / min_thread);
+    if (threads > NOALLOC_MAX_THREADS) threads = NOALLOC_MAX_THREADS;
+    if (threads > n) threads = n;
+    // Records whose trace did not fit a thread's share run again with a quarter of the threads,
+    // so each gets four times the space, down to one thread holding the whole array.
+    unsigned int over[2] = {0, 0};
+    for (bool retry = false;; retry = true) {
+        const uint32_t block = threads >= 128 ? 128 : threads;
+        const uint32_t grid = threads / block;
+        const uint64_t per_thread = (NOALLOC_SCRATCH_BYTES / ((uint64_t)grid * block)) & ~255ull;  // >= min_thread
+        if ((e = cudaMemsetAsync(flag, 0, 2 * sizeof(unsigned int), st)) != cudaSuccess)
+            return fail(RMB_ECUDA, cudaGetErrorString(e));
+        k_traceback_noalloc<<<grid, block, 0, st>>>(S, P, n, prelims, out, ops, ops_cap, scratch, per_thread,
+                                                     band_cells, rows_cap, flag, retry);
+        if ((e = cudaGetLastError()) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+        unsigned int o[2] = {0, 0};
+        if ((e = cudaMemcpyAsync(o, flag, sizeof o, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return fail(RMB_ECUDA, cudaGetErrorString(e));
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(RMB_ECUDA, cudaGetErrorString(e));
+        over[0] = o[0];
+        over[1] += o[1];
+        if (!over[0] || threads == 1) break;
+        threads = threads >= 4 ? threads / 4 : 1;
+    }
+    if (over[0])
+        return fail(RMB_ELIMIT, "some alignments did not fit the 32 MiB scratch even on one thread (status 2 in "
+                                "their records)");
+    if (over[1]) return fail(RMB_ELIMIT, "some edit scripts were longer than ops_cap (status 5 in their records)");
     return RMB_OK;
 }

@@ -46,7 +46,7 @@ cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevPa
                                void* geo, int sms, cudaStream_t st);
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
                                  unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
-                                 const uint32_t* order = nullptr, uint32_t* cells_out = nullptr);
+                                 const uint32_t* order = nullptr, uint32_t* cells_out = nullptr, bool plain = false);
 // Learned schedule (rmb_sched.cuh).  Raw features of each record (n x SCHED_NF floats); the
 // network's predicted log1p cells of every record and the records in descending predicted cost
 // (order, for launch_prelim_stream; scratch: sched_order_scratch_bytes()); the network on given

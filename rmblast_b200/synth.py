@@ -16,6 +16,8 @@ Workloads (sizes in bases):
              searched against themselves; word 7, masklevel off.
 
 Every generator takes a seed and is deterministic; `scale` shrinks the query side for tests.
+The query chunks of plain and batched each come from their own random stream (seed, chunk
+index), so any batch of chunks can be made on its own and in parallel.
 """
 from __future__ import annotations
 
@@ -73,18 +75,23 @@ def mutate(rng: np.random.Generator, s: np.ndarray, div: float, indel: float) ->
     ev = np.nonzero(rng.random(len(s)) < indel)[0]
     if len(ev) == 0:
         return s
+    # every event's length and kind, and the bases of all insertions, drawn at once
+    lens = rng.geometric(0.5, len(ev))
+    is_ins = rng.random(len(ev)) < 0.5
+    ins_bases = random_dna(rng, int(lens[is_ins].sum()))
     out = []
     prev = 0
-    for p in ev:
+    used = 0
+    for p, ln, ins in zip(ev.tolist(), lens.tolist(), is_ins.tolist()):
         if p < prev:
-            continue
+            continue  # inside an earlier deletion
         out.append(s[prev:p])
-        ln = int(rng.geometric(0.5))
-        if rng.random() < 0.5:
-            out.append(random_dna(rng, ln))  # insertion
+        if ins:
+            out.append(ins_bases[used:used + ln])
+            used += ln
             prev = p
         else:
-            prev = p + ln  # deletion
+            prev = p + ln
     out.append(s[prev:])
     return np.concatenate(out)
 
@@ -147,7 +154,61 @@ def to_fasta(names: list[str], seqs: list[np.ndarray]) -> str:
     return "".join(parts)
 
 
-def workload(name: str, seed: int | None = None, scale: float = 1.0):
+def _chunk(args) -> tuple[str, np.ndarray]:
+    """Query chunk i of a genome-vs-library workload, from its own random stream."""
+    name, seed, i, lib = args
+    rng = np.random.default_rng([seed, i])
+    if name == "plain":
+        qlen = 60_000
+    else:
+        qlen = int(np.clip(np.round(rng.lognormal(np.log(20_000), 1.0)), 1_000, 200_000))
+    g = random_dna(rng, qlen)
+    g = plant(rng, g, lib, 0.45, None, (0.02, 0.35), (0.01, 0.05))
+    g = add_n_runs(rng, g)
+    return f"chunk{i}", g
+
+
+_POOL_LIB = None
+
+
+def _init_pool(lib):
+    global _POOL_LIB
+    _POOL_LIB = lib
+
+
+def _chunk_pooled(args):
+    name, seed, i = args
+    return _chunk((name, seed, i, _POOL_LIB))
+
+
+def genome_library(seed: int | None = None) -> list[np.ndarray]:
+    """The 2,000-consensus library of the plain and batched workloads (log-normal lengths,
+    median 1.5 kb, 100-12,000 bp, about 5 Mb)."""
+    lrng = np.random.default_rng(0x524D42 + 1 if seed is None else seed)
+    lens = lognormal_lengths(lrng, 2000, 1500.0, 5_000_000.0, 100, 12_000)
+    return library(lrng, 2000, lens)
+
+
+def chunk_count(name: str, scale: float = 1.0) -> int:
+    return max(1, int(round({"plain": 1000, "batched": 20_000}[name] * scale)))
+
+
+def query_chunks(name: str, lib: list[np.ndarray], start: int, stop: int, seed: int | None = None,
+                 workers: int = 0) -> list[tuple[str, np.ndarray]]:
+    """Chunks start..stop-1 of a plain or batched workload's query set.  Every chunk has its
+    own random stream (seed, chunk index), so a batch of chunks is the same whichever other
+    chunks are made, and `workers` > 1 makes them in that many processes."""
+    base = 0x524D42 + {"plain": 1, "batched": 2}[name] if seed is None else seed
+    idx = range(start, stop)
+    if workers > 1 and stop - start > 8:
+        import multiprocessing as mp
+        # spawn: the callers may already hold a CUDA context, which a forked child must not touch
+        with mp.get_context("spawn").Pool(workers, initializer=_init_pool, initargs=(lib,)) as pool:
+            return pool.map(_chunk_pooled, [(name, base, i) for i in idx], chunksize=4)
+    return [_chunk((name, base, i, lib)) for i in idx]
+
+
+def workload(name: str, seed: int | None = None, scale: float = 1.0, workers: int = 0):
     """Returns (queries, library, params) with sequences as uint8 ASCII arrays.
 
     `scale` < 1 keeps the library and the per-query shapes but generates fewer queries
@@ -165,21 +226,8 @@ def workload(name: str, seed: int | None = None, scale: float = 1.0):
         params = dict(common, word_size=7, mask_level=80)
         return [("genome", g)], [(f"cons{i}", s) for i, s in enumerate(lib)], params
     if name in ("plain", "batched"):
-        lrng = np.random.default_rng(0x524D42 + 1 if seed is None else seed)
-        lens = lognormal_lengths(lrng, 2000, 1500.0, 5_000_000.0, 100, 12_000)
-        lib = library(lrng, 2000, lens)
-        if name == "plain":
-            n = max(1, int(round(1000 * scale)))
-            qlens = np.full(n, 60_000)
-        else:
-            n = max(1, int(round(20_000 * scale)))
-            qlens = np.clip(np.round(rng.lognormal(np.log(20_000), 1.0, n)), 1_000, 200_000).astype(np.int64)
-        qs = []
-        for i in range(n):
-            g = random_dna(rng, int(qlens[i]))
-            g = plant(rng, g, lib, 0.45, None, (0.02, 0.35), (0.01, 0.05))
-            g = add_n_runs(rng, g)
-            qs.append((f"chunk{i}", g))
+        lib = genome_library(seed)
+        qs = query_chunks(name, lib, 0, chunk_count(name, scale), seed, workers)
         params = dict(common, word_size=11, mask_level=80)
         return qs, [(f"cons{i}", s) for i, s in enumerate(lib)], params
     if name == "allvsall":

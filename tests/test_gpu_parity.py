@@ -19,16 +19,22 @@ def _built():
     build.build()
 
 
-def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str, kernels: int = 0):
+def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str, kernels: int = 0, pipeline: int = 0,
+             schedule: int = 0):
     m = api.ScoreMatrix.from_text(matrix_text, matrix_name)
     sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
                           xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
                           min_raw_gapped_score=p["min_raw_gapped_score"],
                           complexity_adjust=bool(p.get("complexity_adjust", 0)), dust=bool(p.get("dust", 0)),
                           mask_level=p.get("mask_level", -1), kernels=kernels, evalue=p.get("evalue", 0.0),
+                          pipeline=pipeline, schedule=schedule,
                           **dict(zip(("matrix_lambda", "matrix_k", "matrix_alpha", "matrix_beta"),
                                      p.get("cli_stats", (0.0, 0.0, 0.0, 0.0)))))
-    return api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
+    s = api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
+    if schedule == 1:
+        from rmblast_b200 import train_sched
+        s.set_schedule_model(train_sched.load_model())
+    return s
 
 
 def gpu_text(p, matrix_text, matrix_name, db_fasta, query_fasta, outfmt):
@@ -473,3 +479,108 @@ def test_gilist_matches_oracle(tmp_path):
                       "--mask-level", str(p["mask_level"]), "--complexity-adjust", "--outfmt", FIELDS])
     assert got.count("\n") > 2
     assert got == want
+
+
+# ---- the reference's chr22 goldens through the device path --------------------------------
+
+def _stage_lines(got: np.ndarray, stage: int) -> str:
+    if stage == 0:
+        lines = sorted(f"SEED strand={'+-'[r[0]]} q={r[1]} s={r[2]}" for r in got.tolist())
+    else:
+        lines = [f"UNGAP strand={'+-'[r[0]]} qs={r[1]} qe={r[2]} ss={r[3]} se={r[4]} score={np.int32(r[5])}"
+                 for r in got.tolist()]
+    return "".join(ln + "\n" for ln in lines)
+
+
+@pytest.mark.parametrize("stage,key", [(0, "seeds"), (1, "ungapped")])
+def test_chr22_stage_goldens_through_gpu(stage, key):
+    """The reference's chr22 regression goldens (rmblast-lib/tests/dedup_seeds_regression.rs and
+    ungapped_regression.rs): chr22 in its 51 NCBI chunks of ~1 Mb against alu.2bit at word 14,
+    through the device lookup tables, scan, exact word extension, ungapped extension and
+    diagonal-hash dedup (stage taps 0 and 1), 247,629 records each, content and order, compared
+    with the goldens' SHA-256."""
+    import chr22_fixture as F
+    _, seq = F.chr22()
+    p = F.STAGE_PARAMS
+    m = api.ScoreMatrix.from_text((G / "comparison.matrix").read_text(), "comparison.matrix")
+    sp = api.SearchParams(gap_open=p["gap_open"], gap_extend=p["gap_extend"], word_size=p["word_size"],
+                          xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"], xdrop_gap_final=p["xdrop_gap_final"],
+                          min_raw_gapped_score=p["min_raw_gapped_score"], complexity_adjust=True, dust=False,
+                          mask_level=p["mask_level"])
+    s = api.Searcher(sp, m, api.SubjectDb.from_twobit(G / "alu.2bit"))
+    q = api.encode(seq)
+    chunks = [np.concatenate([q[:1], q[1 + a:1 + b], q[-1:]]) for a, b in F.chunks(len(seq))]
+    assert len(chunks) == 51
+    text = _stage_lines(s.stage(chunks, stage), stage)
+    s.close()
+    want = F.stage_digests()[key]
+    assert F.digest(text) == (want["lines"], want["sha256"])
+
+
+def test_chr22_chunked_golden_through_c_abi():
+    """rmblastn/tests/cli.rs:246-274: chr22 30-33 Mb (3 Mb, three chunks) against db.fa at word 7,
+    DUST on, masklevel 80, through rmb_search_batch's multi-chunk path, against NCBI 2.17.1's
+    4,236 lines byte for byte."""
+    import chr22_fixture as F
+    _, seq = F.chr22()
+    p = dict(gap_open=20, gap_extend=5, word_size=7, xdrop_ungap=20, xdrop_gap=30, xdrop_gap_final=100,
+             min_raw_gapped_score=200, mask_level=80, dust=1)
+    s = searcher(p, (G / "comparison.matrix").read_text(), "comparison.matrix", (G / "db.fa").read_text())
+    res = s.search([api.encode(seq[30_000_000:33_000_000])], ["chr22_30M_33M"])
+    txt = res.tabular("6 score qseqid qstart qend sstrand sseqid sstart send")
+    s.close()
+    assert txt.count("\n") == 4236
+    assert txt == F.chunked_golden()
+
+
+# ---- the configurations at full or near-full size, and the pipelines ----------------------
+
+def _config_case(name: str, scale: float, **kw):
+    qf, dbf, p = synthetic(name, scale, synth.RM_FLAGS)
+    s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf, **kw)
+    recs = api.read_fasta(qf)
+    res = s.search([api.encode(x) for _, x in recs], [n for n, _ in recs])
+    txt = res.tabular(FIELDS)
+    s.close()
+    want, ctr, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS, threads=16)
+    return txt, want, res, ctr
+
+
+def test_config0_full_size_matches_oracle():
+    """Config 0 at its full size: the 100 kb genome with 300 planted copies against 50 consensi,
+    word 7, every line against the oracle."""
+    txt, want, res, ctr = _config_case("small", 1.0)
+    assert txt.count("\n") > 200
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"]
+
+
+def test_config1_fifty_chunks_matches_oracle():
+    """Config 1's shape at 50 of its 1,000 chunks of 60 kb (3 Mb) against the 2,000-consensus
+    library, word 11."""
+    txt, want, res, ctr = _config_case("plain", 0.05)
+    assert txt.count("\n") > 500
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"]
+
+
+def test_config3_learned_order_matches_oracle():
+    """Config 3: chunks of 1-200 kb through the batched pipeline with the learned record order
+    (the committed network), every line against the oracle."""
+    txt, want, res, ctr = _config_case("batched", 0.005, schedule=1)
+    assert txt.count("\n") > 500
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"]
+
+
+@pytest.mark.parametrize("name,scale", [("plain", 0.02), ("batched", 0.002)])
+def test_plain_pipeline_matches_oracle(name, scale):
+    """The plain pipeline (one launch per stage, one work item per thread, arrival order): the
+    same text as the oracle, and the same DP cells as the batched pipeline (only the
+    assignment of work to threads differs)."""
+    txt, want, res, ctr = _config_case(name, scale, pipeline=1)
+    assert txt == want
+    txt_b, _, res_b, _ = _config_case(name, scale, pipeline=0)
+    assert txt_b == txt
+    for k in ("word_hits", "ungapped", "prelim_dp", "prelims", "so_cells", "tb_cells"):
+        assert res.counters[k] == res_b.counters[k], k

@@ -2,19 +2,19 @@
 
 The CLI goldens are the reference's rmblastn/tests/data fixtures (copied into tests/golden by
 tests/golden/make_fixtures.py) with the command lines of rmblastn/tests/cli.rs:11-35, 144-290.
-The chr22 stage goldens (rmblast-lib/tests/*_regression.rs, 247,629 records each) are read from
-the reference tree when it is present.
+The chr22 stage goldens (rmblast-lib/tests/*_regression.rs, 247,629 records each) and the chunked
+chr22 golden (rmblastn/tests/cli.rs:246-274) are checked against the fixtures of
+tests/golden/make_fixtures.py: chr22 itself as a compressed .2bit, the stage goldens as line count
+and SHA-256 of their text, the chunked golden's text.
 """
-from pathlib import Path
-
 import pytest
 
+import chr22_fixture as F
 import oracle_ref as O
 
 G = O.GOLDEN
 RM = ["--gapopen", "20", "--gapextend", "5", "--word-size", "14", "--xdrop-ungap", "400",
       "--xdrop-gap-final", "200", "--xdrop-gap", "100", "--min-raw-gapped-score", "200", "--outfmt", O.RM_FIELDS]
-REF = Path("/root/reference")
 
 
 def _run(db, q, m, extra):
@@ -49,9 +49,17 @@ def test_identity_matrix_has_no_score_zero_hits():
         assert s >= 1 and b >= a
 
 
-@pytest.mark.skipif(not (REF / "tests/data/chr22.fa").exists(), reason="reference tree not mounted")
-@pytest.mark.parametrize("stage,gold", [(0, "chr22_dedup_seeds.txt"), (1, "chr22_ungapped_hits.txt")])
-def test_oracle_matches_chr22_stage_goldens(stage, gold):
+@pytest.fixture(scope="module")
+def chr22_fasta(tmp_path_factory):
+    name, seq = F.chr22()
+    return F.write_fasta(tmp_path_factory.mktemp("chr22") / "chr22.fa", name, seq)
+
+
+@pytest.mark.parametrize("stage,key", [(0, "seeds"), (1, "ungapped")])
+def test_oracle_matches_chr22_stage_goldens(chr22_fasta, stage, key):
+    """chr22 (51 chunks of ~1 Mb) against alu.2bit at word 14: the deduplicated seeds (sorted
+    text) and the ungapped hits (chunk, then subject, then the reference's hit order), content
+    and order, against the reference's 247,629-line goldens."""
     import ctypes as C
     lib = O.lib()
     lib.rmbo_stage_file.argtypes = [C.c_char_p] * 3 + [C.POINTER(O.OParams), C.c_int, C.POINTER(C.c_void_p),
@@ -59,32 +67,26 @@ def test_oracle_matches_chr22_stage_goldens(stage, gold):
     p = O.oparams(dict(O.RM_PARAMS, complexity_adjust=1, dust=0, mask_level=80))
     out = C.c_void_p()
     err = C.create_string_buffer(512)
-    rc = lib.rmbo_stage_file(str(REF / "tests/data/chr22.fa").encode(), str(REF / "tests/data/alu.2bit").encode(),
-                             str(REF / "rmblast-lib/tests/data/comparison.matrix").encode(), C.byref(p), stage,
-                             C.byref(out), err, 512)
+    rc = lib.rmbo_stage_file(str(chr22_fasta).encode(), str(G / "alu.2bit").encode(),
+                             str(G / "comparison.matrix").encode(), C.byref(p), stage, C.byref(out), err, 512)
     assert rc == 0, err.value
     got = C.string_at(out.value).decode()
     lib.rmbo_free(out)
-    want = (REF / "rmblast-lib/tests/data" / gold).read_text()
-    assert got.count("\n") == 247629
-    assert got == want
+    want = F.stage_digests()[key]
+    assert F.digest(got) == (want["lines"], want["sha256"])
 
 
-@pytest.mark.skipif(not (REF / "tests/data/chr22.fa").exists(), reason="reference tree not mounted")
 def test_oracle_chunked_path_matches_chr22_golden(tmp_path):
     """The multi-chunk path (a 3 Mb query: three chunks, DUST on the whole query, cross-chunk
     merge, full-query traceback) against NCBI 2.17.1: rmblastn/tests/cli.rs:246-274."""
-    seq = "".join(ln.strip() for ln in open(REF / "tests/data/chr22.fa") if not ln.startswith(">"))
-    sl = seq[30_000_000:33_000_000]
-    q = tmp_path / "chr22_30M_33M.fa"
-    q.write_text(">chr22_30M_33M\n" + "".join(sl[i:i + 60] + "\n" for i in range(0, len(sl), 60)))
+    _, seq = F.chr22()
+    q = F.write_fasta(tmp_path / "chr22_30M_33M.fa", "chr22_30M_33M", seq[30_000_000:33_000_000])
     got = O.run_cli(["--db", str(G / "db.fa"), "--query", str(q), "--matrix", str(G / "comparison.matrix"),
                      "--gapopen", "20", "--gapextend", "5", "--word-size", "7", "--min-raw-gapped-score", "200",
                      "--mask-level", "80", "--num-threads", "8",
                      "--outfmt", "6 score qseqid qstart qend sstrand sseqid sstart send"])
-    want = (REF / "rmblastn/tests/data/expected_chr22_30M-33M_ws7.ncbi-2.17.1.tsv").read_text()
     assert got.count("\n") == 4236
-    assert got == want
+    assert got == F.chunked_golden()
 
 
 @pytest.mark.parametrize("name,extra", [

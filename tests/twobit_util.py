@@ -42,3 +42,35 @@ def write_twobit(path, records, big_endian=False):
         off += len(b)
     with open(path, "wb") as f:
         f.write(head + index + b"".join(blobs))
+
+
+def read_twobit_ascii(data: bytes) -> list[tuple[str, bytes]]:
+    """(name, upper-case ASCII sequence with its N blocks as N) per record of a UCSC .2bit image
+    (either byte order); mask blocks are ignored.  For query fixtures kept as .2bit."""
+    magic = struct.unpack("<I", data[:4])[0]
+    e = "<" if magic == 0x1A412743 else ">"
+    _, _, count, _ = struct.unpack(e + "IIII", data[:16])
+    pos, index = 16, []
+    for _ in range(count):
+        ln = data[pos]
+        name = data[pos + 1:pos + 1 + ln].decode()
+        off = struct.unpack(e + "I", data[pos + 1 + ln:pos + 5 + ln])[0]
+        index.append((name, off))
+        pos += 5 + ln
+    letters = np.frombuffer(b"TCAG", dtype=np.uint8)
+    out = []
+    for name, off in index:
+        size, nb = struct.unpack(e + "II", data[off:off + 8])
+        p = off + 8
+        ns = np.frombuffer(data, dtype=e + "u4", count=nb, offset=p)
+        nl = np.frombuffer(data, dtype=e + "u4", count=nb, offset=p + 4 * nb)
+        p += 8 * nb
+        mb = struct.unpack(e + "I", data[p:p + 4])[0]
+        p += 4 + 8 * mb + 4
+        packed = np.frombuffer(data, dtype=np.uint8, count=(size + 3) // 4, offset=p)
+        codes = np.stack([(packed >> 6) & 3, (packed >> 4) & 3, (packed >> 2) & 3, packed & 3], axis=1).ravel()[:size]
+        seq = letters[codes]
+        for st, n in zip(ns.tolist(), nl.tolist()):
+            seq[st:st + n] = ord("N")
+        out.append((name, seq.tobytes()))
+    return out
