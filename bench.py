@@ -63,6 +63,7 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain and FIFO comparison arms")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch knobs")
     ap.add_argument("--dust", action="store_true", help="mask the queries with DUST (the reference's default)")
     ap.add_argument("--schedule", choices=["fifo", "learned"], default=None,
                     help="prelim DP record order (default: learned for the batched workload, else FIFO)")
@@ -76,10 +77,14 @@ def parse(argv=None):
     return a
 
 
+TUNE_SAMPLE_CHUNKS = 200
+
+
 def workload(args, rank: int):
-    """(batches of (id, ASCII chunk), library, params, total chunks) of this rank.  Batched and
-    plain chunk streams are per-chunk seeded, so rank r takes the stream's chunks after ranks
-    0 .. r-1 and shares the library; only the batches the run reaches are made."""
+    """(batches of (id, ASCII chunk), library, params, total chunks, tuning sample) of this rank.
+    Batched and plain chunk streams are per-chunk seeded, so rank r takes the stream's chunks
+    after ranks 0 .. r-1 and shares the library; only the batches the run reaches are made.  The
+    autotuner's sample is the stream's next chunks after every rank's (never a timed chunk)."""
     from rmblast_b200 import synth
     if args.workload in ("plain", "batched"):
         lib = synth.genome_library()
@@ -88,18 +93,23 @@ def workload(args, rank: int):
         nb = (n + step - 1) // step
         need = min(nb, args.warmup + args.steps)
         base = rank * n
-        qs = synth.query_chunks(args.workload, lib, base, base + min(n, need * step), workers=os.cpu_count() or 1)
+        workers = os.cpu_count() or 1
+        qs = synth.query_chunks(args.workload, lib, base, base + min(n, need * step), workers=workers)
         batches = [qs[i:i + step] for i in range(0, len(qs), step)]
         db = [(f"cons{i}", s) for i, s in enumerate(lib)]
         _, _, prm = synth.workload(args.workload, scale=1e-9)
         total = n
+        tail = max(int(os.environ.get("WORLD_SIZE", 1)), 1) * n
+        sample = synth.query_chunks(args.workload, lib, tail, tail + min(TUNE_SAMPLE_CHUNKS, max(step // 5, 1)),
+                                    workers=workers)
     else:
         qs, db, prm = synth.workload(args.workload, scale=args.scale)
         batches, total = [qs], len(qs)
+        sample = qs[:max(1, len(qs) // 20)]
     p = dict(prm, **synth.RM_FLAGS)
     if args.dust:
         p["dust"] = 1
-    return batches, db, p, total
+    return batches, db, p, total, sample
 
 
 def config_of(args, p, total_chunks, batches, db, world) -> dict:
@@ -218,7 +228,7 @@ def reference_arm(args, rank, world):
     taking consecutive queries."""
     if rank != 0:
         return
-    batches, db, p, total = workload(args, 0)
+    batches, db, p, total, _ = workload(args, 0)
     qs = [q for b in batches for q in b]
     per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     vals, start, first = [], 0, None
@@ -267,7 +277,7 @@ def main():
         reference_arm(args, rank, world)
         return
     # the query chunks are made (in spawned processes) before this process touches CUDA
-    batches, db, p, total = workload(args, rank)
+    batches, db, p, total, tune_sample = workload(args, rank)
     import torch
     from rmblast_b200 import api, build, synth
     build.build()
@@ -349,8 +359,11 @@ def main():
                 "stage_ms": {k: round(cc[k], 3) for k in ("gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
                                                           "gpu_ms_prelim", "gpu_ms_traceback")}}
 
-    # ---- the measured arm: resident, then end to end
+    # ---- the measured arm: autotuned launch knobs (batched pipeline), resident, then end to end
     s = searcher(args.pipeline, args.schedule)
+    tuned = None
+    if args.pipeline == "batched" and not args.no_autotune:
+        tuned = s.autotune([api.encode(x) for _, x in tune_sample])
     clk = {}
     ms_step, c = resident_arm(s, clk)
     for b in warm[:max(1, args.warmup // 2)]:
@@ -417,6 +430,10 @@ def main():
                 "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
                 "ms_per_step": e2e_ms},
     }
+    if tuned is not None:
+        line["autotune"] = {"knobs": tuned["tune"], "tuned_ms": tuned["best_ms"], "default_ms": tuned["default_ms"],
+                            "sample": f"{tuned['sample_queries']} chunks ({tuned['sample_bp']} bp) of the workload's "
+                                      "stream past the timed ones; device ms of the ungapped, dedup and prelim stages"}
     if model is not None and not args.sched_model:
         from rmblast_b200 import train_sched
         info = json.loads(train_sched.MODEL_PATH.read_text()).get("info", {})
@@ -456,6 +473,8 @@ def main():
                             "prelim_stage": arms["plain"]["prelim_ms"] / me["prelim_ms"] if me["prelim_ms"] else None}
         if args.schedule == "learned":
             s = searcher("batched", "fifo")
+            if tuned is not None:
+                s.set_tune(tuned["tune"])
             ms, cc = resident_arm(s)
             arms["batched_fifo"] = arm_summary(cc, ms)
             arms["batched_fifo"]["identical_output_first_step"] = s.search(enc[b0], ids[b0]).tabular(FIELDS) == text_b0

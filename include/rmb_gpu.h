@@ -61,6 +61,26 @@ typedef struct rmb_params {
 
 typedef struct rmb_ctx rmb_ctx;
 
+/* Launch knobs of the batched pipeline (no counterpart in the reference; none changes a result,
+ * only how work is laid out on the GPU).  rmb_ctx_create starts from the hand-swept defaults;
+ * rmb_autotune times candidates on sample queries and keeps the fastest; rmb_tune_get/set read
+ * and write them (a caller can persist and reuse a tuned set).
+ *   prelim_group            cell steps a lane of the thread-per-extension DP runs between its
+ *                           row-end blocks: 4, 8 or 16
+ *   prelim_blocks_per_sm    resident blocks per SM of that DP's persistent grid, 1..6
+ *   prelim_window           widest band, in cells, one thread keeps, 16..60: a wider extension is
+ *                           handed to a warp (32 threads per alignment)
+ *   prelim_budget_div       DP cells one thread spends on a record before a warp takes it:
+ *                           records / div, within 8,192 .. 2^20; 16..4096
+ *   ungapped_blocks_per_sm  blocks per SM of the persistent ungapped-extension grid, 1..8
+ *   dedup_extend_hits_per_pair  pair ranges averaging at least this many word hits per
+ *                           (query, subject) pair take the dedup kernel that extends only the
+ *                           hits the diagonal hash admits; 0 = always, < 0 = never */
+typedef struct rmb_tune {
+    int32_t prelim_group, prelim_blocks_per_sm, prelim_window, prelim_budget_div;
+    int32_t ungapped_blocks_per_sm, dedup_extend_hits_per_pair;
+} rmb_tune;
+
 /* Learned schedule of the preliminary DP (no counterpart in the reference, whose records run in
  * a fixed order; the order changes no result).  A 12 -> 64 -> 64 -> 1 ReLU network with BF16
  * weights predicts each ungapped record's DP cells (log1p), and with params.schedule = 1 the
@@ -267,6 +287,16 @@ int rmb_traceback_noalloc(int32_t device, const uint8_t* query, const uint8_t* q
                           uint32_t n, int32_t gap_open, int32_t gap_extend, int32_t xdrop_gap_final,
                           const int32_t scores[256], uint32_t* out, uint32_t* ops, uint32_t ops_cap, void* stream,
                           char* err, size_t errlen);
+
+/* The context's launch knobs (rmb_tune above).  rmb_tune_set rejects values outside the
+ * ranges given there.  rmb_autotune: one search of the sample queries per candidate set (the
+ * defaults, then one knob at a time around the best so far), each timed on the device; the
+ * fastest set stays on the context and is written to *best, its device time per search to
+ * *best_ms and the defaults' to *default_ms.  The sample's output is the same under every set. */
+int rmb_tune_get(const rmb_ctx* ctx, rmb_tune* out);
+int rmb_tune_set(rmb_ctx* ctx, const rmb_tune* tune, char* err, size_t errlen);
+int rmb_autotune(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
+                 rmb_tune* best, double* best_ms, double* default_ms, char* err, size_t errlen);
 
 /* Measurement helper: sustained int32 add/max throughput of the device in Tops/s (the
  * roofline denominator for the integer DP kernels). */

@@ -36,6 +36,11 @@ class _Params(C.Structure):
         "ka_lambda", "ka_k", "ka_h", "ka_alpha", "ka_beta", "evalue")]
 
 
+class _Tune(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("prelim_group", "prelim_blocks_per_sm", "prelim_window", "prelim_budget_div",
+                                         "ungapped_blocks_per_sm", "dedup_extend_hits_per_pair")]
+
+
 class _Hsp(C.Structure):
     _fields_ = [("score", C.c_int32)] + [(n, C.c_uint32) for n in (
         "q_start", "q_end", "q_len", "s_start", "s_end", "s_len", "subject_oid", "strand", "matches",
@@ -86,6 +91,10 @@ def load_library(path: Path = LIB_PATH) -> C.CDLL:
     lib.rmb_text_free.argtypes = [C.c_void_p]
     lib.rmb_text_free.restype = None
     lib.rmb_ctx_destroy.argtypes = [C.c_void_p]
+    lib.rmb_tune_get.argtypes = [C.c_void_p, C.POINTER(_Tune)]
+    lib.rmb_tune_set.argtypes = [C.c_void_p, C.POINTER(_Tune), C.c_char_p, C.c_size_t]
+    lib.rmb_autotune.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32), C.POINTER(_Tune),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_char_p, C.c_size_t]
     lib.rmb_ctx_destroy.restype = None
     lib.rmb_version.restype = C.c_char_p
     lib.rmb_queries_upload.argtypes = [C.c_void_p, C.c_uint32, u8pp, C.POINTER(C.c_uint32), C.POINTER(C.c_void_p),
@@ -104,6 +113,13 @@ def load_library(path: Path = LIB_PATH) -> C.CDLL:
     lib.rmb_sched_grad.argtypes = [C.c_int32, fp, fp, fp, C.c_uint32, fp, fp, C.c_char_p, C.c_size_t]
     lib.rmb_sched_predict.argtypes = [C.c_int32, fp, fp, C.c_uint64, fp, C.c_char_p, C.c_size_t]
     return lib
+
+
+def device_name(device: int = 0) -> tuple[str, int]:
+    """(name, SM count) of a CUDA device, through the CUDA runtime the library links."""
+    import torch
+    pr = torch.cuda.get_device_properties(device)
+    return pr.name, pr.multi_processor_count
 
 
 def int32_peak_tops(device: int = 0) -> float:
@@ -531,6 +547,51 @@ class Searcher:
             lib().rmb_text_free(C.cast(f, C.c_void_p))
             lib().rmb_text_free(C.cast(c, C.c_void_p))
         return feats, cells
+
+    def tune(self) -> dict:
+        """rmb_tune_get: the context's launch knobs."""
+        t = _Tune()
+        _check(lib().rmb_tune_get(self._ctx, C.byref(t)), C.create_string_buffer(1))
+        return {f: getattr(t, f) for f, _ in _Tune._fields_}
+
+    def set_tune(self, knobs: dict) -> None:
+        """rmb_tune_set: launch knobs (unlisted ones keep their current values)."""
+        cur = self.tune()
+        cur.update(knobs)
+        t = _Tune(*[int(cur[f]) for f, _ in _Tune._fields_])
+        err = C.create_string_buffer(512)
+        _check(lib().rmb_tune_set(self._ctx, C.byref(t), err, 512), err)
+
+    def autotune(self, queries: list[np.ndarray], cache: str | Path | None = None, key: str | None = None) -> dict:
+        """rmb_autotune on sample queries: the fastest launch knobs stay on the context.  With a
+        cache file, a set stored under `key` (default: the GPU's name and SM count with the
+        search parameters) is applied without timing anything, and a new result is stored."""
+        import json
+        key = key or self.tune_key()
+        store = {}
+        if cache and Path(cache).exists():
+            store = json.loads(Path(cache).read_text())
+            if key in store:
+                self.set_tune(store[key]["tune"])
+                return dict(store[key], cached=True)
+        n, qp, ql = self._queries(queries)
+        t = _Tune()
+        best, dflt = C.c_double(), C.c_double()
+        err = C.create_string_buffer(1024)
+        _check(lib().rmb_autotune(self._ctx, n, qp, ql, C.byref(t), C.byref(best), C.byref(dflt), err, 1024), err)
+        res = {"tune": {f: getattr(t, f) for f, _ in _Tune._fields_}, "best_ms": best.value,
+               "default_ms": dflt.value, "sample_queries": n, "sample_bp": int(sum(len(q) - 2 for q in queries))}
+        if cache:
+            store[key] = res
+            Path(cache).write_text(json.dumps(store, indent=1, sort_keys=True) + "\n")
+        return dict(res, cached=False)
+
+    def tune_key(self) -> str:
+        """GPU model and SM count plus the parameters that shape the work (word size, gaps, X-drops)."""
+        name, sms = device_name(self.params.device)
+        p = self.params
+        return (f"{name}/{sms}sm/w{p.word_size}/g{p.gap_open}.{p.gap_extend}/x{p.xdrop_ungap}.{p.xdrop_gap}."
+                f"{p.xdrop_gap_final}/s{p.schedule}")
 
     def upload(self, queries: list[np.ndarray]) -> "ResidentQueries":
         """rmb_queries_upload: the queries copied into device memory once."""

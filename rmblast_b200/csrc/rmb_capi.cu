@@ -147,6 +147,19 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
+// The hand-swept launch shape (B200, genome-vs-library workloads): the starting point of
+// rmb_autotune and the plain pipeline's fixed shape.
+static rmb_tune default_tune() {
+    rmb_tune t;
+    t.prelim_group = 8;
+    t.prelim_blocks_per_sm = 6;
+    t.prelim_window = 60;
+    t.prelim_budget_div = 128;
+    t.ungapped_blocks_per_sm = 8;
+    t.dedup_extend_hits_per_pair = 256;
+    return t;
+}
+
 struct rmb_ctx {
     rmb_params p{};
     GlueParams gp{};
@@ -168,6 +181,7 @@ struct rmb_ctx {
     // per-batch device buffers
     DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     bool prelim_stream = false;  // thread-per-extension prelim kernel (else the warp kernel)
+    rmb_tune tune = default_tune();  // launch knobs of the batched pipeline (rmb_tune_set / rmb_autotune)
     KaBlock ka;                  // E-value statistics (lambda <= 0: none)
     DBuf dust_scratch;           // per-thread DUST interval lists
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
@@ -466,28 +480,45 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             ctr.launches += 2;
             ctr.ms_scan += ms_since(t0);
 
-            // ---- ungapped extension of every hit, then the per-pair dedup
+            // ---- ungapped extension of every hit, then the per-pair dedup; or, for hit-dense
+            // pairs (most hits dropped by the hash), the dedup extending only what it admits
             t0 = std::chrono::steady_clock::now();
             C.ub.ensure(nh * sizeof(UngBox));
-            ev.start(st);
-            C.ung_queue.ensure(16);
-            CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
-                               C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st,
-                               P.pipeline == 1 ? nullptr : C.ung_queue.as<unsigned long long>()));
-            ev.stop(st);
-            CK(cudaStreamSynchronize(st));
-            ctr.gpu_ms_ungapped += ev.ms();
-            ctr.launches += nh ? 1 : 0;
-            ctr.ms_ungapped += ms_since(t0);
-            t0 = std::chrono::steady_clock::now();
-            C.flags.ensure(nh + 1);
-            C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
-            C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
-            ev.start(st);
-            CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], pair0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
-                            C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
-            ev.stop(st);
-            ctr.launches += 1;
+            const int32_t dx = C.tune.dedup_extend_hits_per_pair;
+            const bool fused = P.pipeline != 1 && dx >= 0 && nh >= (uint64_t)dx * npairs;
+            if (fused) {
+                C.flags.ensure(nh + 1);
+                C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+                C.ung_queue.ensure(16);
+                ev.start(st);
+                CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], pair0, npairs,
+                                       C.offs.as<uint64_t>(), C.hits.as<SeedHit>(), C.ub.as<UngBox>(),
+                                       C.flags.as<uint8_t>(), C.dd_cells.p, C.ung_queue.as<unsigned long long>(),
+                                       C.sms, st));
+                ev.stop(st);
+                ctr.launches += 1;
+            } else {
+                ev.start(st);
+                C.ung_queue.ensure(16);
+                CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
+                                   C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st,
+                                   P.pipeline == 1 ? nullptr : C.ung_queue.as<unsigned long long>(),
+                                   C.tune.ungapped_blocks_per_sm));
+                ev.stop(st);
+                CK(cudaStreamSynchronize(st));
+                ctr.gpu_ms_ungapped += ev.ms();
+                ctr.launches += nh ? 1 : 0;
+                ctr.ms_ungapped += ms_since(t0);
+                t0 = std::chrono::steady_clock::now();
+                C.flags.ensure(nh + 1);
+                C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
+                C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+                ev.start(st);
+                CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], pair0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
+                                C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
+                ev.stop(st);
+                ctr.launches += 1;
+            }
             C.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
             C.n_sel.ensure(16);
             tb = 0;
@@ -618,10 +649,17 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                     ctr.launches += 3;
                 }
                 ev_main.start(st);
+                // the plain pipeline keeps the hand-swept shape; the batched one takes the tuned knobs
+                const rmb_tune tn = P.pipeline == 1 ? default_tune() : C.tune;
+                StreamLaunch cfg;
+                cfg.group = tn.prelim_group;
+                cfg.blocks_per_sm = tn.prelim_blocks_per_sm;
+                cfg.window = tn.prelim_window;
+                cfg.budget_div = tn.prelim_budget_div;
                 CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
                                         C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
                                         C.cells.as<unsigned long long>(), C.sms, st, order, cells_out,
-                                        P.pipeline == 1));
+                                        P.pipeline == 1, cfg));
                 ev_main.stop(st);
                 if (cells_out) {
                     std::vector<float> f(nu * SCHED_NF_HOST);
@@ -1533,6 +1571,104 @@ int rmb_search_batch(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const
         return fail_out(e, err, errlen, RMB_EINVAL);
     }
     return rmb_search_resident(C, C->batch, out, err, errlen);
+}
+
+static void check_tune(const rmb_tune& t) {
+    if (t.prelim_group != 4 && t.prelim_group != 8 && t.prelim_group != 16)
+        throw Fail(RMB_EINVAL, "prelim_group must be 4, 8 or 16");
+    if (t.prelim_blocks_per_sm < 1 || t.prelim_blocks_per_sm > 6) throw Fail(RMB_EINVAL, "prelim_blocks_per_sm: 1..6");
+    if (t.prelim_window < 16 || t.prelim_window > 60) throw Fail(RMB_EINVAL, "prelim_window: 16..60");
+    if (t.prelim_budget_div < 16 || t.prelim_budget_div > 4096) throw Fail(RMB_EINVAL, "prelim_budget_div: 16..4096");
+    if (t.ungapped_blocks_per_sm < 1 || t.ungapped_blocks_per_sm > 8)
+        throw Fail(RMB_EINVAL, "ungapped_blocks_per_sm: 1..8");
+}
+
+int rmb_tune_get(const rmb_ctx* C, rmb_tune* out) {
+    if (!C || !out) return RMB_EINVAL;
+    *out = C->tune;
+    return RMB_OK;
+}
+
+int rmb_tune_set(rmb_ctx* C, const rmb_tune* t, char* err, size_t errlen) {
+    try {
+        if (!C || !t) throw Fail(RMB_EINVAL, "null argument");
+        check_tune(*t);
+        C->tune = *t;
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    }
+}
+
+// Coordinate descent over the knobs: the defaults, then each knob's alternatives with the others
+// at the best so far.  Each candidate runs the sample search twice; its time is the faster run's
+// device time in the stages the knobs shape (ungapped extension, dedup, prelim DP).
+int rmb_autotune(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uint32_t* qlen, rmb_tune* best,
+                 double* best_ms, double* default_ms, char* err, size_t errlen) {
+    try {
+        if (!C || !best) throw Fail(RMB_EINVAL, "null argument");
+        if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_autotune");
+        if (C->p.pipeline == 1) throw Fail(RMB_EINVAL, "the plain pipeline has no tuned knobs");
+        if (C->p.schedule == 1 && !C->sched_ready)
+            throw Fail(RMB_ESTATE, "schedule 1 needs the network: call rmb_sched_set_model first");
+        CK(cudaSetDevice(C->p.device));
+        QueriesPtr H(make_queries(C, nq, query, qlen));
+        const rmb_tune keep = C->tune;
+        auto time_of = [&](const rmb_tune& t) {
+            C->tune = t;
+            double ms = 1e300;
+            for (int rep = 0; rep < 2; ++rep) {
+                std::vector<std::vector<Hit>> hits;
+                rmb_counters ctr{};
+                run_search(*C, *H, hits, ctr, nullptr);
+                ms = std::min(ms, ctr.gpu_ms_ungapped + ctr.gpu_ms_dedup + ctr.gpu_ms_prelim);
+            }
+            return ms;
+        };
+        try {
+            rmb_tune cur = default_tune();
+            {  // grow the device buffers before anything is timed
+                std::vector<std::vector<Hit>> hits;
+                rmb_counters ctr{};
+                C->tune = cur;
+                run_search(*C, *H, hits, ctr, nullptr);
+            }
+            const double d_ms = time_of(cur);
+            double cur_ms = d_ms;
+            auto knob = [&](int32_t rmb_tune::*field, std::initializer_list<int32_t> alts) {
+                for (int32_t v : alts) {
+                    if (cur.*field == v) continue;
+                    rmb_tune t = cur;
+                    t.*field = v;
+                    const double ms = time_of(t);
+                    if (ms < cur_ms) {
+                        cur_ms = ms;
+                        cur = t;
+                    }
+                }
+            };
+            knob(&rmb_tune::prelim_group, {4, 16});
+            knob(&rmb_tune::prelim_blocks_per_sm, {4, 5});
+            knob(&rmb_tune::prelim_window, {32, 48});
+            knob(&rmb_tune::prelim_budget_div, {32, 512});
+            knob(&rmb_tune::ungapped_blocks_per_sm, {4, 6});
+            knob(&rmb_tune::dedup_extend_hits_per_pair, {0, -1});
+            C->tune = cur;
+            *best = cur;
+            if (best_ms) *best_ms = cur_ms;
+            if (default_ms) *default_ms = d_ms;
+        } catch (...) {
+            C->tune = keep;
+            throw;
+        }
+        return RMB_OK;
+    } catch (const Fail& e) {
+        return fail_out(e, err, errlen, e.code);
+    } catch (const std::bad_alloc& e) {
+        return fail_out(e, err, errlen, RMB_ENOMEM);
+    } catch (const std::exception& e) {
+        return fail_out(e, err, errlen, RMB_EINVAL);
+    }
 }
 
 int rmb_sched_set_model(rmb_ctx* C, const float* params, uint32_t n_params, char* err, size_t errlen) {

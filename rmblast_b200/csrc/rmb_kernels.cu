@@ -446,6 +446,131 @@ __global__ void __launch_bounds__(128) k_dedup(DevLib L, DevQueries Q, int32_t w
     }
 }
 
+// Bucket-parallel dedup with the ungapped extension of the hits the hash admits.  The reference
+// checks a word hit's diagonal against the hash first and extends only the hits it admits
+// (engine.rs:1151-1172, 1220-1261).  The hash's 512 buckets are independent: get and insert walk
+// only the chain of bucket(diag), and a stale cell is recycled only inside that chain
+// (diag_hash.rs:51-110); cells are drawn from one pool, but which index a cell gets changes
+// nothing.  So one warp replays one (query, subject) pair: the pair's hits go by in scan order,
+// 32 a round; the hits of a round that share a bucket take turns in scan order (one sub-round
+// each), the others run at once, and only an admitted hit is extended.  The reference's work,
+// in its order per bucket, with the buckets in parallel: for hit-dense pairs (an all-against-
+// all search keeps ~1% of its hits), where extending every hit first wastes most of the work.
+constexpr int DDX_WARPS = 8;
+
+__global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQueries Q,
+                                                                 const DevParams* __restrict__ P, int32_t ucut,
+                                                                 uint64_t pair0, uint64_t n_pairs,
+                                                                 const uint64_t* __restrict__ offs,
+                                                                 const SeedHit* __restrict__ hits,
+                                                                 UngBox* __restrict__ ub, uint8_t* __restrict__ flags,
+                                                                 DiagCell* __restrict__ cells,
+                                                                 unsigned long long* __restrict__ queue) {
+    __shared__ int32_t mat[256];
+    __shared__ uint32_t heads[DDX_WARPS][512];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
+    __syncthreads();
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    uint32_t* hd = heads[threadIdx.x >> 5];
+    const int32_t ws = P->word_size, xdrop = P->xdrop_ungap, window = 1 - ws;
+    const unsigned lt = (1u << lane) - 1u;
+    for (;;) {
+        unsigned long long w = 0;
+        if (lane == 0) w = atomicAdd(queue, 1ull);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= n_pairs) break;
+        const uint64_t b = offs[w], e = offs[w + 1];
+        if (b == e) continue;
+        const uint64_t pair = pair0 + w;
+        const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
+        const uint32_t qlen = Q.len[qi], slen = L.len[si];
+        const int32_t lw = Q.lw[qi];
+        const uint8_t* qf = Q.q + Q.off[qi];
+        const uint8_t* qr = Q.qrc + Q.off[qi];
+        const uint8_t* sp = L.plus + L.plus_off[si];
+        DiagCell* pool = cells + b;  // at most one cell per hit of the pair
+        for (int k = lane; k < 512; k += 32) hd[k] = 0;
+        __syncwarp();
+        uint32_t occ = 0;  // cells used, the same on every lane
+        for (uint64_t r = b; r < e; r += 32) {
+            const uint64_t i = r + (uint64_t)lane;
+            const bool have = i < e;
+            SeedHit h{0, 0};
+            int32_t diag = 0;
+            uint32_t key = 0, bk = 512u + (uint32_t)lane;  // lanes without a hit: a bucket of their own
+            if (have) {
+                h = hits[i];
+                const uint32_t qo = h.qs & 0x7fffffffu, so = h.s;
+                if (!(h.qs >> 31)) {
+                    diag = (int32_t)(so - qo);
+                    key = so;
+                } else {
+                    diag = (int32_t)(slen - 2u * qlen - 1u + (qo - so));
+                    key = slen - so - (uint32_t)lw;
+                }
+                bk = diag_bucket(diag);
+            }
+            const unsigned same = __match_any_sync(FULL, bk);
+            const int turn = __popc(same & lt);
+            const int turns = __reduce_max_sync(FULL, have ? __popc(same) : 0);
+            for (int t = 0; t < turns; ++t) {
+                const bool mine = have && turn == t;
+                bool ext = false;
+                uint32_t head = 0;
+                if (mine) {
+                    head = hd[bk];
+                    uint32_t last = 0;
+                    for (uint32_t c = head; c; c = pool[c - 1].next)
+                        if (pool[c - 1].diag == diag) { last = pool[c - 1].level; break; }
+                    if (key < last) flags[i] = 0;
+                    else ext = true;
+                }
+                UngBox u{};
+                if (ext) {
+                    const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
+                    UngWalk walk;
+                    if (!(h.qs >> 31)) walk.start(qf, sp, (int32_t)qlen, (int32_t)slen, qo, so, xdrop);
+                    else walk.start(qr, sp, (int32_t)qlen, (int32_t)slen, (int32_t)qlen - 1 - qo,
+                                    (int32_t)slen - 1 - so, xdrop);
+                    while (walk.step(mat) != 2) {
+                    }
+                    int32_t sc;
+                    uint32_t a0, a1, c0, c1;
+                    walk.result(sc, a0, a1, c0, c1);
+                    u.score = sc;
+                    if (!(h.qs >> 31)) {
+                        u.q_start = a0; u.q_end = a1; u.s_start = c0; u.s_end = c1;
+                        u.store = sc >= ucut ? c1 : h.s + (uint32_t)ws;
+                    } else {
+                        u.q_start = qlen - a1; u.q_end = qlen - a0; u.s_start = slen - c1; u.s_end = slen - c0;
+                        u.store = sc >= ucut ? c1 : key + (uint32_t)ws;
+                    }
+                    ub[i] = u;
+                    flags[i] = sc >= ucut ? 3 : 1;
+                }
+                bool append = false;
+                if (ext) {
+                    append = true;
+                    for (uint32_t c = head; c; c = pool[c - 1].next) {
+                        DiagCell& cl = pool[c - 1];
+                        if (cl.diag == diag) { cl.level = u.store; append = false; break; }
+                        if ((int32_t)(key - cl.level) > window) { cl.diag = diag; cl.level = u.store; append = false; break; }
+                    }
+                }
+                const unsigned nn = __ballot_sync(FULL, append);
+                if (append) {
+                    const uint32_t idx = occ + (uint32_t)__popc(nn & lt) + 1u;
+                    pool[idx - 1] = DiagCell{diag, u.store, head};
+                    hd[bk] = idx;
+                }
+                occ += (uint32_t)__popc(nn);
+                __syncwarp();  // this turn's chain updates before the next turn reads them
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // score-only X-drop DP: search/gapped.rs:124-337 (outer sequence a, inner sequence b)
 // ---------------------------------------------------------------------------------------
@@ -1164,9 +1289,10 @@ struct StreamDevEnv {
     }
     __device__ __forceinline__ void overflow(uint32_t t) { wide[atomicAdd(n_wide, 1u)] = t; }
     __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
-    // the initial-row residues of every lane that started an extension: lane k copies index k
-    // (and k + 32) into that lane's ring, so the byte loads of one row go out together
-    __device__ __forceinline__ void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n) {
+    // the initial rows of every lane that started an extension: lane k writes entry k (and
+    // k + 32) of that lane's ring (residue, cell, gap), so the byte loads of one row go out together
+    __device__ __forceinline__ void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n,
+                                              uint32_t J, int32_t goe, int32_t ge) {
         unsigned need = __ballot_sync(0xffffffffu, pending);
         if (!need) return;
         const int lane = threadIdx.x & 31;
@@ -1175,9 +1301,10 @@ struct StreamDevEnv {
             need &= need - 1;
             const uint8_t* q = (const uint8_t*)__shfl_sync(0xffffffffu, (unsigned long long)qal, L);
             const int32_t p = __shfl_sync(0xffffffffu, pb, L), d = __shfl_sync(0xffffffffu, dir, L);
-            const uint32_t c = __shfl_sync(0xffffffffu, n, L);
+            const uint32_t c = __shfl_sync(0xffffffffu, n, L), j = __shfl_sync(0xffffffffu, J, L);
             uint32_t* ringL = my - lane + L;
-            for (uint32_t k = lane; k < c; k += 32) ringL[(k % STREAM_RING) * STREAM_BLOCK] = q[p + d * (int32_t)k] & 15u;
+            for (uint32_t k = lane; k < c; k += 32)
+                ringL[(k % STREAM_RING) * STREAM_BLOCK] = stream_initial_entry(k, j, goe, ge, q[p + d * (int32_t)k] & 15u);
         }
         __syncwarp();
     }
@@ -1189,7 +1316,7 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
                 PrelimOut* __restrict__ out,
                 uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide, unsigned int* __restrict__ queue,
                 unsigned long long* __restrict__ cells_total, uint32_t max_cells,
-                const uint32_t* __restrict__ order, uint32_t* __restrict__ cells_out) {
+                const uint32_t* __restrict__ order, uint32_t* __restrict__ cells_out, uint32_t window) {
     __shared__ uint32_t ring[STREAM_RING * STREAM_BLOCK];
     __shared__ int32_t smat[256];
     {
@@ -1202,7 +1329,7 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
     __syncthreads();
     StreamDevEnv<QUEUE> env{ring + threadIdx.x, queue, n_wide, wide};
     const StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells,
-                       order, cells_out};
+                       order, cells_out, window};
     const unsigned long long cells = prelim_stream_thread<U>(A, env);
     if (cells) atomicAdd(cells_total, cells);
 }
@@ -1848,7 +1975,7 @@ cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t*
 
 cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut, uint64_t n,
                             const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st,
-                            unsigned long long* queue) {
+                            unsigned long long* queue, int blocks_per_sm) {
     if (!n) return cudaSuccess;
     const int block = 256;
     if (!queue) {  // plain: one hit per thread
@@ -1858,7 +1985,8 @@ cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParam
     }
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    k_ungapped<true><<<grid_for(n, block, 8, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out, queue);
+    const int bps = blocks_per_sm < 1 ? 1 : blocks_per_sm > 8 ? 8 : blocks_per_sm;
+    k_ungapped<true><<<grid_for(n, block, bps, sms), block, 0, st>>>(L, Q, P, ucut, n, hits, hit_pair, out, queue);
     return cudaGetLastError();
 }
 
@@ -1876,6 +2004,19 @@ cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32
 }
 
 size_t diag_cell_bytes() { return sizeof(DiagCell); }
+cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
+                                uint64_t pair0, uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits,
+                                UngBox* ub, uint8_t* flags, void* cells, unsigned long long* queue, int sms,
+                                cudaStream_t st) {
+    if (!n_pairs) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    const uint64_t want = (n_pairs + DDX_WARPS - 1) / DDX_WARPS;
+    const uint64_t cap = (uint64_t)sms * 8;
+    k_dedup_extend<<<(unsigned)(want < cap ? want : cap), DDX_WARPS * 32, 0, st>>>(
+        L, Q, P, ucut, pair0, n_pairs, offs, hits, ub, flags, (DiagCell*)cells, queue);
+    return cudaGetLastError();
+}
 
 constexpr int PRELIM_RING = 256;
 
@@ -1915,25 +2056,37 @@ cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevPa
 
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
                                  unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
-                                 const uint32_t* order, uint32_t* cells_out, bool plain) {
+                                 const uint32_t* order, uint32_t* cells_out, bool plain, const StreamLaunch& cfg) {
     if (!n) return cudaSuccess;
     const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
-    const uint64_t cap = (uint64_t)sms * STREAM_BLOCKS_PER_SM;
+    const int bps = cfg.blocks_per_sm < 1 ? 1 : cfg.blocks_per_sm > STREAM_BLOCKS_PER_SM ? STREAM_BLOCKS_PER_SM
+                                                                                          : cfg.blocks_per_sm;
+    const uint64_t cap = (uint64_t)sms * bps;
     const int grid = (int)(want < cap ? want : cap);
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
-    const uint64_t budget = n / 128;
+    const uint64_t budget = n / (uint64_t)(cfg.budget_div > 0 ? cfg.budget_div : 128);
     // with the records in descending predicted cost the long ones start first: the full budget
     const uint32_t max_cells = order ? STREAM_MAX_CELLS
                                      : (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
                                                   : budget > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : budget);
-    // groups of 8 cell steps: 4 and 6 lose more to row ends, 12 and 16 to idle lanes (B200 sweep)
-    if (plain)  // one record per thread, the whole grid at once
-        k_prelim_stream<8, false><<<(unsigned)want, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide,
-                                                                            n_wide, n_wide + 1, cells, max_cells,
-                                                                            order, cells_out);
-    else
-        k_prelim_stream<8, true><<<grid, STREAM_BLOCK, 0, st>>>(P, n, (const PrelimGeo*)geo, out, wide, n_wide,
-                                                                n_wide + 1, cells, max_cells, order, cells_out);
+    const uint32_t window = cfg.window < 1 ? 1 : cfg.window > STREAM_WINDOW ? STREAM_WINDOW : (uint32_t)cfg.window;
+    const PrelimGeo* g = (const PrelimGeo*)geo;
+#define RMB_STREAM_LAUNCH(U)                                                                                      \
+    do {                                                                                                         \
+        if (plain) /* one record per thread, the whole grid at once */                                           \
+            k_prelim_stream<U, false><<<(unsigned)want, STREAM_BLOCK, 0, st>>>(P, n, g, out, wide, n_wide,       \
+                                                                               n_wide + 1, cells, max_cells,     \
+                                                                               order, cells_out, window);        \
+        else                                                                                                     \
+            k_prelim_stream<U, true><<<grid, STREAM_BLOCK, 0, st>>>(P, n, g, out, wide, n_wide, n_wide + 1,      \
+                                                                    cells, max_cells, order, cells_out, window); \
+    } while (0)
+    // groups of cell steps between row-end blocks: smaller groups run more row-end blocks, larger
+    // ones leave lanes idle longer (8 was the B200 hand sweep's best on the genome workloads)
+    if (cfg.group == 4) RMB_STREAM_LAUNCH(4);
+    else if (cfg.group == 16) RMB_STREAM_LAUNCH(16);
+    else RMB_STREAM_LAUNCH(8);
+#undef RMB_STREAM_LAUNCH
     return cudaGetLastError();
 }
 

@@ -25,8 +25,14 @@ cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t*
 // queue: 8 bytes of device scratch (the hit queue counter; zeroed here)
 cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut, uint64_t n,
                             const SeedHit* hits, const uint32_t* hit_pair, UngBox* out, int sms, cudaStream_t st,
-                            unsigned long long* queue);
+                            unsigned long long* queue, int blocks_per_sm = 8);
 uint64_t dedup_threads(int sms);
+// Bucket-parallel diagonal dedup that extends only the hits the hash admits (one warp per pair):
+// flags and boxes as launch_ungapped + launch_dedup give them.
+cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
+                                uint64_t pair0, uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits,
+                                UngBox* ub, uint8_t* flags, void* cells, unsigned long long* queue, int sms,
+                                cudaStream_t st);
 size_t diag_cell_bytes();
 cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32_t ucut, uint64_t pair0,
                          uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits, const UngBox* ub, uint8_t* flags,
@@ -44,9 +50,14 @@ size_t prelim_geo_bytes();
 cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                void* geo, int sms, cudaStream_t st);
+// Launch shape of the thread-per-extension DP (from rmb_tune): group of cell steps between
+// row-end blocks (4, 8, 16), resident blocks per SM, widest band a thread keeps, cell budget divisor.
+struct StreamLaunch {
+    int group = 8, blocks_per_sm = 6, window = 60, budget_div = 128;
+};
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
                                  unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
-                                 const uint32_t* order = nullptr, uint32_t* cells_out = nullptr, bool plain = false);
+                                 const uint32_t* order, uint32_t* cells_out, bool plain, const StreamLaunch& cfg);
 // Learned schedule (rmb_sched.cuh).  Raw features of each record (n x SCHED_NF floats); the
 // network's predicted log1p cells of every record and the records in descending predicted cost
 // (order, for launch_prelim_stream; scratch: sched_order_scratch_bytes()); the network on given

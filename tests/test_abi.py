@@ -112,7 +112,7 @@ def test_python_mirror_matches_header_struct_layout(tmp_path):
     if cc is None:
         pytest.skip("no C compiler")
     structs = {"rmb_params": api._Params, "rmb_hsp": api._Hsp, "rmb_counters": api._Counters,
-               "rmb_results": api._Results}
+               "rmb_results": api._Results, "rmb_tune": api._Tune}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rmb_gpu.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -584,3 +584,31 @@ def test_plain_pipeline_matches_oracle(name, scale):
     assert txt_b == txt
     for k in ("word_hits", "ungapped", "prelim_dp", "prelims", "so_cells", "tb_cells"):
         assert res.counters[k] == res_b.counters[k], k
+
+
+@pytest.mark.parametrize("name,scale", [("plain", 0.01), ("allvsall", 0.03)])
+def test_tune_knobs_leave_output_unchanged(name, scale):
+    """The launch knobs (rmb_tune) shape only how the work is laid out: extreme settings of each,
+    both dedup paths (the fused bucket-parallel dedup-extension and the extend-then-dedup pair),
+    and the autotuner's pick give the oracle's text byte for byte."""
+    qf, dbf, p = synthetic(name, scale, synth.RM_FLAGS)
+    s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf)
+    recs = api.read_fasta(qf)
+    enc = [api.encode(x) for _, x in recs]
+    ids = [n for n, _ in recs]
+    want, _, _ = O.search_text(qf, dbf, synth.MATRIX_TEXT, synth.MATRIX_NAME, p, FIELDS, threads=16)
+    assert want.count("\n") > 20
+    default = s.tune()
+    assert s.search(enc, ids).tabular(FIELDS) == want
+    for knobs in (dict(prelim_group=4), dict(prelim_group=16), dict(prelim_window=16, prelim_budget_div=16),
+                  dict(prelim_blocks_per_sm=1, ungapped_blocks_per_sm=1), dict(prelim_budget_div=4096),
+                  dict(dedup_extend_hits_per_pair=0), dict(dedup_extend_hits_per_pair=-1)):
+        s.set_tune(dict(default, **knobs))
+        assert s.search(enc, ids).tabular(FIELDS) == want, knobs
+    s.set_tune(default)
+    with pytest.raises(api.RmbError):
+        s.set_tune(dict(default, prelim_group=5))
+    r = s.autotune(enc[:max(1, len(enc) // 2)])
+    assert r["best_ms"] <= r["default_ms"] and r["tune"] == s.tune()
+    assert s.search(enc, ids).tabular(FIELDS) == want
+    s.close()
