@@ -39,6 +39,23 @@ def ranking_stats(pred: np.ndarray, cells: np.ndarray) -> dict:
             "cells_share_true_top5": round(float(np.sort(cells)[::-1][:k5].sum()) / tot, 4)}
 
 
+def queue_makespan(cells: np.ndarray, order: np.ndarray, workers: int) -> int:
+    """The finishing time, in DP cells, of `workers` lanes that each take the next record of one
+    queue (in `order`) when their last one is done -- the record queue of k_prelim_stream, with a
+    record's time taken as its cells.  Records are handed out in queue order to whichever lane is
+    free first (list scheduling), the lanes all starting at 0."""
+    import heapq
+    c = np.asarray(cells, dtype=np.int64)[np.asarray(order)]
+    w = min(workers, len(c))
+    if w == 0:
+        return 0
+    free = [int(x) for x in c[:w]]
+    heapq.heapify(free)
+    for x in c[w:].tolist():
+        heapq.heapreplace(free, free[0] + x)
+    return max(free)
+
+
 def load_model(path: Path = MODEL_PATH) -> np.ndarray:
     """The committed network parameters (rmb_sched layout) for Searcher.set_schedule_model."""
     return np.asarray(json.loads(path.read_text())["params"], dtype=np.float32)

@@ -49,3 +49,19 @@ def test_ranking_stats():
     assert perfect["cells_share_pred_top5"] == perfect["cells_share_true_top5"]
     chance = train_sched.ranking_stats(rng.normal(size=20000), cells)
     assert abs(chance["spearman"]) < 0.05 and chance["recall_true_top1_in_pred_top5"] < 0.15
+
+
+def test_queue_makespan_list_scheduling():
+    """The queue simulation behind the schedule's gain test: lanes take records in queue order,
+    each record going to the lane that is free first."""
+    cells = np.array([5, 1, 1, 1, 1, 1])
+    assert train_sched.queue_makespan(cells, np.arange(6), 2) == 5  # 5 | 1+1+1+1+1
+    assert train_sched.queue_makespan(cells, np.arange(6)[::-1], 2) == 7  # the long record last
+    assert train_sched.queue_makespan(cells, np.arange(6), 1) == 10
+    assert train_sched.queue_makespan(cells, np.arange(6), 64) == 5
+    rng = np.random.default_rng(3)
+    c = rng.integers(1, 1000, 5000)
+    # longest first is never worse than 4/3 of the optimum; any order is within 2x the lower bound
+    lb = max(c.sum() / 16, c.max())
+    assert train_sched.queue_makespan(c, np.argsort(-c, kind="stable"), 16) <= 4 / 3 * lb + 1
+    assert train_sched.queue_makespan(c, np.arange(5000), 16) <= 2 * lb
