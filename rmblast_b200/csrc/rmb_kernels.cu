@@ -1289,10 +1289,9 @@ struct StreamDevEnv {
     }
     __device__ __forceinline__ void overflow(uint32_t t) { wide[atomicAdd(n_wide, 1u)] = t; }
     __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
-    // the initial rows of every lane that started an extension: lane k writes entry k (and
-    // k + 32) of that lane's ring (residue, cell, gap), so the byte loads of one row go out together
-    __device__ __forceinline__ void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n,
-                                              uint32_t J, int32_t goe, int32_t ge) {
+    // the initial-row residues of every lane that started an extension: lane k copies index k
+    // (and k + 32) into that lane's ring, so the byte loads of one row go out together
+    __device__ __forceinline__ void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n) {
         unsigned need = __ballot_sync(0xffffffffu, pending);
         if (!need) return;
         const int lane = threadIdx.x & 31;
@@ -1301,10 +1300,9 @@ struct StreamDevEnv {
             need &= need - 1;
             const uint8_t* q = (const uint8_t*)__shfl_sync(0xffffffffu, (unsigned long long)qal, L);
             const int32_t p = __shfl_sync(0xffffffffu, pb, L), d = __shfl_sync(0xffffffffu, dir, L);
-            const uint32_t c = __shfl_sync(0xffffffffu, n, L), j = __shfl_sync(0xffffffffu, J, L);
+            const uint32_t c = __shfl_sync(0xffffffffu, n, L);
             uint32_t* ringL = my - lane + L;
-            for (uint32_t k = lane; k < c; k += 32)
-                ringL[(k % STREAM_RING) * STREAM_BLOCK] = stream_initial_entry(k, j, goe, ge, q[p + d * (int32_t)k] & 15u);
+            for (uint32_t k = lane; k < c; k += 32) ringL[(k % STREAM_RING) * STREAM_BLOCK] = q[p + d * (int32_t)k] & 15u;
         }
         __syncwarp();
     }

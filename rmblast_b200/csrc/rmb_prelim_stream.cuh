@@ -13,12 +13,12 @@
 // row.  Record changes happen in the same place.  A warp-wide vote at the top of every group
 // brings the lanes back together.
 //
-// Within a group the cell step keeps no band index: it records which of its U cells survived the
-// X-drop test and which raised the best score as bits of two masks, and the group's end turns them
-// into the row's first and last surviving cell and the best cell's index (gapped.rs:243-256 keeps
-// them per cell; the first surviving cell, the last one and the last improving one are the same).
-//
-// Storage differs from the reference's in two ways, neither of which changes a result:
+// Storage differs from the reference's in three ways, none of which changes a result:
+//  - The band entries that the reference writes in a loop, the initial row (gapped.rs:187-200)
+//    and the end-of-row extension cells (gapped.rs:307-319), are not written: a row computes
+//    them from (vlo, nvirt, ext_val) when it reads them, a few predicated operations a cell
+//    (cheaper than a loop in the row end, which runs divergently).  The MININT sentinel
+//    (gapped.rs:325-330) is written at the row end as a clamped entry (below).
 //  - An entry is 32 bits: bits 0-3 the column residue, bits 4-17 the cell and bits 18-31 the
 //    vertical gap, both as 14-bit values relative to the extension's origin and clamped below at
 //    FLOOR.  The DP runs in the same frame, so entries are read and written without conversion.
@@ -29,9 +29,6 @@
 //    score, so the clamp only moves values that can no longer make a cell survive (MININT
 //    included).  The residues of a row's band are copied in (a word of the column sequence at a
 //    time) at the row end that sets the band, so the cell step reads the residue with the entry.
-//    The initial row (gapped.rs:187-200) is written with its residues by the whole warp when an
-//    extension starts; the end-of-row extension cells (gapped.rs:307-319, half a cell a row on
-//    the genome workloads) and the MININT sentinel (gapped.rs:325-330) are written at the row end.
 //  - The band window of a row (b_size - first_b cells) must fit the launch's window (at most
 //    STREAM_WINDOW); a record whose window grows past it, or whose cell count passes the budget,
 //    is listed for the warp kernel.
@@ -81,33 +78,6 @@ __host__ __device__ __forceinline__ uint32_t stream_pack(int32_t ex, int32_t ey,
 #endif
 }
 
-// Index of the lowest / highest set bit of a nonzero mask.
-__host__ __device__ __forceinline__ uint32_t stream_low_bit(uint32_t m) {
-#ifdef __CUDA_ARCH__
-    return (uint32_t)(__ffs((int)m) - 1);
-#else
-    return (uint32_t)__builtin_ctz(m);
-#endif
-}
-__host__ __device__ __forceinline__ uint32_t stream_high_bit(uint32_t m) {
-#ifdef __CUDA_ARCH__
-    return 31u - (uint32_t)__clz((int)m);
-#else
-    return 31u - (uint32_t)__builtin_clz(m);
-#endif
-}
-
-// The entry of band index k of an extension's initial row (gapped.rs:187-200): cell 0 is 0 with
-// gap -goe; cell k in 1..J is v = -goe - (k - 1) ge with gap v - goe (clamped at FLOOR); past J
-// only the residue.
-__host__ __device__ __forceinline__ uint32_t stream_initial_entry(uint32_t k, uint32_t J, int32_t goe, int32_t ge,
-                                                                  uint32_t residue) {
-    if (k > J) return residue;
-    const int32_t v = k == 0 ? 0 : -goe - (int32_t)(k - 1) * ge;
-    const int32_t g = v - goe;
-    return stream_pack(v, g > STREAM_FLOOR ? g : STREAM_FLOOR, residue);
-}
-
 // Constants of one launch.
 struct StreamArgs {
     const int32_t* smat;  // 16 x 16 scores, clamped below at -(X + 1) for the largest X
@@ -138,13 +108,11 @@ struct StreamDiv {
 // The work of one thread until the record queue is empty; returns the DP cells of the records
 // it completed.  Env supplies the thread's ring (`uint32_t& at(j)`: the entry of band index j,
 // slot j % STREAM_RING), the queue (`uint32_t take()`), the overflow list (`overflow(t)`), a
-// warp-wide vote (`bool any(bool)`) and `fill_rows(pending, qal, pb, dir, n, J, goe, ge)`: called
-// by every lane of the warp together, it writes entry k (k < n) of each pending lane's ring: the
-// residue qal[pb + dir * k] & 15 and, for k <= J, the initial row's cell and gap (k = 0: 0 and
-// -goe; k >= 1: v = -goe - (k - 1) ge and v - goe, clamped at FLOOR).
+// warp-wide vote (`bool any(bool)`) and `fill_rows(pending, qal, pb, dir, n)`: called by every
+// lane of the warp together, it sets entry k (k < n) of each pending lane's ring to the residue
+// qal[pb + dir * k] & 15.
 template <int U, class Env>
 __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(const StreamArgs& A, Env& env) {
-    static_assert(U <= 16, "the group masks hold 16 cell steps");
     const int32_t ge = A.ge, goe = A.goe;
     const StreamDiv div_ge(ge);
 
@@ -164,23 +132,25 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
     uint8_t a_nx = 0, a0_left = 0, a0_right = 0;
     const int32_t* srow = A.smat;
     uint32_t m = 0, nb = 0, ai = 0, bi = 0, first_b = 0, b_size = 0, last_b = 0, best_a = 0, best_b = 0;
-    bool seen = false;  // a cell of this row survived (first_b is set)
     // scores relative to `origin` (the extension's score 0 until the first rebase)
     int32_t best = 0, prev_best = 0, thr = 0, sc = 0, gap_row = 0, origin = 0;
-    uint32_t init_j = 0;  // J of an extension whose initial row is still to be written
+    // the extension cells of the last row end (gapped.rs:307-319), computed when read: band
+    // indices vlo .. vlo + nvirt - 1 hold ext_val - (j - vlo) * ge and that minus gap_open_extend
+    uint32_t vlo = 0, nvirt = 0;
+    int32_t ext_val = 0;
     unsigned long long cells = 0;
     // records come from one queue; the next index is fetched one record ahead
     uint32_t next_t = env.take();
     bool fetch = true;  // no extension running: finish the last one and start the next
     bool dp_fail = false;
     bool out_of_records = false;
-    bool init_pending = false;  // an extension started whose initial row is not in yet
+    bool init_pending = false;  // an extension started whose initial residues are not in yet
 
     auto new_row = [&]() {
         srow = A.smat + (uint32_t)(a_nx & 15) * 16u;
         if (ai + 1 < m) a_nx = abase[(ptrdiff_t)dir * (ptrdiff_t)(ai + 1)];  // next row's residue
         sc = MININT; gap_row = MININT;
-        last_b = first_b; prev_best = best; bi = first_b; seen = false;
+        last_b = first_b; prev_best = best; bi = first_b;
         rec_cells += b_size - first_b;
     };
     // The residues of the band indices of one aligned word of the column sequence, from the
@@ -209,22 +179,23 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
     for (;;) {
         if (!env.any(!out_of_records)) break;
         // U cell steps (gapped.rs:234-296); a lane whose row has ended waits for the row end
-        const uint32_t bi0 = bi;
-        const uint32_t rem = bi < b_size ? b_size - bi : 0u;
-        uint32_t amask = 0, imask = 0;  // bit u: step u's cell survived / raised the best
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if ((uint32_t)u < rem) {
-                uint32_t& slot = env.at(bi0 + (uint32_t)u);
+            if (bi < b_size) {
+                uint32_t& slot = env.at(bi);
                 const uint32_t w = slot;
-                const int32_t cx = (int32_t)(w << 14) >> 18;
-                const int32_t cy = (int32_t)w >> 18;
-                // the diagonal of the next cell; at the row's last cell it is not used
+                const uint32_t rel = bi - vlo;
+                const bool virt = rel < nvirt;
+                const int32_t v = ext_val - (int32_t)rel * ge;
+                const int32_t cx = virt ? v : (int32_t)(w << 14) >> 18;
+                const int32_t cy = virt ? v - goe : (int32_t)w >> 18;
+                // the diagonal of the next cell; at bi == nb (the row's last cell) it is not used
                 const int32_t nxt = cx + srow[w & 15u];
                 const int32_t cell = __vimax3_s32(sc, cy, gap_row);
                 const bool alive = cell >= thr;
-                if (alive) amask |= 1u << u;
-                if (cell > best) imask |= 1u << u;
+                if (!alive && bi == first_b) ++first_b;
+                if (alive) last_b = bi;
+                if (cell > best) best_b = bi;
                 best = max(best, cell);
                 thr = __viaddmax_s32(cell, -xdrop, thr);  // best - xdrop
                 const int32_t open = cell - goe;
@@ -233,19 +204,8 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                 const int32_t ey = alive ? __vimax3_s32(cy - ge, open, STREAM_FLOOR) : cy;
                 slot = stream_pack(ex, ey, w);
                 sc = nxt;
+                ++bi;
             }
-        }
-        if (rem) {
-            // the group's cells: first surviving (while none before it in the row), last surviving,
-            // last improving (gapped.rs:243-256)
-            const uint32_t done = rem < (uint32_t)U ? rem : (uint32_t)U;
-            if (!seen) first_b = amask ? bi0 + stream_low_bit(amask) : bi0 + done;
-            if (amask) {
-                seen = true;
-                last_b = bi0 + stream_high_bit(amask);
-            }
-            if (imask) best_b = bi0 + stream_high_bit(imask);
-            bi = bi0 + done;
         }
         if (!fetch && bi >= b_size) {
             // end of row (gapped.rs:298-334).  The band keeps [first_b, last_b] and, when the
@@ -254,7 +214,7 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
             if (best > prev_best) best_a = ai + 1;
             ++ai;
             const bool empty = first_b >= b_size;
-            const uint32_t vlo = last_b + 1;
+            vlo = last_b + 1;
             uint32_t k = 0;
             const int32_t num = gap_row - thr;  // <= xdrop (gap_row never exceeds best)
             if (vlo == b_size && b_size <= nb && num >= 0) {
@@ -283,12 +243,8 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                     origin += d; best = 0; thr -= d; gap_row -= d;
                 }
                 while (filled < b_size) fill_word();
-                // the extension cells: gap_row decaying by ge (gapped.rs:307-319)
-                for (uint32_t j = 0; j < k; ++j) {
-                    uint32_t& e = env.at(vlo + j);
-                    const int32_t v = gap_row - (int32_t)j * ge;
-                    e = stream_pack(v, max(v - goe, STREAM_FLOOR), e);
-                }
+                nvirt = k;
+                ext_val = gap_row;
                 {
                     // the sentinel; with nbs = nb + 1 (no sentinel) the store lands past the band,
                     // on a slot no live index shares (window <= STREAM_WINDOW), and is never read
@@ -363,24 +319,26 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                 const uint32_t jmax = div_ge((uint32_t)(xdrop - goe)) + 1u;
                 const uint32_t J = jmax < nb ? jmax : nb;
                 if (J + 1 > A.window) { dp_fail = true; continue; }
-                // initial row: cell 0 and the J gap cells -goe - (i - 1) * ge, written below
-                b_size = J + 1;
+                // initial row: cell 0 written, the J gap cells -goe - (i - 1) * ge computed on read
+                b_size = J + 1; vlo = 1; nvirt = J; ext_val = -goe;
                 first_b = 0; ai = 0; thr = -xdrop;
                 // residues of indices 0 .. filled - 1 come in below, with the warp's help: up to
                 // the next word boundary of the column sequence, so later whole-word fills start
                 // on one (at most 3 past b_size <= STREAM_WINDOW: inside the ring)
                 filled = b_size + (uint32_t)(dir > 0 ? -(pb + (int32_t)b_size) & 3 : (pb - (int32_t)b_size + 1) & 3);
                 init_pending = true;
-                init_j = J;
                 a_nx = dir < 0 ? a0_left : a0_right;
                 new_row();
                 fetch = false;
             }
         }
-        // the initial rows of the extensions started above: all lanes write the entries (residue,
-        // cell, gap) of the lanes that started one, one band index a lane at a time
-        env.fill_rows(init_pending, qal, pb, dir, filled, init_j, goe, ge);
-        init_pending = false;
+        // the initial rows of the extensions started above: all lanes copy residues into the
+        // rings of the lanes that started one, one band index a lane at a time
+        env.fill_rows(init_pending, qal, pb, dir, filled);
+        if (init_pending) {
+            env.at(0) = stream_pack(0, -goe, env.at(0));
+            init_pending = false;
+        }
     }
     return cells;
 }

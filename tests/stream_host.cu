@@ -25,11 +25,9 @@ struct HostEnv {
     uint32_t take() { return (*queue)++; }
     void overflow(uint32_t t) { overflow_list->push_back(t); }
     bool any(bool p) { return p; }
-    void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n, uint32_t J, int32_t goe,
-                   int32_t ge) {
+    void fill_rows(bool pending, const uint8_t* qal, int32_t pb, int32_t dir, uint32_t n) {
         if (pending)
-            for (uint32_t k = 0; k < n; ++k)
-                at(k) = rmb::stream_initial_entry(k, J, goe, ge, qal[pb + dir * (int32_t)k] & 15u);
+            for (uint32_t k = 0; k < n; ++k) at(k) = qal[pb + dir * (int32_t)k] & 15u;
     }
 };
 
