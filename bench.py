@@ -353,11 +353,24 @@ def main():
         cc = {k: sum(x[k] for x in ctrs) / len(ctrs) for k in ctrs[0]}
         return max_over_ranks(ev0.elapsed_time(ev1) / args.steps), cc
 
-    def arm_summary(cc: dict, ms: float) -> dict:
-        return {"value": timed_bases * world / (ms * 1e-3) / 1e6, "ms_per_step": ms, "prelim_ms": cc["gpu_ms_prelim"],
-                "gcups_computed": cc["so_cells"] / (cc["gpu_ms_prelim"] * 1e-3) / 1e9 if cc["gpu_ms_prelim"] else None,
-                "stage_ms": {k: round(cc[k], 3) for k in ("gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
-                                                          "gpu_ms_prelim", "gpu_ms_traceback")}}
+    def kernel_pass(s) -> dict:
+        """The timed steps again on one pipeline lane, untimed: each stage's device time alone (two
+        lanes' kernels overlap, so their event times include each other)."""
+        knobs = s.tune()
+        s.set_tune(dict(knobs, lanes=1))
+        rq = [s.upload(enc[b]) for b in timed]
+        kc = [s.search_resident(r).counters for r in rq]
+        for r in rq:
+            r.free()
+        s.set_tune(knobs)
+        return {key: sum(x[key] for x in kc) / len(kc) for key in kc[0]}
+
+    def arm_summary(ms: float, kc: dict) -> dict:
+        """An arm's throughput (its timed steps) and its stages' device times (one lane)."""
+        return {"value": timed_bases * world / (ms * 1e-3) / 1e6, "ms_per_step": ms, "prelim_ms": kc["gpu_ms_prelim"],
+                "gcups_computed": kc["so_cells"] / (kc["gpu_ms_prelim"] * 1e-3) / 1e9 if kc["gpu_ms_prelim"] else None,
+                "stage_ms": {key: round(kc[key], 3) for key in ("gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
+                                                              "gpu_ms_prelim", "gpu_ms_traceback")}}
 
     # ---- the measured arm: autotuned launch knobs (batched pipeline), resident, then end to end
     s = searcher(args.pipeline, args.schedule)
@@ -386,15 +399,18 @@ def main():
     text_b0 = s.search(enc[b0], ids[b0]).tabular(FIELDS)
 
     peak_int = api.int32_peak_tops(local)
-    prelim_ms = c["gpu_ms_prelim"]
-    so_cells = c["so_cells"]
-    # the dominant kernel: k_prelim_stream (one launch per step), timed alone with CUDA events
-    main_ms, main_cells = c["gpu_ms_prelim_main"], c["so_cells_main"]
+    # the kernels alone (one lane): the roofline, GCUPS and stage times come from these
+    knobs = s.tune() if args.pipeline == "batched" else {"lanes": 1}
+    k = kernel_pass(s) if args.pipeline == "batched" else c
+    prelim_ms = k["gpu_ms_prelim"]
+    so_cells = k["so_cells"]
+    # the dominant kernel: k_prelim_stream (one launch per sub-batch), timed alone with CUDA events
+    main_ms, main_cells = k["gpu_ms_prelim_main"], k["so_cells_main"]
     if main_ms <= 0:  # parameters outside the thread kernel's range: the warp kernel does it all
         main_ms, main_cells = prelim_ms, so_cells
     achieved = main_cells * OPS_PER_CELL / (main_ms * 1e-3) / 1e12 if main_ms > 0 else 0.0
-    traffic = (PRELIM_STREAM_DRAM_BYTES_PER_RECORD * c["prelim_dp"]
-               if PRELIM_STREAM_DRAM_BYTES_PER_RECORD and c["gpu_ms_prelim_main"] > 0 else None)
+    traffic = (PRELIM_STREAM_DRAM_BYTES_PER_RECORD * k["prelim_dp"]
+               if PRELIM_STREAM_DRAM_BYTES_PER_RECORD and k["gpu_ms_prelim_main"] > 0 else None)
     peaks, peak_source = {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
@@ -408,11 +424,17 @@ def main():
         # DP cells the GPU computed (gapped.rs:188 counting) per second of the stage; the reference-
         # counted figures (gcups_reference) follow from the oracle's cells on the CPU sample
         "gcups_computed": so_cells / (prelim_ms * 1e-3) / 1e9 if prelim_ms > 0 else None,
-        "traceback_gcups_computed": (c["tb_cells"] / (c["gpu_ms_traceback"] * 1e-3) / 1e9
-                                     if c["gpu_ms_traceback"] > 0 else None),
-        "scan_roofline": scan_roofline(sum(len(enc[b]) for b in timed) / args.steps, db, c, peaks),
-        "stage_ms": {k: round(c[k], 3) for k in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
-                                                  "gpu_ms_prelim", "gpu_ms_traceback", "ms_host_2a", "ms_host_2b")},
+        "traceback_gcups_computed": (k["tb_cells"] / (k["gpu_ms_traceback"] * 1e-3) / 1e9
+                                     if k["gpu_ms_traceback"] > 0 else None),
+        "scan_roofline": scan_roofline(sum(len(enc[b]) for b in timed) / args.steps, db, k, peaks),
+        # device time per stage on one lane (the kernels alone), and the lanes' sum in the timed run
+        "stage_ms": {key: round(k[key], 3) for key in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped",
+                                                      "gpu_ms_dedup", "gpu_ms_prelim", "gpu_ms_traceback",
+                                                      "ms_host_2a", "ms_host_2b")},
+        "lanes": knobs.get("lanes", 1),
+        # wall-clock per stage on the host (device work, syncs and host steps together)
+        "wall_ms": {k: round(c[k], 3) for k in ("ms_lookup", "ms_scan", "ms_ungapped", "ms_dedup", "ms_prelim_dp",
+                                                 "ms_host_2a", "ms_traceback", "ms_host_2b")},
         "counts": {k: int(c[k]) for k in ("word_hits", "ungapped", "prelim_dp", "prelims", "tb_dp", "finals",
                                           "so_cells", "tb_cells")},
         "roofline": {"kernel": "k_prelim_stream (score-only X-drop DP)", "bound": "int32", "achieved": achieved,
@@ -462,11 +484,11 @@ def main():
     s.close()
     # ---- the comparison arms on the same steps
     if compare:
-        me = arm_summary(c, ms_step)
+        me = arm_summary(ms_step, k)
         arms = {"measured": me}
         s = searcher("plain", "fifo")
         ms, cc = resident_arm(s)
-        arms["plain"] = arm_summary(cc, ms)
+        arms["plain"] = arm_summary(ms, cc)  # the plain pipeline runs one lane
         arms["plain"]["identical_output_first_step"] = s.search(enc[b0], ids[b0]).tabular(FIELDS) == text_b0
         s.close()
         line["vs_plain"] = {"value": me["value"] / arms["plain"]["value"],
@@ -478,7 +500,7 @@ def main():
             if tuned is not None:
                 s.set_tune(tuned["tune"])
             ms, cc = resident_arm(s)
-            arms["batched_fifo"] = arm_summary(cc, ms)
+            arms["batched_fifo"] = arm_summary(ms, kernel_pass(s))
             arms["batched_fifo"]["identical_output_first_step"] = s.search(enc[b0], ids[b0]).tabular(FIELDS) == text_b0
             s.close()
             line["learned_vs_fifo"] = {"value": me["value"] / arms["batched_fifo"]["value"],

@@ -75,10 +75,14 @@ typedef struct rmb_ctx rmb_ctx;
  *   ungapped_blocks_per_sm  blocks per SM of the persistent ungapped-extension grid, 1..8
  *   dedup_extend_hits_per_pair  pair ranges averaging at least this many word hits per
  *                           (query, subject) pair take the dedup kernel that extends only the
- *                           hits the diagonal hash admits; 0 = always, < 0 = never */
+ *                           hits the diagonal hash admits; 0 = always, < 0 = never
+ *   lanes                   1 or 2 pipeline lanes: with 2, a search's queries go in about four
+ *                           sub-batches to two streams with their own buffers and host threads,
+ *                           so one lane's host steps overlap the other's kernels (twice the
+ *                           per-batch device memory) */
 typedef struct rmb_tune {
     int32_t prelim_group, prelim_blocks_per_sm, prelim_window, prelim_budget_div;
-    int32_t ungapped_blocks_per_sm, dedup_extend_hits_per_pair;
+    int32_t ungapped_blocks_per_sm, dedup_extend_hits_per_pair, lanes;
 } rmb_tune;
 
 /* Learned schedule of the preliminary DP (no counterpart in the reference, whose records run in

@@ -147,6 +147,28 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
+// One pipeline lane: a stream and the device buffers of the sub-batch it is working on.  Two
+// lanes take alternate sub-batches, so one lane's host steps (Phase 2a/2b, the per-query end) run
+// while the other's kernels do, and the kernels of both fill each other's launch tails.
+struct Work {
+    cudaStream_t st = nullptr;
+    DBuf pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
+    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo,
+        n_wide, band, sel, surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over,
+        tb_ooff, tb_ops2, ung_queue;
+    DBuf sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
+    void release() {
+        DBuf* all[] = {&pv, &pv_off, &cs, &cs_off, &cq, &cq_off, &pos_off, &lut_keys, &lut_vals, &lut_keys2,
+                       &lut_vals2, &lut_counts, &counts, &offs, &hits, &hit_pair, &ub, &flags, &dd_scratch, &dd_cells,
+                       &ung_idx, &n_sel, &po, &wide, &wide2, &dres, &geo, &n_wide, &band, &sel, &surv, &cells, &fails,
+                       &temp, &tb_in, &tb_out, &tb_ops, &tb_scratch, &stage, &stage_start, &stage_over, &tb_ooff,
+                       &tb_ops2, &ung_queue, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
+        for (DBuf* b : all) b->release();
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+};
+
 // The hand-swept launch shape (B200, genome-vs-library workloads): the starting point of
 // rmb_autotune and the plain pipeline's fixed shape.
 static rmb_tune default_tune() {
@@ -157,6 +179,7 @@ static rmb_tune default_tune() {
     t.prelim_budget_div = 128;
     t.ungapped_blocks_per_sm = 8;
     t.dedup_extend_hits_per_pair = 256;
+    t.lanes = 2;
     return t;
 }
 
@@ -178,20 +201,19 @@ struct rmb_ctx {
     bool loaded = false;
     // library, device
     DBuf d_plus, d_rc, d_align, d_align_rc, d_packed, d_plus_off, d_packed_off, d_len, d_params;
-    // per-batch device buffers
-    DBuf lw, pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
+    // the query set's lookup widths (read by every lane)
+    DBuf lw;
     bool prelim_stream = false;  // thread-per-extension prelim kernel (else the warp kernel)
     rmb_tune tune = default_tune();  // launch knobs of the batched pipeline (rmb_tune_set / rmb_autotune)
     KaBlock ka;                  // E-value statistics (lambda <= 0: none)
-    DBuf dust_scratch;           // per-thread DUST interval lists
-    DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo, n_wide, band, sel,
-        surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over, tb_ooff, tb_ops2,
-        ung_queue;
+    DBuf dust_scratch, fails;    // per-thread DUST interval lists, their overflow flag
+    // the pipeline lanes: each a stream and the device buffers of one sub-batch at a time
+    Work work[2];
     DevLib L{};
     rmb_queries* batch = nullptr;  // the query set of rmb_search_batch, reused from call to call
     // learned schedule: the network's parameters (rmb_sched_set_model) and its per-batch buffers;
     // sched_log, while rmb_sched_log runs, collects (features, cells) of the FIFO run
-    DBuf sched_params, sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
+    DBuf sched_params;
     bool sched_ready = false;
     struct SchedLog {
         std::vector<float> feats;
@@ -276,7 +298,7 @@ struct PairPrelims {
     std::vector<Prelim> p;
 };
 
-bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
+bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
                   std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps);
 
@@ -294,6 +316,22 @@ void finish_query(const rmb_ctx& C, std::vector<Hit>& v, uint32_t qlen) {
         v.erase(std::remove_if(v.begin(), v.end(), [&](const Hit& h) { return h.evalue > P.evalue; }), v.end());
     apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
     sort_hit_list_order(v, C.ids);
+}
+
+// Counters of one lane added into another's (the device times of the two lanes add up: they
+// overlap in wall time).
+void add_counters(rmb_counters& a, const rmb_counters& b) {
+    a.word_hits += b.word_hits; a.seeds += b.seeds; a.ungapped += b.ungapped; a.prelim_dp += b.prelim_dp;
+    a.prelims += b.prelims; a.tb_dp += b.tb_dp; a.finals += b.finals; a.so_cells += b.so_cells;
+    a.tb_cells += b.tb_cells;
+    a.ms_lookup += b.ms_lookup; a.ms_scan += b.ms_scan; a.ms_ungapped += b.ms_ungapped; a.ms_dedup += b.ms_dedup;
+    a.ms_prelim_dp += b.ms_prelim_dp; a.ms_host_2a += b.ms_host_2a; a.ms_traceback += b.ms_traceback;
+    a.ms_host_2b += b.ms_host_2b;
+    a.gpu_ms_scan += b.gpu_ms_scan; a.gpu_ms_ungapped += b.gpu_ms_ungapped; a.gpu_ms_dedup += b.gpu_ms_dedup;
+    a.gpu_ms_prelim += b.gpu_ms_prelim; a.gpu_ms_traceback += b.gpu_ms_traceback; a.gpu_ms_lookup += b.gpu_ms_lookup;
+    a.launches += b.launches;
+    a.gpu_ms_prelim_main += b.gpu_ms_prelim_main; a.so_cells_main += b.so_cells_main;
+    a.gpu_ms_dust += b.gpu_ms_dust;
 }
 
 // The search of a set of single-chunk queries.  ucut_override: per-query ungapped cutoffs (the
@@ -321,18 +359,29 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
     if (P.dust && !QH.dusted && nq) mask_queries(C, QH, false, ctr);
     const uint8_t* qmask = P.dust ? QH.d_qm.as<uint8_t>() : QH.d_q.as<uint8_t>();
     const uint8_t* qmask_rc = P.dust ? QH.d_qmrc.as<uint8_t>() : QH.d_qrc.as<uint8_t>();
-    // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table size.
-    uint32_t qb = 0;
-    while (qb < nq) {
+    // Sub-batches of queries sharing one ungapped cutoff, bounded by lookup-table size; with two
+    // lanes, cut further so each lane gets about two.
+    const int lanes = (P.pipeline == 0 && !taps && !collect && !C.sched_log && C.tune.lanes > 1 && nq > 1) ? 2 : 1;
+    const uint32_t piece = lanes > 1 ? std::max<uint32_t>(1, (nq + 2 * lanes - 1) / (2 * lanes)) : nq;
+    std::vector<std::pair<uint32_t, uint32_t>> subs;
+    for (uint32_t qb = 0; qb < nq;) {
         uint64_t cells_b = 0, pos_b = 0;
         uint32_t qe = qb;
         while (qe < nq) {
             const uint64_t c = (1ull << (2 * lw_all[qe])) + 1, p2 = 2ull * qlen[qe] + 1;
-            if (qe > qb && (ucut[qe] != ucut[qb] || cells_b + c > (1ull << 30) || pos_b + p2 > (1ull << 30))) break;
+            if (qe > qb && (ucut[qe] != ucut[qb] || cells_b + c > (1ull << 30) || pos_b + p2 > (1ull << 30) ||
+                            qe - qb >= piece))
+                break;
             cells_b += c;
             pos_b += p2;
             ++qe;
         }
+        subs.emplace_back(qb, qe);
+        qb = qe;
+    }
+    CK(cudaStreamSynchronize(st));  // the lanes start after the query set's own work (upload, DUST)
+    auto sub_batch = [&](Work& W, uint32_t qb, uint32_t qe, rmb_counters& ctr) {
+        cudaStream_t st = W.st;
         const uint32_t nb = qe - qb;
         auto t0 = std::chrono::steady_clock::now();
         // ---- lookup tables of the sub-batch, built on the device
@@ -348,39 +397,39 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             ncs += (1ull << (2 * hlw[i])) + 1;
             npos += 2ull * hqlen[i] + 1;
         }
-        upload(C.pv_off, hpvoff, st);
-        upload(C.cs_off, hcsoff, st);
-        upload(C.cq_off, hzero, st);
-        upload(C.pos_off, hposoff, st);
-        C.pv.ensure(npv * 4);
-        C.cs.ensure((ncs + 1) * 4);
-        C.lut_counts.ensure((ncs + 1) * 4);
-        C.cq.ensure(npos * 4);
-        C.lut_keys.ensure(npos * 4);
-        C.lut_vals.ensure(npos * 4);
-        C.lut_keys2.ensure(npos * 4);
-        C.lut_vals2.ensure(npos * 4);
+        upload(W.pv_off, hpvoff, st);
+        upload(W.cs_off, hcsoff, st);
+        upload(W.cq_off, hzero, st);
+        upload(W.pos_off, hposoff, st);
+        W.pv.ensure(npv * 4);
+        W.cs.ensure((ncs + 1) * 4);
+        W.lut_counts.ensure((ncs + 1) * 4);
+        W.cq.ensure(npos * 4);
+        W.lut_keys.ensure(npos * 4);
+        W.lut_vals.ensure(npos * 4);
+        W.lut_keys2.ensure(npos * 4);
+        W.lut_vals2.ensure(npos * 4);
         DevQueries Q{QH.d_q.as<uint8_t>(),       QH.d_qrc.as<uint8_t>(),  qmask, qmask_rc,
-                     QH.d_off.as<uint64_t>() + qb, QH.d_len.as<uint32_t>() + qb, C.pv.as<uint32_t>(),
-                     C.pv_off.as<uint64_t>(),    C.cs.as<uint32_t>(),     C.cs_off.as<uint64_t>(),
-                     C.cq.as<uint32_t>(),        C.cq_off.as<uint64_t>(), C.lw.as<int32_t>() + qb, nb};
+                     QH.d_off.as<uint64_t>() + qb, QH.d_len.as<uint32_t>() + qb, W.pv.as<uint32_t>(),
+                     W.pv_off.as<uint64_t>(),    W.cs.as<uint32_t>(),     W.cs_off.as<uint64_t>(),
+                     W.cq.as<uint32_t>(),        W.cq_off.as<uint64_t>(), C.lw.as<int32_t>() + qb, nb};
         EvTimer ev;
         ev.start(st);
         {
-            size_t tb = C.temp.cap;
+            size_t tb = W.temp.cap;
             uint64_t nvalid = 0;
-            cudaError_t e = launch_lut_build(Q, P.word_size, nb, C.pos_off.as<uint64_t>(), npos, ncs, npv,
-                                             C.lut_keys.as<uint32_t>(), C.lut_vals.as<uint32_t>(),
-                                             C.lut_keys2.as<uint32_t>(), C.lut_vals2.as<uint32_t>(),
-                                             C.lut_counts.as<uint32_t>(), C.cs.as<uint32_t>(), C.cq.as<uint32_t>(),
-                                             C.pv.as<uint32_t>(), C.temp.p, tb, nvalid, st);
+            cudaError_t e = launch_lut_build(Q, P.word_size, nb, W.pos_off.as<uint64_t>(), npos, ncs, npv,
+                                             W.lut_keys.as<uint32_t>(), W.lut_vals.as<uint32_t>(),
+                                             W.lut_keys2.as<uint32_t>(), W.lut_vals2.as<uint32_t>(),
+                                             W.lut_counts.as<uint32_t>(), W.cs.as<uint32_t>(), W.cq.as<uint32_t>(),
+                                             W.pv.as<uint32_t>(), W.temp.p, tb, nvalid, st);
             if (e == cudaErrorNotReady) {
-                C.temp.ensure(tb);
-                tb = C.temp.cap;
-                e = launch_lut_build(Q, P.word_size, nb, C.pos_off.as<uint64_t>(), npos, ncs, npv,
-                                     C.lut_keys.as<uint32_t>(), C.lut_vals.as<uint32_t>(), C.lut_keys2.as<uint32_t>(),
-                                     C.lut_vals2.as<uint32_t>(), C.lut_counts.as<uint32_t>(), C.cs.as<uint32_t>(),
-                                     C.cq.as<uint32_t>(), C.pv.as<uint32_t>(), C.temp.p, tb, nvalid, st);
+                W.temp.ensure(tb);
+                tb = W.temp.cap;
+                e = launch_lut_build(Q, P.word_size, nb, W.pos_off.as<uint64_t>(), npos, ncs, npv,
+                                     W.lut_keys.as<uint32_t>(), W.lut_vals.as<uint32_t>(), W.lut_keys2.as<uint32_t>(),
+                                     W.lut_vals2.as<uint32_t>(), W.lut_counts.as<uint32_t>(), W.cs.as<uint32_t>(),
+                                     W.cq.as<uint32_t>(), W.pv.as<uint32_t>(), W.temp.p, tb, nvalid, st);
             }
             CK(e);
         }
@@ -390,9 +439,9 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         ctr.launches += 3;  // codes, place, pv
         if (taps && taps->lookup) {
             std::vector<uint32_t> hcs(ncs + 1), hcq(npos), hpv(npv);
-            CK(cudaMemcpy(hcs.data(), C.cs.p, (ncs + 1) * 4, cudaMemcpyDeviceToHost));
-            CK(cudaMemcpy(hcq.data(), C.cq.p, npos * 4, cudaMemcpyDeviceToHost));
-            CK(cudaMemcpy(hpv.data(), C.pv.p, npv * 4, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(hcs.data(), W.cs.p, (ncs + 1) * 4, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(hcq.data(), W.cq.p, npos * 4, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(hpv.data(), W.pv.p, npv * 4, cudaMemcpyDeviceToHost));
             for (uint32_t i = 0; i < nb; ++i) {
                 const uint64_t cells = 1ull << (2 * hlw[i]);
                 for (uint64_t c = 0; c < cells; ++c) {
@@ -402,8 +451,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                     for (uint32_t j = b; j < e; ++j) taps->lookup->insert(taps->lookup->end(), {qb + i, (uint32_t)c, hcq[j]});
                 }
             }
-            qb = qe;
-            continue;
+            return;
         }
         ctr.ms_lookup += ms_since(t0);
         auto qhost = [&](uint32_t local) { return QH.host.data() + QH.off[qb + local]; };
@@ -412,25 +460,25 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         // pair order (pair ids are local to the sub-batch)
         t0 = std::chrono::steady_clock::now();
         const uint64_t npairs = (uint64_t)nb * ns;
-        C.counts.ensure((npairs + 1) * 4);
-        C.offs.ensure((npairs + 1) * 8);
-        C.stage_start.ensure(npairs * 4);
-        C.stage.ensure(scan_stage_entries(npairs, C.sms) * sizeof(SeedHit));
-        C.stage_over.ensure(4);
-        CK(cudaMemsetAsync(C.counts.p, 0, (npairs + 1) * 4, st));
-        CK(cudaMemsetAsync(C.stage_over.p, 0, 4, st));
+        W.counts.ensure((npairs + 1) * 4);
+        W.offs.ensure((npairs + 1) * 8);
+        W.stage_start.ensure(npairs * 4);
+        W.stage.ensure(scan_stage_entries(npairs, C.sms) * sizeof(SeedHit));
+        W.stage_over.ensure(4);
+        CK(cudaMemsetAsync(W.counts.p, 0, (npairs + 1) * 4, st));
+        CK(cudaMemsetAsync(W.stage_over.p, 0, 4, st));
         ev.start(st);
-        CK(launch_scan_stage(C.L, Q, P.word_size, npairs, C.counts.as<uint32_t>(), C.stage_start.as<uint32_t>(),
-                             C.stage.as<SeedHit>(), C.stage_over.as<unsigned int>(), C.sms, st));
+        CK(launch_scan_stage(C.L, Q, P.word_size, npairs, W.counts.as<uint32_t>(), W.stage_start.as<uint32_t>(),
+                             W.stage.as<SeedHit>(), W.stage_over.as<unsigned int>(), C.sms, st));
         size_t tb = 0;
-        CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), nullptr, tb, st));
-        C.temp.ensure(tb);
-        CK(launch_offsets(C.counts.as<uint32_t>(), npairs + 1, C.offs.as<uint64_t>(), C.temp.p, tb, st));
+        CK(launch_offsets(W.counts.as<uint32_t>(), npairs + 1, W.offs.as<uint64_t>(), nullptr, tb, st));
+        W.temp.ensure(tb);
+        CK(launch_offsets(W.counts.as<uint32_t>(), npairs + 1, W.offs.as<uint64_t>(), W.temp.p, tb, st));
         ev.stop(st);
         uint64_t nh = 0;
         unsigned int stage_over = 0;
-        CK(cudaMemcpyAsync(&nh, C.offs.as<uint64_t>() + npairs, 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&stage_over, C.stage_over.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&nh, W.offs.as<uint64_t>() + npairs, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&stage_over, W.stage_over.p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctr.gpu_ms_scan += ev.ms();
         ctr.word_hits += nh;
@@ -443,7 +491,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         if (nh > MAX_RANGE_HITS) {
             if (taps) throw Fail(RMB_ELIMIT, "stage taps take batches of at most 2^29 word hits");
             hoffs.resize(npairs + 1);
-            CK(cudaMemcpy(hoffs.data(), C.offs.p, (npairs + 1) * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(hoffs.data(), W.offs.p, (npairs + 1) * 8, cudaMemcpyDeviceToHost));
             ranges.assign(1, 0);
             for (uint64_t pr = 0; pr < npairs; ++pr)
                 if (hoffs[pr + 1] - hoffs[ranges.back()] > MAX_RANGE_HITS && pr > ranges.back()) ranges.push_back(pr);
@@ -458,22 +506,22 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             if (nh >= 0xffffffffull) throw Fail(RMB_ELIMIT, "more than 2^32 word hits in one pair range");
             if (ranges.size() > 2) {  // offsets local to the range
                 tb = 0;
-                CK(launch_offsets(C.counts.as<uint32_t>() + pair0, npairs + 1, C.offs.as<uint64_t>(), nullptr, tb,
+                CK(launch_offsets(W.counts.as<uint32_t>() + pair0, npairs + 1, W.offs.as<uint64_t>(), nullptr, tb,
                                   st));
-                C.temp.ensure(tb);
-                CK(launch_offsets(C.counts.as<uint32_t>() + pair0, npairs + 1, C.offs.as<uint64_t>(), C.temp.p, tb,
+                W.temp.ensure(tb);
+                CK(launch_offsets(W.counts.as<uint32_t>() + pair0, npairs + 1, W.offs.as<uint64_t>(), W.temp.p, tb,
                                   st));
             }
-            C.hits.ensure(nh * sizeof(SeedHit));
-            C.hit_pair.ensure(nh * 4);
+            W.hits.ensure(nh * sizeof(SeedHit));
+            W.hit_pair.ensure(nh * 4);
             ev.start(st);
             if (!stage_over)
-                CK(launch_scan_gather(pair0, npairs, C.counts.as<uint32_t>(), C.offs.as<uint64_t>(),
-                                      C.stage_start.as<uint32_t>(), C.stage.as<SeedHit>(), C.hits.as<SeedHit>(),
-                                      C.hit_pair.as<uint32_t>(), C.sms, st));
+                CK(launch_scan_gather(pair0, npairs, W.counts.as<uint32_t>(), W.offs.as<uint64_t>(),
+                                      W.stage_start.as<uint32_t>(), W.stage.as<SeedHit>(), W.hits.as<SeedHit>(),
+                                      W.hit_pair.as<uint32_t>(), C.sms, st));
             else  // a warp's stretch of the stage ran out: scan this range again, writing in place
-                CK(launch_scan(true, C.L, Q, P.word_size, pair0, npairs, nullptr, C.offs.as<uint64_t>(),
-                               C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.sms, st));
+                CK(launch_scan(true, C.L, Q, P.word_size, pair0, npairs, nullptr, W.offs.as<uint64_t>(),
+                               W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), C.sms, st));
             ev.stop(st);
             CK(cudaStreamSynchronize(st));
             ctr.gpu_ms_scan += ev.ms();
@@ -483,26 +531,26 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             // ---- ungapped extension of every hit, then the per-pair dedup; or, for hit-dense
             // pairs (most hits dropped by the hash), the dedup extending only what it admits
             t0 = std::chrono::steady_clock::now();
-            C.ub.ensure(nh * sizeof(UngBox));
+            W.ub.ensure(nh * sizeof(UngBox));
             const int32_t dx = C.tune.dedup_extend_hits_per_pair;
             const bool fused = P.pipeline != 1 && dx >= 0 && nh >= (uint64_t)dx * npairs;
             if (fused) {
-                C.flags.ensure(nh + 1);
-                C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
-                C.ung_queue.ensure(16);
+                W.flags.ensure(nh + 1);
+                W.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+                W.ung_queue.ensure(16);
                 ev.start(st);
                 CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], pair0, npairs,
-                                       C.offs.as<uint64_t>(), C.hits.as<SeedHit>(), C.ub.as<UngBox>(),
-                                       C.flags.as<uint8_t>(), C.dd_cells.p, C.ung_queue.as<unsigned long long>(),
+                                       W.offs.as<uint64_t>(), W.hits.as<SeedHit>(), W.ub.as<UngBox>(),
+                                       W.flags.as<uint8_t>(), W.dd_cells.p, W.ung_queue.as<unsigned long long>(),
                                        C.sms, st));
                 ev.stop(st);
                 ctr.launches += 1;
             } else {
                 ev.start(st);
-                C.ung_queue.ensure(16);
-                CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, C.hits.as<SeedHit>(),
-                                   C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.sms, st,
-                                   P.pipeline == 1 ? nullptr : C.ung_queue.as<unsigned long long>(),
+                W.ung_queue.ensure(16);
+                CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], nh, W.hits.as<SeedHit>(),
+                                   W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), C.sms, st,
+                                   P.pipeline == 1 ? nullptr : W.ung_queue.as<unsigned long long>(),
                                    C.tune.ungapped_blocks_per_sm));
                 ev.stop(st);
                 CK(cudaStreamSynchronize(st));
@@ -510,25 +558,25 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 ctr.launches += nh ? 1 : 0;
                 ctr.ms_ungapped += ms_since(t0);
                 t0 = std::chrono::steady_clock::now();
-                C.flags.ensure(nh + 1);
-                C.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
-                C.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
+                W.flags.ensure(nh + 1);
+                W.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
+                W.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
                 ev.start(st);
-                CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], pair0, npairs, C.offs.as<uint64_t>(), C.hits.as<SeedHit>(),
-                                C.ub.as<UngBox>(), C.flags.as<uint8_t>(), C.dd_scratch.as<uint32_t>(), C.dd_cells.p, C.sms, st));
+                CK(launch_dedup(C.L, Q, P.word_size, ucut[qb], pair0, npairs, W.offs.as<uint64_t>(), W.hits.as<SeedHit>(),
+                                W.ub.as<UngBox>(), W.flags.as<uint8_t>(), W.dd_scratch.as<uint32_t>(), W.dd_cells.p, C.sms, st));
                 ev.stop(st);
                 ctr.launches += 1;
             }
-            C.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
-            C.n_sel.ensure(16);
+            W.ung_idx.ensure(std::max<uint64_t>(nh, 1) * 4);
+            W.n_sel.ensure(16);
             tb = 0;
-            CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb,
+            CK(launch_select_eq(W.flags.as<uint8_t>(), nh, 3, W.ung_idx.as<uint32_t>(), W.n_sel.as<uint32_t>(), nullptr, tb,
                                 st));
-            C.temp.ensure(tb);
-            CK(launch_select_eq(C.flags.as<uint8_t>(), nh, 3, C.ung_idx.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p,
+            W.temp.ensure(tb);
+            CK(launch_select_eq(W.flags.as<uint8_t>(), nh, 3, W.ung_idx.as<uint32_t>(), W.n_sel.as<uint32_t>(), W.temp.p,
                                 tb, st));
             uint32_t nu = 0;
-            CK(cudaMemcpyAsync(&nu, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&nu, W.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             ctr.gpu_ms_dedup += ev.ms();
             ctr.ms_dedup += ms_since(t0);
@@ -539,10 +587,10 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 std::vector<uint8_t> fl(nh);
                 std::vector<UngBox> uu(nh);
                 if (nh) {
-                    CK(cudaMemcpy(hh.data(), C.hits.p, nh * sizeof(SeedHit), cudaMemcpyDeviceToHost));
-                    CK(cudaMemcpy(hp.data(), C.hit_pair.p, nh * 4, cudaMemcpyDeviceToHost));
-                    CK(cudaMemcpy(fl.data(), C.flags.p, nh, cudaMemcpyDeviceToHost));
-                    CK(cudaMemcpy(uu.data(), C.ub.p, nh * sizeof(UngBox), cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(hh.data(), W.hits.p, nh * sizeof(SeedHit), cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(hp.data(), W.hit_pair.p, nh * 4, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(fl.data(), W.flags.p, nh, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(uu.data(), W.ub.p, nh * sizeof(UngBox), cudaMemcpyDeviceToHost));
                 }
                 for (uint64_t i = 0; i < nh; ++i) {
                     if (!fl[i]) continue;
@@ -608,44 +656,44 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
 
             // ---- preliminary gapped DP of every ungapped record
             t0 = std::chrono::steady_clock::now();
-            C.po.ensure(std::max<uint64_t>(nu, 1) * sizeof(PrelimOut));
-            C.wide.ensure(std::max<uint64_t>(nu, 1) * 4);
-            C.n_wide.ensure(16);
-            C.cells.ensure(16);
-            C.fails.ensure(16);
-            CK(cudaMemsetAsync(C.n_wide.p, 0, 16, st));
-            CK(cudaMemsetAsync(C.cells.p, 0, 16, st));
-            CK(cudaMemsetAsync(C.fails.p, 0, 16, st));
+            W.po.ensure(std::max<uint64_t>(nu, 1) * sizeof(PrelimOut));
+            W.wide.ensure(std::max<uint64_t>(nu, 1) * 4);
+            W.n_wide.ensure(16);
+            W.cells.ensure(16);
+            W.fails.ensure(16);
+            CK(cudaMemsetAsync(W.n_wide.p, 0, 16, st));
+            CK(cudaMemsetAsync(W.cells.p, 0, 16, st));
+            CK(cudaMemsetAsync(W.fails.p, 0, 16, st));
             ev.start(st);
             EvTimer ev_main;
             if (C.prelim_stream) {
-                C.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
-                CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
-                                      C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.geo.p, C.sms,
+                W.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
+                CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), nu, W.ung_idx.as<uint32_t>(),
+                                      W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.geo.p, C.sms,
                                       st));
                 ctr.launches += nu ? 1 : 0;
                 const uint32_t* order = nullptr;
                 uint32_t* cells_out = nullptr;
                 if (C.sched_log && nu) {
                     // training pairs: each record's features, and its cells from the DP below
-                    C.sched_feat.ensure(nu * SCHED_NF_HOST * 4);
-                    C.sched_cells.ensure(nu * 4);
-                    CK(launch_sched_features(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
-                                             C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
-                                             C.counts.as<uint32_t>(), C.sched_feat.as<float>(), C.sms, st));
-                    cells_out = C.sched_cells.as<uint32_t>();
+                    W.sched_feat.ensure(nu * SCHED_NF_HOST * 4);
+                    W.sched_cells.ensure(nu * 4);
+                    CK(launch_sched_features(C.L, Q, C.d_params.as<DevParams>(), nu, W.ung_idx.as<uint32_t>(),
+                                             W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
+                                             W.counts.as<uint32_t>(), W.sched_feat.as<float>(), C.sms, st));
+                    cells_out = W.sched_cells.as<uint32_t>();
                     ctr.launches += 1;
                 } else if (C.p.schedule == 1 && nu) {
                     // the records in descending predicted cost
-                    C.sched_pred.ensure(nu * 4);
-                    C.sched_order.ensure(nu * 4);
-                    C.sched_scratch.ensure(sched_order_scratch_bytes());
-                    CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), nu, C.ung_idx.as<uint32_t>(),
-                                          C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
-                                          C.counts.as<uint32_t>(), C.sched_params.as<float>(),
-                                          C.sched_pred.as<float>(), C.sched_scratch.p, C.sched_order.as<uint32_t>(),
+                    W.sched_pred.ensure(nu * 4);
+                    W.sched_order.ensure(nu * 4);
+                    W.sched_scratch.ensure(sched_order_scratch_bytes());
+                    CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), nu, W.ung_idx.as<uint32_t>(),
+                                          W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
+                                          W.counts.as<uint32_t>(), C.sched_params.as<float>(),
+                                          W.sched_pred.as<float>(), W.sched_scratch.p, W.sched_order.as<uint32_t>(),
                                           C.sms, st));
-                    order = C.sched_order.as<uint32_t>();
+                    order = W.sched_order.as<uint32_t>();
                     ctr.launches += 3;
                 }
                 ev_main.start(st);
@@ -656,16 +704,16 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 cfg.blocks_per_sm = tn.prelim_blocks_per_sm;
                 cfg.window = tn.prelim_window;
                 cfg.budget_div = tn.prelim_budget_div;
-                CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, C.geo.p, C.po.as<PrelimOut>(),
-                                        C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(),
-                                        C.cells.as<unsigned long long>(), C.sms, st, order, cells_out,
+                CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, W.geo.p, W.po.as<PrelimOut>(),
+                                        W.wide.as<uint32_t>(), W.n_wide.as<unsigned int>(),
+                                        W.cells.as<unsigned long long>(), C.sms, st, order, cells_out,
                                         P.pipeline == 1, cfg));
                 ev_main.stop(st);
                 if (cells_out) {
                     std::vector<float> f(nu * SCHED_NF_HOST);
                     std::vector<uint32_t> c(nu);
-                    CK(cudaMemcpyAsync(f.data(), C.sched_feat.p, f.size() * 4, cudaMemcpyDeviceToHost, st));
-                    CK(cudaMemcpyAsync(c.data(), C.sched_cells.p, c.size() * 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(f.data(), W.sched_feat.p, f.size() * 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(c.data(), W.sched_cells.p, c.size() * 4, cudaMemcpyDeviceToHost, st));
                     CK(cudaStreamSynchronize(st));
                     for (uint64_t r = 0; r < nu; ++r) {
                         if (c[r] == 0xFFFFFFFFu) continue;  // passed on to the warp kernel
@@ -676,81 +724,81 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 }
             }
             else
-                CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, C.ung_idx.as<uint32_t>(),
-                                 C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
-                                 C.wide.as<uint32_t>(), C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(),
+                CK(launch_prelim(C.L, Q, C.d_params.as<DevParams>(), nu, nullptr, W.ung_idx.as<uint32_t>(),
+                                 W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.po.as<PrelimOut>(),
+                                 W.wide.as<uint32_t>(), W.n_wide.as<unsigned int>(), W.cells.as<unsigned long long>(),
                                  C.sms, st));
             ev.stop(st);
             ctr.launches += nu ? 1 : 0;
             uint32_t nw = 0;
             unsigned long long main_cells = 0;
-            CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(&main_cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&nw, W.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&main_cells, W.cells.p, 8, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             ctr.gpu_ms_prelim += ev.ms();
             if (C.prelim_stream) {
                 ctr.gpu_ms_prelim_main += ev_main.ms();
                 ctr.so_cells_main += main_cells;
             }
-            DBuf* wide_list = &C.wide;
+            DBuf* wide_list = &W.wide;
             if (nw && C.prelim_stream) {
                 // records whose band window outgrew the thread ring: the warp kernel's 256-cell rings
-                C.wide2.ensure((uint64_t)nw * 4);
-                C.dres.ensure((uint64_t)nw * 2 * sizeof(int4));
-                CK(cudaMemsetAsync(C.n_wide.p, 0, 4, st));
+                W.wide2.ensure((uint64_t)nw * 4);
+                W.dres.ensure((uint64_t)nw * 2 * sizeof(int4));
+                CK(cudaMemsetAsync(W.n_wide.p, 0, 4, st));
                 EvTimer e2;
                 e2.start(st);
-                CK(launch_prelim_split(C.L, Q, C.d_params.as<DevParams>(), nw, C.wide.as<uint32_t>(),
-                                       C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(),
-                                       C.ub.as<UngBox>(), C.dres.as<int4>(), C.po.as<PrelimOut>(), C.wide2.as<uint32_t>(),
-                                       C.n_wide.as<unsigned int>(), C.cells.as<unsigned long long>(), C.sms, st));
+                CK(launch_prelim_split(C.L, Q, C.d_params.as<DevParams>(), nw, W.wide.as<uint32_t>(),
+                                       W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(),
+                                       W.ub.as<UngBox>(), W.dres.as<int4>(), W.po.as<PrelimOut>(), W.wide2.as<uint32_t>(),
+                                       W.n_wide.as<unsigned int>(), W.cells.as<unsigned long long>(), C.sms, st));
                 e2.stop(st);
                 ctr.launches += 2;
-                CK(cudaMemcpyAsync(&nw, C.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&nw, W.n_wide.p, 4, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 ctr.gpu_ms_prelim += e2.ms();
-                wide_list = &C.wide2;
+                wide_list = &W.wide2;
             }
             if (nw) {
                 uint32_t qmax = 0;
                 for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
                 const uint64_t cap = (uint64_t)std::max(qmax, C.max_slen) + 2;
                 const uint32_t threads = std::min<uint32_t>(nw, (uint32_t)std::max<uint64_t>(128, (1ull << 31) / (cap * 8)));
-                C.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
+                W.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
                 EvTimer ew;
                 ew.start(st);
                 ctr.launches += 1;
-                CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, wide_list->as<uint32_t>(), C.ung_idx.as<uint32_t>(),
-                                      C.hits.as<SeedHit>(), C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(),
-                                      C.po.as<PrelimOut>(), C.band.as<int2>(), cap, threads,
-                                      C.cells.as<unsigned long long>(), C.fails.as<unsigned int>(), st));
+                CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw, wide_list->as<uint32_t>(), W.ung_idx.as<uint32_t>(),
+                                      W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
+                                      W.po.as<PrelimOut>(), W.band.as<int2>(), cap, threads,
+                                      W.cells.as<unsigned long long>(), W.fails.as<unsigned int>(), st));
                 ew.stop(st);
                 ctr.gpu_ms_prelim += ew.ms();
             }
             unsigned long long cells = 0;
             unsigned int fails = 0;
-            CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(&fails, C.fails.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&cells, W.cells.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&fails, W.fails.p, 4, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (fails) throw Fail(RMB_ECUDA, "prelim DP band exceeded its storage");
             ctr.so_cells += cells;
             ctr.prelim_dp += nu;
             // survivors (score >= gapped cutoff) to the host
-            C.sel.ensure(std::max<uint64_t>(nu, 1) * 4);
+            W.sel.ensure(std::max<uint64_t>(nu, 1) * 4);
             tb = 0;
-            CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), nullptr, tb, st));
-            C.temp.ensure(tb);
-            CK(launch_select_prelim(C.po.as<PrelimOut>(), nu, C.sel.as<uint32_t>(), C.n_sel.as<uint32_t>(), C.temp.p, tb, st));
+            CK(launch_select_prelim(W.po.as<PrelimOut>(), nu, W.sel.as<uint32_t>(), W.n_sel.as<uint32_t>(), nullptr, tb, st));
+            W.temp.ensure(tb);
+            CK(launch_select_prelim(W.po.as<PrelimOut>(), nu, W.sel.as<uint32_t>(), W.n_sel.as<uint32_t>(), W.temp.p, tb, st));
             uint32_t nsv = 0;
-            CK(cudaMemcpyAsync(&nsv, C.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&nsv, W.n_sel.p, 4, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
-            C.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
+            W.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
             ctr.launches += nsv ? 1 : 0;
-            CK(launch_gather_survivors(nsv, C.sel.as<uint32_t>(), C.ung_idx.as<uint32_t>(), C.hits.as<SeedHit>(),
-                                       C.hit_pair.as<uint32_t>(), C.ub.as<UngBox>(), C.po.as<PrelimOut>(),
-                                       C.surv.as<SurvivorRec>(), st));
+            CK(launch_gather_survivors(nsv, W.sel.as<uint32_t>(), W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(),
+                                       W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.po.as<PrelimOut>(),
+                                       W.surv.as<SurvivorRec>(), st));
             std::vector<SurvivorRec> sv(nsv);
-            if (nsv) CK(cudaMemcpyAsync(sv.data(), C.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
+            if (nsv) CK(cudaMemcpyAsync(sv.data(), W.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             ctr.ms_prelim_dp += ms_since(t0);
 
@@ -810,33 +858,54 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             }
 
             // ---- traceback DP and host Phase 2b of every prelim
-            if (traceback_2b(C, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps)) {
+            if (traceback_2b(C, W, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps)) {
                 tapped = true;
                 continue;
             }
         }
-        if (tapped || collect) {
-            qb = qe;
-            continue;
-        }
+        if (tapped || collect) return;
         t0 = std::chrono::steady_clock::now();
         parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
         for (uint32_t i = 0; i < nb; ++i) ctr.finals += out_hits[qb + i].size();
         ctr.ms_host_2b += ms_since(t0);
-        qb = qe;
+    };
+    if (lanes == 1) {
+        for (auto& sb : subs) sub_batch(C.work[0], sb.first, sb.second, ctr);
+        return;
     }
+    // lane k takes sub-batches k, k + 2, ... in order; lane 1 on a host thread of its own
+    rmb_counters c1{};
+    std::exception_ptr err1;
+    std::thread t1([&]() {
+        try {
+            CK(cudaSetDevice(C.p.device));
+            for (size_t i = 1; i < subs.size(); i += 2) sub_batch(C.work[1], subs[i].first, subs[i].second, c1);
+        } catch (...) {
+            err1 = std::current_exception();
+        }
+    });
+    std::exception_ptr err0;
+    try {
+        for (size_t i = 0; i < subs.size(); i += 2) sub_batch(C.work[0], subs[i].first, subs[i].second, ctr);
+    } catch (...) {
+        err0 = std::current_exception();
+    }
+    t1.join();
+    if (err0) std::rethrow_exception(err0);
+    if (err1) std::rethrow_exception(err1);
+    add_counters(ctr, c1);
 }
 
 // Traceback DP on the device and the host Phase 2b (engine.rs:1438-1762) of the prelims of
 // (query, subject) pairs; pair = local query * n_subjects + subject over the queries of Q, whose
 // lengths are hqlen and host copies qhost(local).  Hits go to out[local query].  Returns true
 // when the traceback stage tap took the results instead.
-bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
+bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
                   std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps) {
     const uint32_t ns = (uint32_t)C.ids.size();
     const size_t np = pair_ids.size();
-    cudaStream_t st = C.st;
+    cudaStream_t st = W.st;
     unsigned long long cells = 0;
     auto t0 = std::chrono::steady_clock::now();
     {
@@ -879,21 +948,21 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
                 // one warp per scratch slot, blocks of 8 warps
                 uint32_t threads = (uint32_t)std::min<uint64_t>(todo.size(), std::max<uint64_t>(8, budget / per_thread));
                 threads = (threads + 7) / 8 * 8;
-                upload(C.tb_in, chunk_in, st);
-                C.tb_out.ensure(todo.size() * sizeof(TbOut));
-                C.tb_ops.ensure(todo.size() * (uint64_t)ops_cap * 4);
-                C.tb_scratch.ensure((uint64_t)threads * per_thread);
-                CK(cudaMemsetAsync(C.cells.p, 0, 8, st));
+                upload(W.tb_in, chunk_in, st);
+                W.tb_out.ensure(todo.size() * sizeof(TbOut));
+                W.tb_ops.ensure(todo.size() * (uint64_t)ops_cap * 4);
+                W.tb_scratch.ensure((uint64_t)threads * per_thread);
+                CK(cudaMemsetAsync(W.cells.p, 0, 8, st));
                 EvTimer et;
                 et.start(st);
                 ctr.launches += 1;
-                CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), C.tb_in.as<TbIn>(),
-                                    C.tb_out.as<TbOut>(), C.tb_ops.as<uint32_t>(), ops_cap, C.tb_scratch.as<uint8_t>(),
-                                    per_thread, band_cells, rows_cap, threads, C.cells.as<unsigned long long>(), st));
+                CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), W.tb_in.as<TbIn>(),
+                                    W.tb_out.as<TbOut>(), W.tb_ops.as<uint32_t>(), ops_cap, W.tb_scratch.as<uint8_t>(),
+                                    per_thread, band_cells, rows_cap, threads, W.cells.as<unsigned long long>(), st));
                 et.stop(st);
                 std::vector<TbOut> to(todo.size());
-                CK(cudaMemcpyAsync(to.data(), C.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(&cells, C.cells.p, 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(to.data(), W.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&cells, W.cells.p, 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 ctr.gpu_ms_traceback += et.ms();
                 // only the ops of the finished items come back, packed
@@ -902,11 +971,11 @@ bool traceback_2b(rmb_ctx& C, const DevQueries& Q, const uint32_t* hqlen, uint32
                     ooff[i + 1] = ooff[i] + (to[i].status == 2 ? 0 : to[i].n_ops);
                 std::vector<uint32_t> ops(ooff.back());
                 if (!ops.empty()) {
-                    upload(C.tb_ooff, ooff, st);
-                    C.tb_ops2.ensure(ops.size() * 4);
-                    CK(launch_gather_ops((uint32_t)todo.size(), C.tb_ops.as<uint32_t>(), ops_cap, C.tb_out.as<TbOut>(),
-                                         C.tb_ooff.as<uint64_t>(), C.tb_ops2.as<uint32_t>(), C.sms, st));
-                    CK(cudaMemcpyAsync(ops.data(), C.tb_ops2.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
+                    upload(W.tb_ooff, ooff, st);
+                    W.tb_ops2.ensure(ops.size() * 4);
+                    CK(launch_gather_ops((uint32_t)todo.size(), W.tb_ops.as<uint32_t>(), ops_cap, W.tb_out.as<TbOut>(),
+                                         W.tb_ooff.as<uint64_t>(), W.tb_ops2.as<uint32_t>(), C.sms, st));
+                    CK(cudaMemcpyAsync(ops.data(), W.tb_ops2.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
                     CK(cudaStreamSynchronize(st));
                     ctr.launches += 1;
                 }
@@ -1045,6 +1114,7 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         if (prop.major < 10) throw Fail(RMB_EINVAL, "this library is built for sm_100a (B200)");
         C->sms = prop.multiProcessorCount;
         CK(cudaStreamCreateWithFlags(&C->st, cudaStreamNonBlocking));
+        for (Work& w : C->work) CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking));
         DevParams dp{};
         dp.gap_open = p.gap_open;
         dp.gap_extend = p.gap_extend;
@@ -1441,7 +1511,7 @@ void run_search(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_
                  nullptr, nullptr, nl};
     std::vector<std::vector<Hit>> lh(nl);
     auto qhost = [&](uint32_t j) { return (const uint8_t*)QL->host.data() + QL->off[j]; };
-    traceback_2b(C, Q, QL->len.data(), nl, qhost, pair_ids, prelims, lh.data(), ctr, nullptr);
+    traceback_2b(C, C.work[0], Q, QL->len.data(), nl, qhost, pair_ids, prelims, lh.data(), ctr, nullptr);
     t0 = std::chrono::steady_clock::now();
     for (uint32_t j = 0; j < nl; ++j) {
         finish_query(C, lh[j], QL->len[j]);
@@ -1581,6 +1651,7 @@ static void check_tune(const rmb_tune& t) {
     if (t.prelim_budget_div < 16 || t.prelim_budget_div > 4096) throw Fail(RMB_EINVAL, "prelim_budget_div: 16..4096");
     if (t.ungapped_blocks_per_sm < 1 || t.ungapped_blocks_per_sm > 8)
         throw Fail(RMB_EINVAL, "ungapped_blocks_per_sm: 1..8");
+    if (t.lanes < 1 || t.lanes > 2) throw Fail(RMB_EINVAL, "lanes: 1 or 2");
 }
 
 int rmb_tune_get(const rmb_ctx* C, rmb_tune* out) {
@@ -1614,8 +1685,10 @@ int rmb_autotune(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uin
         CK(cudaSetDevice(C->p.device));
         QueriesPtr H(make_queries(C, nq, query, qlen));
         const rmb_tune keep = C->tune;
+        // candidates run on one lane: two lanes' kernels overlap and blur each kernel's time
         auto time_of = [&](const rmb_tune& t) {
             C->tune = t;
+            C->tune.lanes = 1;
             double ms = 1e300;
             for (int rep = 0; rep < 2; ++rep) {
                 std::vector<std::vector<Hit>> hits;
@@ -1895,15 +1968,9 @@ void rmb_ctx_destroy(rmb_ctx* C) {
     if (!C) return;
     cudaSetDevice(C->p.device);
     DBuf* all[] = {&C->d_plus, &C->d_rc, &C->d_align, &C->d_align_rc, &C->d_packed, &C->d_plus_off, &C->d_packed_off,
-                   &C->d_len, &C->d_params, &C->pv, &C->pv_off, &C->cs, &C->cs_off, &C->pos_off, &C->lut_keys,
-                   &C->lut_vals, &C->lut_keys2, &C->lut_vals2, &C->lut_counts,
-                   &C->cq, &C->cq_off, &C->lw, &C->counts, &C->offs, &C->hits, &C->hit_pair, &C->ub, &C->flags,
-                   &C->dd_scratch, &C->dd_cells, &C->ung_idx, &C->n_sel, &C->po, &C->wide, &C->wide2, &C->dres, &C->geo, &C->n_wide, &C->band,
-                   &C->sel, &C->surv, &C->cells, &C->fails, &C->temp, &C->tb_in, &C->tb_out, &C->tb_ops,
-                   &C->tb_scratch, &C->dust_scratch, &C->stage, &C->stage_start, &C->stage_over, &C->tb_ooff,
-                   &C->tb_ops2, &C->sched_params, &C->sched_pred, &C->sched_order, &C->sched_scratch,
-                   &C->sched_feat, &C->sched_cells, &C->ung_queue};
+                   &C->d_len, &C->d_params, &C->lw, &C->dust_scratch, &C->fails, &C->sched_params};
     for (DBuf* b : all) b->release();
+    for (Work& w : C->work) w.release();
     if (C->batch) {
         C->batch->release();
         delete C->batch;

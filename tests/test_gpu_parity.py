@@ -590,7 +590,7 @@ def test_plain_pipeline_matches_oracle(name, scale):
 def test_tune_knobs_leave_output_unchanged(name, scale):
     """The launch knobs (rmb_tune) shape only how the work is laid out: extreme settings of each,
     both dedup paths (the fused bucket-parallel dedup-extension and the extend-then-dedup pair),
-    and the autotuner's pick give the oracle's text byte for byte."""
+    one and two pipeline lanes, and the autotuner's pick give the oracle's text byte for byte."""
     qf, dbf, p = synthetic(name, scale, synth.RM_FLAGS)
     s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf)
     recs = api.read_fasta(qf)
@@ -601,7 +601,7 @@ def test_tune_knobs_leave_output_unchanged(name, scale):
     default = s.tune()
     assert s.search(enc, ids).tabular(FIELDS) == want
     for knobs in (dict(prelim_group=4), dict(prelim_group=16), dict(prelim_window=16, prelim_budget_div=16),
-                  dict(prelim_blocks_per_sm=1, ungapped_blocks_per_sm=1), dict(prelim_budget_div=4096),
+                  dict(prelim_blocks_per_sm=1, ungapped_blocks_per_sm=1), dict(prelim_budget_div=4096), dict(lanes=1),
                   dict(dedup_extend_hits_per_pair=0), dict(dedup_extend_hits_per_pair=-1)):
         s.set_tune(dict(default, **knobs))
         assert s.search(enc, ids).tabular(FIELDS) == want, knobs
