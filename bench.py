@@ -65,14 +65,16 @@ def parse(argv=None):
     ap.add_argument("--no-compare", action="store_true", help="skip the plain and FIFO comparison arms")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch knobs")
     ap.add_argument("--dust", action="store_true", help="mask the queries with DUST (the reference's default)")
-    ap.add_argument("--schedule", choices=["fifo", "learned"], default=None,
-                    help="prelim DP record order (default: learned for the batched workload, else FIFO)")
+    ap.add_argument("--schedule", choices=["fifo", "learned", "learned-full"], default=None,
+                    help="prelim DP record order: FIFO; learned (the predicted-costliest records first); "
+                         "learned-full (all in descending predicted cost).  Default: learned for the batched "
+                         "workload, else FIFO")
     ap.add_argument("--pipeline", choices=["batched", "plain"], default="batched")
     ap.add_argument("--sched-model", default=None, help="schedule network JSON (default: the committed one)")
     a = ap.parse_args(argv)
     if a.schedule is None:
         a.schedule = "learned" if a.workload == "batched" and a.pipeline == "batched" else "fifo"
-    if a.schedule == "learned" and a.pipeline == "plain":
+    if a.schedule != "fifo" and a.pipeline == "plain":
         ap.error("the learned order feeds the batched pipeline's queue")
     return a
 
@@ -291,7 +293,7 @@ def main():
     sdb = api.SubjectDb.from_records(db)
     compare = not args.no_compare and args.workload in ("batched", "plain") and args.pipeline == "batched"
     model = None
-    if args.schedule == "learned":
+    if args.schedule != "fifo":
         from rmblast_b200 import train_sched
         model = train_sched.load_model(Path(args.sched_model) if args.sched_model else train_sched.MODEL_PATH)
 
@@ -300,10 +302,11 @@ def main():
                               xdrop_ungap=p["xdrop_ungap"], xdrop_gap=p["xdrop_gap"],
                               xdrop_gap_final=p["xdrop_gap_final"], min_raw_gapped_score=p["min_raw_gapped_score"],
                               complexity_adjust=bool(p["complexity_adjust"]), mask_level=p["mask_level"],
-                              dust=bool(p.get("dust", 0)), device=local, schedule=1 if schedule == "learned" else 0,
+                              dust=bool(p.get("dust", 0)), device=local,
+                              schedule={"fifo": 0, "learned": 1, "learned-full": 2}[schedule],
                               pipeline=1 if pipeline == "plain" else 0)
         s = api.Searcher(sp, m, sdb)
-        if schedule == "learned":
+        if schedule != "fifo":
             s.set_schedule_model(model)
         return s
 
@@ -495,7 +498,7 @@ def main():
                             "gcups_computed": (me["gcups_computed"] / arms["plain"]["gcups_computed"]
                                                if arms["plain"]["gcups_computed"] else None),
                             "prelim_stage": arms["plain"]["prelim_ms"] / me["prelim_ms"] if me["prelim_ms"] else None}
-        if args.schedule == "learned":
+        if args.schedule != "fifo":
             s = searcher("batched", "fifo")
             if tuned is not None:
                 s.set_tune(tuned["tune"])

@@ -42,7 +42,10 @@ typedef struct rmb_params {
     int32_t complexity_adjust, dust, mask_level;
     int32_t ungapped_cutoff;
     int32_t device;       /* CUDA device ordinal */
-    int32_t schedule;     /* 0 = FIFO record queue; 1 = learned cost order (rmb_sched_set_model) */
+    int32_t schedule;     /* 0 = FIFO record queue; 1 = learned, front-loaded: the records the
+                             network (rmb_sched_set_model) predicts costliest, about 1/32 of them,
+                             go first and the rest keep their arrival order (reversed); 2 = learned,
+                             every record in descending predicted cost */
     int32_t kernels;      /* 0 = automatic; 1 = run every preliminary DP on the warp-cooperative
                              kernel (the thread-per-extension kernel's fallback), for testing */
     int32_t pipeline;     /* 0 = batched: the ungapped extension and the preliminary DP run as
@@ -87,16 +90,18 @@ typedef struct rmb_tune {
 
 /* Learned schedule of the preliminary DP (no counterpart in the reference, whose records run in
  * a fixed order; the order changes no result).  A 12 -> 64 -> 64 -> 1 ReLU network with BF16
- * weights predicts each ungapped record's DP cells (log1p), and with params.schedule = 1 the
- * records leave the DP queue in descending predicted cost, so long extensions start first.
+ * weights predicts each ungapped record's DP cells (log1p), and with params.schedule = 1 or 2 the
+ * records leave the DP queue with the long extensions first (schedule 1 moves only the predicted
+ * costliest ~1/32 to the front, so the others keep the neighbours they share sequences with;
+ * schedule 2 orders all of them by predicted cost).
  * Parameters: RMB_SCHED_NPARAM floats, W1[12][64] (W1[k*64+n]), b1[64], W2[64][64], b2[64],
  * w3[64], b3, then the features' mean[12] and 1/std[12].  Features of a record: ungapped score /
  * 100, log1p ungapped extent, log1p of the room left and right of the pivot on query and
  * subject, X / 100, strand, GC of ~32 subject bases at the pivot, score per base, log1p of the
  * pair's word hits, log1p of the diagonal room.
  *
- * rmb_sched_set_model: the network for this context's searches with schedule 1 (a search with
- * schedule 1 and no model fails with RMB_ESTATE).
+ * rmb_sched_set_model: the network for this context's searches with schedule 1 or 2 (such a search
+ * with no model fails with RMB_ESTATE).
  * rmb_sched_log: one FIFO search of the queries, returning for every record the thread kernel
  * completed its raw features (n x 12, malloc'd) and DP cells (n, malloc'd); free both with
  * rmb_text_free.  Training pairs for rmb_sched_train.

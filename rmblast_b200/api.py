@@ -227,7 +227,8 @@ class SearchParams:
     device: int = 0
     # 0: automatic kernel choice; 1: every preliminary DP on the warp-cooperative kernel
     kernels: int = 0
-    # 0: FIFO record queue; 1: learned cost order (Searcher.set_schedule_model)
+    # 0: FIFO record queue; 1: learned, the predicted-costliest records first; 2: learned, all in
+    # descending predicted cost (Searcher.set_schedule_model)
     schedule: int = 0
     # 0: batched (persistent kernels with device work queues); 1: plain (one launch per stage,
     # one work item per thread in arrival order)

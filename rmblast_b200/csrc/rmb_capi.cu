@@ -683,16 +683,18 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                                              W.counts.as<uint32_t>(), W.sched_feat.as<float>(), C.sms, st));
                     cells_out = W.sched_cells.as<uint32_t>();
                     ctr.launches += 1;
-                } else if (C.p.schedule == 1 && nu) {
-                    // the records in descending predicted cost
+                } else if (C.p.schedule >= 1 && nu) {
+                    // the records front-loaded by predicted cost (1), or all in descending cost (2)
                     W.sched_pred.ensure(nu * 4);
                     W.sched_order.ensure(nu * 4);
                     W.sched_scratch.ensure(sched_order_scratch_bytes());
+                    size_t tb = C.p.schedule == 1 ? sched_front_temp_bytes(nu) : 0;
+                    if (tb) W.temp.ensure(tb);
                     CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), nu, W.ung_idx.as<uint32_t>(),
                                           W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
                                           W.counts.as<uint32_t>(), C.sched_params.as<float>(),
                                           W.sched_pred.as<float>(), W.sched_scratch.p, W.sched_order.as<uint32_t>(),
-                                          C.sms, st));
+                                          C.sms, st, C.p.schedule, W.temp.p, tb));
                     order = W.sched_order.as<uint32_t>();
                     ctr.launches += 3;
                 }
@@ -1088,11 +1090,11 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         if (p.gap_open < 0 || p.gap_extend < 1) throw Fail(RMB_EINVAL, "gap costs out of range");
         if (p.xdrop_ungap < 0 || p.xdrop_gap < 0 || p.xdrop_gap_final < 0 || p.min_raw_gapped_score < 0)
             throw Fail(RMB_EINVAL, "negative X-drop or cutoff");
-        if (p.schedule != 0 && p.schedule != 1)
-            throw Fail(RMB_EINVAL, "schedule must be 0 (FIFO) or 1 (learned cost order)");
+        if (p.schedule < 0 || p.schedule > 2)
+            throw Fail(RMB_EINVAL, "schedule must be 0 (FIFO), 1 (learned, front-loaded) or 2 (learned, full order)");
         if (p.kernels != 0 && p.kernels != 1) throw Fail(RMB_EINVAL, "kernels must be 0 (automatic) or 1 (warp prelim)");
         if (p.pipeline != 0 && p.pipeline != 1) throw Fail(RMB_EINVAL, "pipeline must be 0 (batched) or 1 (plain)");
-        if (p.pipeline == 1 && p.schedule == 1)
+        if (p.pipeline == 1 && p.schedule != 0)
             throw Fail(RMB_EINVAL, "the learned order feeds the batched pipeline's record queue (pipeline 0)");
         C = new rmb_ctx();
         C->p = p;
@@ -1601,7 +1603,7 @@ int rmb_search_resident(rmb_ctx* C, rmb_queries* H, rmb_results** out, char* err
         if (!C || !H || !out) throw Fail(RMB_EINVAL, "null argument");
         if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before the search");
         if (H->device != C->p.device) throw Fail(RMB_EINVAL, "queries were uploaded to another device");
-        if (C->p.schedule == 1 && !C->sched_ready)
+        if (C->p.schedule >= 1 && !C->sched_ready)
             throw Fail(RMB_ESTATE, "schedule 1 needs the network: call rmb_sched_set_model first");
         CK(cudaSetDevice(C->p.device));
         std::vector<std::vector<Hit>> hits;
@@ -1680,7 +1682,7 @@ int rmb_autotune(rmb_ctx* C, uint32_t nq, const uint8_t* const* query, const uin
         if (!C || !best) throw Fail(RMB_EINVAL, "null argument");
         if (!C->loaded) throw Fail(RMB_ESTATE, "rmb_db_load must come before rmb_autotune");
         if (C->p.pipeline == 1) throw Fail(RMB_EINVAL, "the plain pipeline has no tuned knobs");
-        if (C->p.schedule == 1 && !C->sched_ready)
+        if (C->p.schedule >= 1 && !C->sched_ready)
             throw Fail(RMB_ESTATE, "schedule 1 needs the network: call rmb_sched_set_model first");
         CK(cudaSetDevice(C->p.device));
         QueriesPtr H(make_queries(C, nq, query, qlen));

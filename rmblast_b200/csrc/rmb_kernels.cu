@@ -25,6 +25,9 @@
 #include "rmb_dust.cuh"
 #include "rmb_kernels.hpp"
 #include "rmb_prelim_stream.cuh"
+
+#include <cub/device/device_partition.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include "rmb_sched.cuh"
 #include "rmb_ungapped.cuh"
 
@@ -2098,10 +2101,40 @@ cudaError_t launch_sched_features(const DevLib& L, const DevQueries& Q, const De
 
 size_t sched_order_scratch_bytes() { return 3 * SCHED_BINS * sizeof(unsigned int); }
 
+// The front of the front-loaded order: the lowest cost bin b such that the records in bins >= b
+// are at most n / SCHED_FRONT_DIV (SCHED_BINS when even the costliest bin holds more).
+constexpr uint64_t SCHED_FRONT_DIV = 32;
+__global__ void k_sched_cut(const unsigned int* __restrict__ hist, uint64_t n, unsigned int* __restrict__ cut) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint64_t limit = n / SCHED_FRONT_DIV;
+    uint64_t acc = 0;
+    unsigned int c = SCHED_BINS;
+    for (int b = SCHED_BINS - 1; b >= 0; --b) {
+        if (acc + hist[b] > limit) break;
+        acc += hist[b];
+        c = (unsigned int)b;
+    }
+    *cut = c;
+}
+
+struct SchedFront {
+    const float* pred;
+    const unsigned int* cut;
+    __host__ __device__ bool operator()(const uint32_t& i) const { return sched_bin(pred[i]) >= *cut; }
+};
+
+size_t sched_front_temp_bytes(uint64_t n) {
+    size_t tb = 0;
+    thrust::counting_iterator<uint32_t> it(0);
+    cub::DevicePartition::If(nullptr, tb, it, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)n,
+                             SchedFront{nullptr, nullptr});
+    return tb;
+}
+
 cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                const uint32_t* pair_hits, const float* params, float* pred, void* scratch,
-                               uint32_t* order, int sms, cudaStream_t st) {
+                               uint32_t* order, int sms, cudaStream_t st, int layout, void* temp, size_t temp_bytes) {
     if (!n) return cudaSuccess;
     unsigned int* hist = (unsigned int*)scratch;
     cudaError_t e = cudaMemsetAsync(hist, 0, SCHED_BINS * sizeof(unsigned int), st);
@@ -2110,6 +2143,18 @@ cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevPa
     const int grid = (int)std::min<uint64_t>((warps + SCHED_BLOCK / 32 - 1) / (SCHED_BLOCK / 32), (uint64_t)sms * 8);
     k_sched_predict<<<grid, SCHED_BLOCK, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, pair_hits, nullptr, params, pred,
                                                   hist);
+    if (layout == 1) {
+        // front-loaded: the predicted-costliest records (about n / 32) first, in arrival order, then
+        // the rest in reverse arrival order -- neighbouring records keep sharing their sequences
+        unsigned int* cut = hist + SCHED_BINS;
+        k_sched_cut<<<1, 1, 0, st>>>(hist, n, cut);
+        thrust::counting_iterator<uint32_t> it(0);
+        unsigned int* n_front = hist + SCHED_BINS + 1;
+        e = cub::DevicePartition::If(temp, temp_bytes, it, order, n_front, (int64_t)n, SchedFront{pred, cut}, st);
+        if (e != cudaSuccess) return e;
+        return cudaGetLastError();
+    }
+    // the full descending cost order
     k_sched_binstart<<<1, 1, 0, st>>>(hist, hist + SCHED_BINS, hist + 2 * SCHED_BINS);
     const uint64_t tile = 256ull * SCHED_TILE_PER_THREAD;
     const int g2 = (int)std::min<uint64_t>((n + tile - 1) / tile, (uint64_t)sms * 8);

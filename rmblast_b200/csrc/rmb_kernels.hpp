@@ -66,10 +66,13 @@ cudaError_t launch_sched_features(const DevLib& L, const DevQueries& Q, const De
                                   const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                   const uint32_t* pair_hits, float* out, int sms, cudaStream_t st);
 size_t sched_order_scratch_bytes();
+// layout 1: the predicted-costliest ~1/32 of the records first, the rest after in reverse arrival
+// order (temp: sched_front_temp_bytes(n) bytes); 2: all records in descending predicted cost
+size_t sched_front_temp_bytes(uint64_t n);
 cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                const uint32_t* pair_hits, const float* params, float* pred, void* scratch,
-                               uint32_t* order, int sms, cudaStream_t st);
+                               uint32_t* order, int sms, cudaStream_t st, int layout, void* temp, size_t temp_bytes);
 cudaError_t launch_sched_predict_features(uint64_t n, const float* feats, const float* params, float* pred, int sms,
                                           cudaStream_t st);
 // Records `list` (the thread kernel's overflow), one warp per extension; dres holds 2 x n_list

@@ -56,6 +56,30 @@ def queue_makespan(cells: np.ndarray, order: np.ndarray, workers: int) -> int:
     return max(free)
 
 
+def cost_bins(pred: np.ndarray) -> np.ndarray:
+    """rmb_sched.cuh sched_bin: 64 bins a quarter of a log-cell wide (0 for <= 0, 63 from 15.75)."""
+    b = np.asarray(pred, dtype=np.float32) * np.float32(4.0)
+    return np.where(b <= 0, 0, np.where(b >= 63, 63, np.trunc(np.clip(b, 0, 63)))).astype(np.int64)
+
+
+def front_loaded_order(pred: np.ndarray, front_div: int = 32) -> np.ndarray:
+    """The queue order of schedule 1 (k_sched_cut + the partition in rmb_kernels.cu) on the host:
+    the records in the costliest of 64 predicted-cost bins, as many bins as hold at most
+    n / front_div records, in arrival order, then the rest in reverse arrival order."""
+    pred = np.asarray(pred, dtype=np.float32)
+    b = cost_bins(pred)
+    hist = np.bincount(b, minlength=64)
+    limit, acc, cut = len(pred) // front_div, 0, 64
+    for k in range(63, -1, -1):
+        if acc + hist[k] > limit:
+            break
+        acc += hist[k]
+        cut = k
+    sel = b >= cut
+    idx = np.arange(len(pred))
+    return np.concatenate([idx[sel], idx[~sel][::-1]])
+
+
 def load_model(path: Path = MODEL_PATH) -> np.ndarray:
     """The committed network parameters (rmb_sched layout) for Searcher.set_schedule_model."""
     return np.asarray(json.loads(path.read_text())["params"], dtype=np.float32)

@@ -564,10 +564,11 @@ def test_config1_fifty_chunks_matches_oracle():
     assert res.counters["ungapped"] == ctr["ungapped"]
 
 
-def test_config3_learned_order_matches_oracle():
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_config3_learned_order_matches_oracle(schedule):
     """Config 3: chunks of 1-200 kb through the batched pipeline with the learned record order
-    (the committed network), every line against the oracle."""
-    txt, want, res, ctr = _config_case("batched", 0.005, schedule=1)
+    (the committed network; front-loaded and full cost order), every line against the oracle."""
+    txt, want, res, ctr = _config_case("batched", 0.005, schedule=schedule)
     assert txt.count("\n") > 500
     assert txt == want
     assert res.counters["ungapped"] == ctr["ungapped"]

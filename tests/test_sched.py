@@ -173,5 +173,9 @@ def test_learned_order_shortens_the_record_queue():
     fifo = train_sched.queue_makespan(cells, np.arange(len(cells)), lanes)
     learned = train_sched.queue_makespan(cells, np.argsort(-pred, kind="stable"), lanes)
     ideal = train_sched.queue_makespan(cells, np.argsort(-cells.astype(np.int64), kind="stable"), lanes)
-    print(f"records {len(cells)} lanes {lanes} makespan fifo {fifo} learned {learned} true-cost order {ideal}")
-    assert learned < fifo
+    # the library's default learned layout: the predicted-costliest 1/32 first, the rest reversed
+    front = train_sched.front_loaded_order(pred)
+    loaded = train_sched.queue_makespan(cells, front, lanes)
+    print(f"records {len(cells)} lanes {lanes} makespan fifo {fifo} learned {learned} front-loaded {loaded} "
+          f"true-cost order {ideal}")
+    assert learned < fifo and loaded < fifo

@@ -65,3 +65,23 @@ def test_queue_makespan_list_scheduling():
     lb = max(c.sum() / 16, c.max())
     assert train_sched.queue_makespan(c, np.argsort(-c, kind="stable"), 16) <= 4 / 3 * lb + 1
     assert train_sched.queue_makespan(c, np.arange(5000), 16) <= 2 * lb
+
+
+def test_front_loaded_order():
+    """Schedule 1's queue on the host: the costliest bins (at most n / 32 records) first in arrival
+    order, the others after them in reverse arrival order."""
+    rng = np.random.default_rng(5)
+    pred = rng.normal(7.0, 1.0, 4096).astype(np.float32)
+    order = train_sched.front_loaded_order(pred)
+    assert sorted(order.tolist()) == list(range(4096))
+    b = train_sched.cost_bins(pred)
+    hist = np.bincount(b, minlength=64)
+    cut = 64
+    while cut > 0 and hist[cut - 1:].sum() <= 4096 // 32:
+        cut -= 1
+    nf = int((b >= cut).sum())
+    front, back = order[:nf], order[nf:]
+    assert 0 < len(front) <= 4096 // 32
+    assert (np.diff(front) > 0).all() and (np.diff(back) < 0).all()
+    assert b[front].min() > b[back].max()
+    assert train_sched.cost_bins(np.array([-1.0, 0.0, 0.3, 2.26, 15.8, 99.0])).tolist() == [0, 0, 1, 9, 63, 63]
