@@ -64,6 +64,8 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain and FIFO comparison arms")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch knobs")
+    ap.add_argument("--lanes", type=int, choices=[1, 2], default=None,
+                    help="pipeline lanes of the measured arm (default: the library's, 2)")
     ap.add_argument("--dust", action="store_true", help="mask the queries with DUST (the reference's default)")
     ap.add_argument("--schedule", choices=["fifo", "learned", "learned-full"], default=None,
                     help="prelim DP record order: FIFO; learned (the predicted-costliest records first); "
@@ -380,6 +382,8 @@ def main():
     tuned = None
     if args.pipeline == "batched" and not args.no_autotune:
         tuned = s.autotune([api.encode(x) for _, x in tune_sample])
+    if args.lanes:
+        s.set_tune(dict(s.tune(), lanes=args.lanes))
     clk = {}
     ms_step, c = resident_arm(s, clk)
     # the context's query buffers (device and pinned host) grow to the largest step untimed

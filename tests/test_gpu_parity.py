@@ -555,6 +555,16 @@ def test_config0_full_size_matches_oracle():
     assert res.counters["ungapped"] == ctr["ungapped"]
 
 
+def test_config1_full_size_matches_oracle():
+    """Config 1 at its full size: all 1,000 chunks of 60 kb (60 Mb) against the 2,000-consensus
+    library, word 11, through the batched pipeline (two lanes, tuned defaults); every one of the
+    ~25,000 lines against the oracle (about a minute on 16 host cores)."""
+    txt, want, res, ctr = _config_case("plain", 1.0)
+    assert txt.count("\n") > 20000
+    assert txt == want
+    assert res.counters["ungapped"] == ctr["ungapped"] and res.counters["prelims"] >= ctr["prelims"]
+
+
 def test_config1_fifty_chunks_matches_oracle():
     """Config 1's shape at 50 of its 1,000 chunks of 60 kb (3 Mb) against the 2,000-consensus
     library, word 11."""
