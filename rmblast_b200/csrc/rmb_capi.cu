@@ -179,7 +179,7 @@ static rmb_tune default_tune() {
     t.prelim_budget_div = 128;
     t.ungapped_blocks_per_sm = 8;
     t.dedup_extend_hits_per_pair = 256;
-    t.lanes = 2;
+    t.lanes = 1;
     return t;
 }
 

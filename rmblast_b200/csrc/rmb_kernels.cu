@@ -455,8 +455,8 @@ __global__ void __launch_bounds__(128) k_dedup(DevLib L, DevQueries Q, int32_t w
 // only the chain of bucket(diag), and a stale cell is recycled only inside that chain
 // (diag_hash.rs:51-110); cells are drawn from one pool, but which index a cell gets changes
 // nothing.  So one warp replays one (query, subject) pair: the pair's hits go by in scan order,
-// 32 a round; the hits of a round that share a bucket take turns in scan order (one sub-round
-// each), the others run at once, and only an admitted hit is extended.  The reference's work,
+// 32 a round; the hits of a round that share a bucket are decided in scan order, the buckets at
+// once, and only an admitted hit is extended.  The reference's work,
 // in its order per bucket, with the buckets in parallel: for hit-dense pairs (an all-against-
 // all search keeps ~1% of its hits), where extending every hit first wastes most of the work.
 constexpr int DDX_WARPS = 8;
@@ -515,19 +515,34 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
                 bk = diag_bucket(diag);
             }
             const unsigned same = __match_any_sync(FULL, bk);
-            const int turn = __popc(same & lt);
-            const int turns = __reduce_max_sync(FULL, have ? __popc(same) : 0);
-            for (int t = 0; t < turns; ++t) {
-                const bool mine = have && turn == t;
-                bool ext = false;
+            // Passes over the round's pending hits.  Each looks its diagonal up in the chains as
+            // they stand; in each bucket the pending hits before the first one the hash admits are
+            // dropped at once (a dropped hit changes no chain, so the lookups of the ones after it
+            // stay right), the first admitted one is extended and inserted, and the bucket's hits
+            // after it wait for the next pass.  A run of dropped hits on one repeat's diagonal
+            // takes one pass instead of one turn each.
+            bool pending = have;
+            while (__any_sync(FULL, pending)) {
                 uint32_t head = 0;
-                if (mine) {
+                bool admitted = false;
+                if (pending) {
                     head = hd[bk];
                     uint32_t last = 0;
                     for (uint32_t c = head; c; c = pool[c - 1].next)
                         if (pool[c - 1].diag == diag) { last = pool[c - 1].level; break; }
-                    if (key < last) flags[i] = 0;
-                    else ext = true;
+                    admitted = key >= last;
+                }
+                const unsigned adm = __ballot_sync(FULL, pending && admitted) & same;
+                const int first = adm ? __ffs((int)adm) - 1 : 32;
+                bool ext = false;
+                if (pending) {
+                    if (lane < first) {
+                        flags[i] = 0;
+                        pending = false;
+                    } else if (lane == first) {
+                        ext = true;
+                        pending = false;
+                    }
                 }
                 UngBox u{};
                 if (ext) {
@@ -568,7 +583,7 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
                     hd[bk] = idx;
                 }
                 occ += (uint32_t)__popc(nn);
-                __syncwarp();  // this turn's chain updates before the next turn reads them
+                __syncwarp();  // this pass's chain updates before the next pass reads them
             }
         }
     }

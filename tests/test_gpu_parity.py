@@ -31,7 +31,7 @@ def searcher(p: dict, matrix_text: str, matrix_name: str, db_fasta: str, kernels
                           **dict(zip(("matrix_lambda", "matrix_k", "matrix_alpha", "matrix_beta"),
                                      p.get("cli_stats", (0.0, 0.0, 0.0, 0.0)))))
     s = api.Searcher(sp, m, api.SubjectDb.from_fasta(db_fasta))
-    if schedule == 1:
+    if schedule >= 1:
         from rmblast_b200 import train_sched
         s.set_schedule_model(train_sched.load_model())
     return s
