@@ -82,10 +82,16 @@ typedef struct rmb_ctx rmb_ctx;
  *   lanes                   1 or 2 pipeline lanes: with 2, a search's queries go in about four
  *                           sub-batches to two streams with their own buffers and host threads,
  *                           so one lane's host steps overlap the other's kernels (twice the
- *                           per-batch device memory) */
+ *                           per-batch device memory)
+ *   graph                   1: each pair range's device chain from the dedup to the prelim
+ *                           survivors runs as one CUDA graph, its counts kept on the device;
+ *                           0: stage by stage, the host reading each count; 2: the graph with
+ *                           room for one warp-kernel record and one survivor, so that every range
+ *                           also runs the stage-by-stage finish past those capacities (a test
+ *                           setting) */
 typedef struct rmb_tune {
     int32_t prelim_group, prelim_blocks_per_sm, prelim_window, prelim_budget_div;
-    int32_t ungapped_blocks_per_sm, dedup_extend_hits_per_pair, lanes;
+    int32_t ungapped_blocks_per_sm, dedup_extend_hits_per_pair, lanes, graph;
 } rmb_tune;
 
 /* Learned schedule of the preliminary DP (no counterpart in the reference, whose records run in

@@ -38,7 +38,7 @@ class _Params(C.Structure):
 
 class _Tune(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("prelim_group", "prelim_blocks_per_sm", "prelim_window", "prelim_budget_div",
-                                         "ungapped_blocks_per_sm", "dedup_extend_hits_per_pair", "lanes")]
+                                         "ungapped_blocks_per_sm", "dedup_extend_hits_per_pair", "lanes", "graph")]
 
 
 class _Hsp(C.Structure):

@@ -157,7 +157,19 @@ struct Work {
         n_wide, band, sel, surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over,
         tb_ooff, tb_ops2, ung_queue;
     DBuf sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
+    // the device chain as a CUDA graph (chain_graph): its executable, its timing events and the
+    // pinned block its counts come back in
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev[6] = {};
+    HostBuf hcount;
     void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        for (cudaEvent_t& e : ev)
+            if (e) {
+                cudaEventDestroy(e);
+                e = nullptr;
+            }
         DBuf* all[] = {&pv, &pv_off, &cs, &cs_off, &cq, &cq_off, &pos_off, &lut_keys, &lut_vals, &lut_keys2,
                        &lut_vals2, &lut_counts, &counts, &offs, &hits, &hit_pair, &ub, &flags, &dd_scratch, &dd_cells,
                        &ung_idx, &n_sel, &po, &wide, &wide2, &dres, &geo, &n_wide, &band, &sel, &surv, &cells, &fails,
@@ -180,6 +192,7 @@ static rmb_tune default_tune() {
     t.ungapped_blocks_per_sm = 8;
     t.dedup_extend_hits_per_pair = 256;
     t.lanes = 1;
+    t.graph = 1;
     return t;
 }
 
@@ -316,6 +329,235 @@ void finish_query(const rmb_ctx& C, std::vector<Hit>& v, uint32_t qlen) {
         v.erase(std::remove_if(v.begin(), v.end(), [&](const Hit& h) { return h.evalue > P.evalue; }), v.end());
     apply_mask_level(v, P.mask_level < 0 ? 101u : (uint32_t)P.mask_level);
     sort_hit_list_order(v, C.ids);
+}
+
+// The batched pipeline's device chain of one pair range as one CUDA graph: the dedup with the
+// ungapped extension, the ungapped records' selection, the prelim DP geometry, the learned order,
+// the prelim DP with its warp fallback for the records it passes on, and the survivors' selection
+// and gather.  Every count after the word hits is read by the kernels from device memory, so the
+// chain runs with no host round trip; buffers are sized for the range's word hits, an upper bound
+// on every later count.  The graph is captured per pair range and updated in place
+// (cudaGraphExecUpdate) while its shape repeats.  The rare cases past the graph's capacities (a
+// fallback list longer than it holds, records wider than the warp ring, more survivors than it
+// gathers) finish stage by stage after it.  Sets the survivors and the counters the
+// stage-by-stage path sets.
+void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_t pair0, uint64_t npairs,
+                 uint64_t nh, uint32_t qmax, std::vector<SurvivorRec>& sv, rmb_counters& ctr) {
+    const rmb_params& P = C.p;
+    cudaStream_t st = W.st;
+    const int32_t dx = C.tune.dedup_extend_hits_per_pair;
+    const bool fused = dx >= 0 && nh >= (uint64_t)dx * npairs;
+    const bool learned = P.schedule == 1;
+    const uint64_t n1 = std::max<uint64_t>(nh, 1);
+    // the warp kernel's list and the survivors gathered in the graph (graph knob 2: one of each,
+    // so that every range also takes the finish past them)
+    const uint64_t cap_min = C.tune.graph == 2 ? 1 : 1u << 16;
+    const uint64_t wcap = std::min<uint64_t>(n1, std::max<uint64_t>(cap_min, C.tune.graph == 2 ? 1 : n1 / 64));
+    const uint64_t scap = std::min<uint64_t>(n1, std::max<uint64_t>(cap_min, C.tune.graph == 2 ? 1 : n1 / 256));
+    W.flags.ensure(nh + 1);
+    W.dd_cells.ensure(n1 * diag_cell_bytes());
+    W.ung_queue.ensure(16);
+    if (!fused) W.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
+    W.ung_idx.ensure(n1 * 4);
+    W.n_sel.ensure(16);   // [0] ungapped records, [1] survivors
+    W.n_wide.ensure(16);  // [0] records the thread kernel passed on, [1] its queue, [2] those the warp kernel did
+    W.cells.ensure(16);   // [0] DP cells, [1] the thread kernel's alone
+    W.fails.ensure(16);
+    W.po.ensure(n1 * sizeof(PrelimOut));
+    W.geo.ensure(n1 * prelim_geo_bytes());
+    W.wide.ensure(n1 * 4);
+    W.wide2.ensure(wcap * 4);
+    W.dres.ensure(wcap * 2 * sizeof(int4));
+    W.sel.ensure(n1 * 4);
+    W.surv.ensure(scap * sizeof(SurvivorRec));
+    if (learned) {
+        W.sched_pred.ensure(n1 * 4);
+        W.sched_order.ensure(n1 * 4);
+        W.sched_scratch.ensure(sched_order_scratch_bytes());
+    }
+    size_t t_eq = 0, t_pre = 0, t_front = learned ? sched_front_temp_bytes(n1) : 0;
+    CK(launch_select_eq(W.flags.as<uint8_t>(), nh, 3, W.ung_idx.as<uint32_t>(), W.n_sel.as<uint32_t>(), nullptr, t_eq,
+                        st));
+    CK(launch_select_prelim(W.po.as<PrelimOut>(), n1, W.sel.as<uint32_t>(), W.n_sel.as<uint32_t>() + 1, nullptr, t_pre,
+                            st, W.n_sel.as<unsigned int>()));
+    W.temp.ensure(std::max(t_eq, std::max(t_pre, t_front)));
+    W.hcount.resize(64);
+    for (cudaEvent_t& e : W.ev)
+        if (!e) CK(cudaEventCreate(&e));
+    const rmb_tune& tn = C.tune;
+    StreamLaunch cfg;
+    cfg.group = tn.prelim_group;
+    cfg.blocks_per_sm = tn.prelim_blocks_per_sm;
+    cfg.window = tn.prelim_window;
+    cfg.budget_div = tn.prelim_budget_div;
+    auto rec = [&](int k) { CK(cudaEventRecordWithFlags(W.ev[k], st, cudaEventRecordExternal)); };
+
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+        CK(cudaMemsetAsync(W.n_wide.p, 0, 16, st));
+        CK(cudaMemsetAsync(W.cells.p, 0, 16, st));
+        CK(cudaMemsetAsync(W.fails.p, 0, 16, st));
+        rec(0);
+        if (fused) {
+            CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut, pair0, npairs, W.offs.as<uint64_t>(),
+                                   W.hits.as<SeedHit>(), W.ub.as<UngBox>(), W.flags.as<uint8_t>(), W.dd_cells.p,
+                                   W.ung_queue.as<unsigned long long>(), C.sms, st));
+        } else {
+            CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut, nh, W.hits.as<SeedHit>(),
+                               W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), C.sms, st,
+                               W.ung_queue.as<unsigned long long>(), tn.ungapped_blocks_per_sm));
+            CK(launch_dedup(C.L, Q, P.word_size, ucut, pair0, npairs, W.offs.as<uint64_t>(), W.hits.as<SeedHit>(),
+                            W.ub.as<UngBox>(), W.flags.as<uint8_t>(), W.dd_scratch.as<uint32_t>(), W.dd_cells.p,
+                            C.sms, st));
+        }
+        CK(launch_select_eq(W.flags.as<uint8_t>(), nh, 3, W.ung_idx.as<uint32_t>(), W.n_sel.as<uint32_t>(), W.temp.p,
+                            t_eq, st));
+        rec(1);
+        const unsigned int* nu_dev = W.n_sel.as<unsigned int>();
+        CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), n1, W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(),
+                              W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.geo.p, C.sms, st, nu_dev));
+        const uint32_t* order = nullptr;
+        if (learned) {
+            CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), n1, W.ung_idx.as<uint32_t>(),
+                                  W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
+                                  W.counts.as<uint32_t>(), C.sched_params.as<float>(), W.sched_pred.as<float>(),
+                                  W.sched_scratch.p, W.sched_order.as<uint32_t>(), C.sms, st, 1, W.temp.p, t_front,
+                                  nu_dev));
+            order = W.sched_order.as<uint32_t>();
+        }
+        rec(2);
+        CK(launch_prelim_stream(C.d_params.as<DevParams>(), n1, W.geo.p, W.po.as<PrelimOut>(), W.wide.as<uint32_t>(),
+                                W.n_wide.as<unsigned int>(), W.cells.as<unsigned long long>(), C.sms, st, order,
+                                nullptr, false, cfg,
+                                StreamDevCounts{nu_dev, learned ? sched_front_count(W.sched_scratch.p) : nullptr, n1}));
+        rec(3);
+        CK(cudaMemcpyAsync(W.cells.as<unsigned long long>() + 1, W.cells.p, 8, cudaMemcpyDeviceToDevice, st));
+        CK(launch_prelim_split(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)wcap, W.wide.as<uint32_t>(),
+                               W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(),
+                               W.ub.as<UngBox>(), W.dres.as<int4>(), W.po.as<PrelimOut>(), W.wide2.as<uint32_t>(),
+                               W.n_wide.as<unsigned int>() + 2, W.cells.as<unsigned long long>(), C.sms, st,
+                               W.n_wide.as<unsigned int>()));
+        rec(4);
+        CK(launch_select_prelim(W.po.as<PrelimOut>(), n1, W.sel.as<uint32_t>(), W.n_sel.as<uint32_t>() + 1, W.temp.p,
+                                t_pre, st, nu_dev));
+        CK(launch_gather_survivors((uint32_t)scap, W.sel.as<uint32_t>(), W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(),
+                                   W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.po.as<PrelimOut>(),
+                                   W.surv.as<SurvivorRec>(), st, W.n_sel.as<unsigned int>() + 1));
+        rec(5);
+        uint8_t* hc = W.hcount.data();
+        CK(cudaMemcpyAsync(hc, W.n_sel.p, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hc + 8, W.n_wide.p, 12, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hc + 24, W.cells.p, 16, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hc + 40, W.fails.p, 4, cudaMemcpyDeviceToHost, st));
+    } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    CK(cudaStreamEndCapture(st, &g));
+    if (W.exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(W.exec, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(W.exec);
+            W.exec = nullptr;
+        }
+    }
+    if (!W.exec) {
+        const cudaError_t e = cudaGraphInstantiate(&W.exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            CK(e);
+        }
+    }
+    cudaGraphDestroy(g);
+    CK(cudaGraphLaunch(W.exec, st));
+    CK(cudaStreamSynchronize(st));
+    const uint8_t* hc = W.hcount.data();
+    uint32_t nu, nsv, nw, nw2;
+    unsigned long long cells, main_cells;
+    unsigned int fails;
+    memcpy(&nu, hc, 4);
+    memcpy(&nsv, hc + 4, 4);
+    memcpy(&nw, hc + 8, 4);
+    memcpy(&nw2, hc + 16, 4);
+    memcpy(&cells, hc + 24, 8);
+    memcpy(&main_cells, hc + 32, 8);
+    memcpy(&fails, hc + 40, 4);
+    auto ms = [&](int a, int b) {
+        float m = 0;
+        if (cudaEventElapsedTime(&m, W.ev[a], W.ev[b]) != cudaSuccess) {
+            cudaGetLastError();  // a timing gap is not a search failure
+            m = 0;
+        }
+        return (double)m;
+    };
+    ctr.gpu_ms_dedup += ms(0, 1);
+    ctr.gpu_ms_prelim += ms(1, 5);
+    ctr.gpu_ms_prelim_main += ms(2, 3);
+    ctr.so_cells_main += main_cells;
+    ctr.launches += (fused ? 1 : 2) + 1 + 1 + (learned ? 3 : 0) + 1 + 2 + 1 + 1;
+    ctr.ungapped += nu;
+    ctr.prelim_dp += nu;
+    if (nw > wcap || nw2 || nsv > scap) {
+        // past the graph's capacities: the fallbacks, the selection and the gather stage by stage
+        EvTimer ex;
+        ex.start(st);
+        if (nw > wcap) {
+            W.wide2.ensure((uint64_t)nw * 4);
+            W.dres.ensure((uint64_t)nw * 2 * sizeof(int4));
+            CK(cudaMemsetAsync(W.n_wide.as<unsigned int>() + 2, 0, 4, st));
+            // the listed records again, all of them (the same results for the first wcap)
+            CK(cudaMemsetAsync(W.cells.p, 0, 8, st));
+            CK(launch_prelim_split(C.L, Q, C.d_params.as<DevParams>(), nw, W.wide.as<uint32_t>(),
+                                   W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(),
+                                   W.ub.as<UngBox>(), W.dres.as<int4>(), W.po.as<PrelimOut>(), W.wide2.as<uint32_t>(),
+                                   W.n_wide.as<unsigned int>() + 2, W.cells.as<unsigned long long>(), C.sms, st));
+            unsigned long long warp_cells = 0;
+            CK(cudaMemcpyAsync(&nw2, W.n_wide.as<unsigned int>() + 2, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&warp_cells, W.cells.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            cells = main_cells + warp_cells;
+            ctr.launches += 2;
+        }
+        if (nw2) {
+            const uint64_t cap = (uint64_t)std::max(qmax, C.max_slen) + 2;
+            const uint32_t threads = std::min<uint32_t>(nw2, (uint32_t)std::max<uint64_t>(128, (1ull << 31) / (cap * 8)));
+            W.band.ensure((uint64_t)((threads + 127) / 128 * 128) * cap * 8);
+            CK(cudaMemsetAsync(W.cells.p, 0, 8, st));
+            CK(launch_prelim_wide(C.L, Q, C.d_params.as<DevParams>(), nw2, W.wide2.as<uint32_t>(),
+                                  W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(),
+                                  W.ub.as<UngBox>(), W.po.as<PrelimOut>(), W.band.as<int2>(), cap, threads,
+                                  W.cells.as<unsigned long long>(), W.fails.as<unsigned int>(), st));
+            unsigned long long wide_cells = 0;
+            CK(cudaMemcpyAsync(&wide_cells, W.cells.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&fails, W.fails.p, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            cells += wide_cells;
+            ctr.launches += 1;
+        }
+        size_t tb = 0;
+        CK(launch_select_prelim(W.po.as<PrelimOut>(), nu, W.sel.as<uint32_t>(), W.n_sel.as<uint32_t>() + 1, nullptr, tb,
+                                st));
+        W.temp.ensure(tb);
+        CK(launch_select_prelim(W.po.as<PrelimOut>(), nu, W.sel.as<uint32_t>(), W.n_sel.as<uint32_t>() + 1, W.temp.p,
+                                tb, st));
+        CK(cudaMemcpyAsync(&nsv, W.n_sel.as<uint32_t>() + 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        W.surv.ensure(std::max<uint64_t>(nsv, 1) * sizeof(SurvivorRec));
+        CK(launch_gather_survivors(nsv, W.sel.as<uint32_t>(), W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(),
+                                   W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.po.as<PrelimOut>(),
+                                   W.surv.as<SurvivorRec>(), st));
+        ex.stop(st);
+        ctr.gpu_ms_prelim += ex.ms();
+        ctr.launches += 2;
+    }
+    if (fails) throw Fail(RMB_ECUDA, "prelim DP band exceeded its storage");
+    ctr.so_cells += cells;
+    sv.resize(nsv);
+    if (nsv) CK(cudaMemcpyAsync(sv.data(), W.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
 }
 
 // Counters of one lane added into another's (the device times of the two lanes add up: they
@@ -528,10 +770,19 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             ctr.launches += 2;
             ctr.ms_scan += ms_since(t0);
 
+            W.ub.ensure(std::max<uint64_t>(nh, 1) * sizeof(UngBox));
+            std::vector<SurvivorRec> sv;
+            if (C.tune.graph && P.pipeline != 1 && C.prelim_stream && !taps && !C.sched_log && P.schedule != 2) {
+                // ---- the dedup through the prelim survivors as one graph, no host round trip
+                t0 = std::chrono::steady_clock::now();
+                uint32_t qmax = 0;
+                for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
+                chain_graph(C, W, Q, ucut[qb], pair0, npairs, nh, qmax, sv, ctr);
+                ctr.ms_prelim_dp += ms_since(t0);
+            } else {
             // ---- ungapped extension of every hit, then the per-pair dedup; or, for hit-dense
             // pairs (most hits dropped by the hash), the dedup extending only what it admits
             t0 = std::chrono::steady_clock::now();
-            W.ub.ensure(nh * sizeof(UngBox));
             const int32_t dx = C.tune.dedup_extend_hits_per_pair;
             const bool fused = P.pipeline != 1 && dx >= 0 && nh >= (uint64_t)dx * npairs;
             if (fused) {
@@ -709,7 +960,10 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 CK(launch_prelim_stream(C.d_params.as<DevParams>(), nu, W.geo.p, W.po.as<PrelimOut>(),
                                         W.wide.as<uint32_t>(), W.n_wide.as<unsigned int>(),
                                         W.cells.as<unsigned long long>(), C.sms, st, order, cells_out,
-                                        P.pipeline == 1, cfg));
+                                        P.pipeline == 1, cfg,
+                                        C.p.schedule == 1 && order
+                                            ? StreamDevCounts{nullptr, sched_front_count(W.sched_scratch.p), nu}
+                                            : StreamDevCounts{}));
                 ev_main.stop(st);
                 if (cells_out) {
                     std::vector<float> f(nu * SCHED_NF_HOST);
@@ -799,10 +1053,11 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             CK(launch_gather_survivors(nsv, W.sel.as<uint32_t>(), W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(),
                                        W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.po.as<PrelimOut>(),
                                        W.surv.as<SurvivorRec>(), st));
-            std::vector<SurvivorRec> sv(nsv);
+            sv.resize(nsv);
             if (nsv) CK(cudaMemcpyAsync(sv.data(), W.surv.p, nsv * sizeof(SurvivorRec), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             ctr.ms_prelim_dp += ms_since(t0);
+            }
 
             // ---- host Phase 2a filter per pair
             t0 = std::chrono::steady_clock::now();
@@ -1654,6 +1909,7 @@ static void check_tune(const rmb_tune& t) {
     if (t.ungapped_blocks_per_sm < 1 || t.ungapped_blocks_per_sm > 8)
         throw Fail(RMB_EINVAL, "ungapped_blocks_per_sm: 1..8");
     if (t.lanes < 1 || t.lanes > 2) throw Fail(RMB_EINVAL, "lanes: 1 or 2");
+    if (t.graph < 0 || t.graph > 2) throw Fail(RMB_EINVAL, "graph: 0, 1 or 2");
 }
 
 int rmb_tune_get(const rmb_ctx* C, rmb_tune* out) {

@@ -1028,7 +1028,9 @@ __global__ void __launch_bounds__(256) k_prelim_warp_dir(DevLib L, DevQueries Q,
                                                           const SeedHit* __restrict__ hits,
                                                           const uint32_t* __restrict__ hit_pair,
                                                           const UngBox* __restrict__ ub, int4* __restrict__ dres,
-                                                          unsigned long long* __restrict__ cells_total) {
+                                                          unsigned long long* __restrict__ cells_total,
+                                                          const unsigned int* __restrict__ n_dev) {
+    if (n_dev) n_list = min(*n_dev, n_list);  // the count on the device, n_list the list's capacity
     __shared__ int2 ring[(256 / 32) * RING_W];
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
@@ -1064,7 +1066,8 @@ __global__ void k_prelim_combine(DevLib L, DevQueries Q, const DevParams* __rest
                                  const SeedHit* __restrict__ hits, const uint32_t* __restrict__ hit_pair,
                                  const UngBox* __restrict__ ub, const int4* __restrict__ dres,
                                  PrelimOut* __restrict__ out, uint32_t* __restrict__ wide,
-                                 unsigned int* __restrict__ n_wide) {
+                                 unsigned int* __restrict__ n_wide, const unsigned int* __restrict__ n_dev) {
+    if (n_dev) n_list = min(*n_dev, n_list);
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n_list) return;
     const uint32_t t = list[k];
@@ -1097,7 +1100,9 @@ __global__ void __launch_bounds__(128) k_prelim_wide(DevLib L, DevQueries Q, con
                                                       const UngBox* __restrict__ ub, PrelimOut* __restrict__ out,
                                                       int2* __restrict__ band_mem, uint64_t band_cap,
                                                       unsigned long long* __restrict__ cells_total,
-                                                      unsigned int* __restrict__ failures) {
+                                                      unsigned int* __restrict__ failures,
+                                                      const unsigned int* __restrict__ n_dev) {
+    if (n_dev) n_wide = min(*n_dev, n_wide);
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
     __syncthreads();
@@ -1181,7 +1186,9 @@ __global__ void __launch_bounds__(SCHED_BLOCK) k_sched_predict(DevLib L, DevQuer
                                                                 const uint32_t* __restrict__ pair_hits,
                                                                 const float* __restrict__ feats,
                                                                 const float* __restrict__ params,
-                                                                float* __restrict__ pred, unsigned int* __restrict__ hist) {
+                                                                float* __restrict__ pred, unsigned int* __restrict__ hist,
+                                                                const unsigned int* __restrict__ n_dev) {
+    if (n_dev) n = *n_dev;
     __shared__ SchedSmem S;
     __shared__ __align__(16) uint16_t xs[SCHED_BLOCK / 32][32][16];
     __shared__ float ys[SCHED_BLOCK / 32][32];
@@ -1272,7 +1279,9 @@ __global__ void __launch_bounds__(256) k_prelim_prep(DevLib L, DevQueries Q, con
                                                       uint64_t n, const uint32_t* __restrict__ idx,
                                                       const SeedHit* __restrict__ hits,
                                                       const uint32_t* __restrict__ hit_pair,
-                                                      const UngBox* __restrict__ ub, PrelimGeo* __restrict__ geo) {
+                                                      const UngBox* __restrict__ ub, PrelimGeo* __restrict__ geo,
+                                                      const unsigned int* __restrict__ n_dev) {
+    if (n_dev) n = *n_dev;  // the count on the device (a graph-captured chain), n its capacity
     const int32_t goe = P->gap_open + P->gap_extend;
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
         const RecGeom g = rec_geom(L, Q, P, idx[t], hits, hit_pair, ub);
@@ -1332,7 +1341,8 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
                 PrelimOut* __restrict__ out,
                 uint32_t* __restrict__ wide, unsigned int* __restrict__ n_wide, unsigned int* __restrict__ queue,
                 unsigned long long* __restrict__ cells_total, uint32_t max_cells,
-                const uint32_t* __restrict__ order, uint32_t* __restrict__ cells_out, uint32_t window) {
+                const uint32_t* __restrict__ order, uint32_t* __restrict__ cells_out, uint32_t window,
+                StreamDevCounts dc, uint32_t budget_div) {
     __shared__ uint32_t ring[STREAM_RING * STREAM_BLOCK];
     __shared__ int32_t smat[256];
     {
@@ -1344,8 +1354,20 @@ k_prelim_stream(const DevParams* __restrict__ P, uint64_t n, const PrelimGeo* __
     }
     __syncthreads();
     StreamDevEnv<QUEUE> env{ring + threadIdx.x, queue, n_wide, wide};
-    const StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells,
-                       order, cells_out, window};
+    if (dc.n) {
+        // the record count on the device (a graph-captured chain): the cell budget follows from it
+        n = *dc.n;
+        if (!order) {
+            const uint64_t b = n / budget_div;
+            max_cells = (uint32_t)(b < STREAM_MIN_CELLS ? STREAM_MIN_CELLS : b > STREAM_MAX_CELLS ? STREAM_MAX_CELLS : b);
+        }
+    }
+    StreamArgs A{smat, P->gap_extend, P->gap_open + P->gap_extend, P->gapped_cutoff, n, geo, out, max_cells,
+                 order, cells_out, window};
+    if (dc.n_front) {
+        A.n_front = *dc.n_front;
+        A.order_end = dc.order_end;
+    }
     const unsigned long long cells = prelim_stream_thread<U>(A, env);
     if (cells) atomicAdd(cells_total, cells);
 }
@@ -2064,15 +2086,17 @@ size_t prelim_geo_bytes() { return sizeof(PrelimGeo); }
 
 cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
-                               void* geo, int sms, cudaStream_t st) {
+                               void* geo, int sms, cudaStream_t st, const unsigned int* n_dev) {
     if (!n) return cudaSuccess;
-    k_prelim_prep<<<grid_for(n, 256, 8, sms), 256, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, (PrelimGeo*)geo);
+    k_prelim_prep<<<grid_for(n, 256, 8, sms), 256, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, (PrelimGeo*)geo,
+                                                            n_dev);
     return cudaGetLastError();
 }
 
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
                                  unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
-                                 const uint32_t* order, uint32_t* cells_out, bool plain, const StreamLaunch& cfg) {
+                                 const uint32_t* order, uint32_t* cells_out, bool plain, const StreamLaunch& cfg,
+                                 StreamDevCounts dc) {
     if (!n) return cudaSuccess;
     const uint64_t want = (n + STREAM_BLOCK - 1) / STREAM_BLOCK;
     const int bps = cfg.blocks_per_sm < 1 ? 1 : cfg.blocks_per_sm > STREAM_BLOCKS_PER_SM ? STREAM_BLOCKS_PER_SM
@@ -2080,7 +2104,8 @@ cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo
     const uint64_t cap = (uint64_t)sms * bps;
     const int grid = (int)(want < cap ? want : cap);
     // the record queue counter sits after the overflow count in n_wide (zeroed by the caller)
-    const uint64_t budget = n / (uint64_t)(cfg.budget_div > 0 ? cfg.budget_div : 128);
+    const uint32_t bdiv = (uint32_t)(cfg.budget_div > 0 ? cfg.budget_div : 128);
+    const uint64_t budget = n / bdiv;
     // with the records in descending predicted cost the long ones start first: the full budget
     const uint32_t max_cells = order ? STREAM_MAX_CELLS
                                      : (uint32_t)(budget < STREAM_MIN_CELLS ? STREAM_MIN_CELLS
@@ -2092,10 +2117,12 @@ cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo
         if (plain) /* one record per thread, the whole grid at once */                                           \
             k_prelim_stream<U, false><<<(unsigned)want, STREAM_BLOCK, 0, st>>>(P, n, g, out, wide, n_wide,       \
                                                                                n_wide + 1, cells, max_cells,     \
-                                                                               order, cells_out, window);        \
+                                                                               order, cells_out, window, dc,     \
+                                                                               bdiv);                            \
         else                                                                                                     \
             k_prelim_stream<U, true><<<grid, STREAM_BLOCK, 0, st>>>(P, n, g, out, wide, n_wide, n_wide + 1,      \
-                                                                    cells, max_cells, order, cells_out, window); \
+                                                                    cells, max_cells, order, cells_out, window,  \
+                                                                    dc, bdiv);                                   \
     } while (0)
     // groups of cell steps between row-end blocks: smaller groups run more row-end blocks, larger
     // ones leave lanes idle longer (8 was the B200 hand sweep's best on the genome workloads)
@@ -2119,8 +2146,10 @@ size_t sched_order_scratch_bytes() { return 3 * SCHED_BINS * sizeof(unsigned int
 // The front of the front-loaded order: the lowest cost bin b such that the records in bins >= b
 // are at most n / SCHED_FRONT_DIV (SCHED_BINS when even the costliest bin holds more).
 constexpr uint64_t SCHED_FRONT_DIV = 32;
-__global__ void k_sched_cut(const unsigned int* __restrict__ hist, uint64_t n, unsigned int* __restrict__ cut) {
+__global__ void k_sched_cut(const unsigned int* __restrict__ hist, uint64_t n, unsigned int* __restrict__ cut,
+                            const unsigned int* __restrict__ n_dev) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (n_dev) n = *n_dev;
     const uint64_t limit = n / SCHED_FRONT_DIV;
     uint64_t acc = 0;
     unsigned int c = SCHED_BINS;
@@ -2135,21 +2164,27 @@ __global__ void k_sched_cut(const unsigned int* __restrict__ hist, uint64_t n, u
 struct SchedFront {
     const float* pred;
     const unsigned int* cut;
-    __host__ __device__ bool operator()(const uint32_t& i) const { return sched_bin(pred[i]) >= *cut; }
+    const unsigned int* n_dev;  // records past the device count are never at the front
+    __host__ __device__ bool operator()(const uint32_t& i) const {
+        return (!n_dev || i < *n_dev) && sched_bin(pred[i]) >= *cut;
+    }
 };
+
+const unsigned int* sched_front_count(const void* scratch) { return (const unsigned int*)scratch + SCHED_BINS + 1; }
 
 size_t sched_front_temp_bytes(uint64_t n) {
     size_t tb = 0;
     thrust::counting_iterator<uint32_t> it(0);
     cub::DevicePartition::If(nullptr, tb, it, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)n,
-                             SchedFront{nullptr, nullptr});
+                             SchedFront{nullptr, nullptr, nullptr});
     return tb;
 }
 
 cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                const uint32_t* pair_hits, const float* params, float* pred, void* scratch,
-                               uint32_t* order, int sms, cudaStream_t st, int layout, void* temp, size_t temp_bytes) {
+                               uint32_t* order, int sms, cudaStream_t st, int layout, void* temp, size_t temp_bytes,
+                               const unsigned int* n_dev) {
     if (!n) return cudaSuccess;
     unsigned int* hist = (unsigned int*)scratch;
     cudaError_t e = cudaMemsetAsync(hist, 0, SCHED_BINS * sizeof(unsigned int), st);
@@ -2157,15 +2192,16 @@ cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevPa
     const uint64_t warps = (n + 31) / 32;
     const int grid = (int)std::min<uint64_t>((warps + SCHED_BLOCK / 32 - 1) / (SCHED_BLOCK / 32), (uint64_t)sms * 8);
     k_sched_predict<<<grid, SCHED_BLOCK, 0, st>>>(L, Q, P, n, idx, hits, hit_pair, ub, pair_hits, nullptr, params, pred,
-                                                  hist);
+                                                  hist, n_dev);
     if (layout == 1) {
         // front-loaded: the predicted-costliest records (about n / 32) first, in arrival order, then
         // the rest in reverse arrival order -- neighbouring records keep sharing their sequences
         unsigned int* cut = hist + SCHED_BINS;
-        k_sched_cut<<<1, 1, 0, st>>>(hist, n, cut);
+        k_sched_cut<<<1, 1, 0, st>>>(hist, n, cut, n_dev);
         thrust::counting_iterator<uint32_t> it(0);
         unsigned int* n_front = hist + SCHED_BINS + 1;
-        e = cub::DevicePartition::If(temp, temp_bytes, it, order, n_front, (int64_t)n, SchedFront{pred, cut}, st);
+        e = cub::DevicePartition::If(temp, temp_bytes, it, order, n_front, (int64_t)n, SchedFront{pred, cut, n_dev},
+                                     st);
         if (e != cudaSuccess) return e;
         return cudaGetLastError();
     }
@@ -2183,7 +2219,7 @@ cudaError_t launch_sched_predict_features(uint64_t n, const float* feats, const 
     const uint64_t warps = (n + 31) / 32;
     const int grid = (int)std::min<uint64_t>((warps + SCHED_BLOCK / 32 - 1) / (SCHED_BLOCK / 32), (uint64_t)sms * 8);
     k_sched_predict<<<grid, SCHED_BLOCK, 0, st>>>(DevLib{}, DevQueries{}, nullptr, n, nullptr, nullptr, nullptr, nullptr,
-                                                  nullptr, feats, params, pred, nullptr);
+                                                  nullptr, feats, params, pred, nullptr, nullptr);
     return cudaGetLastError();
 }
 
@@ -2191,29 +2227,31 @@ cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevP
                                 const uint32_t* list, const uint32_t* idx, const SeedHit* hits,
                                 const uint32_t* hit_pair, const UngBox* ub, int4* dres, PrelimOut* out,
                                 uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
-                                cudaStream_t st) {
+                                cudaStream_t st, const unsigned int* n_dev) {
     if (!n_list) return cudaSuccess;
     const int block = 256;
     const uint64_t blocks_wanted = (2ull * n_list + 7) / 8;
     const uint64_t cap = (uint64_t)sms * 8;
     const int grid = (int)(blocks_wanted < cap ? blocks_wanted : cap);
-    k_prelim_warp_dir<PRELIM_RING><<<grid, block, 0, st>>>(L, Q, P, n_list, list, idx, hits, hit_pair, ub, dres, cells);
+    k_prelim_warp_dir<PRELIM_RING><<<grid, block, 0, st>>>(L, Q, P, n_list, list, idx, hits, hit_pair, ub, dres, cells,
+                                                           n_dev);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_prelim_combine<<<(n_list + 127) / 128, 128, 0, st>>>(L, Q, P, n_list, list, idx, hits, hit_pair, ub, dres, out,
-                                                          wide, n_wide);
+                                                          wide, n_wide, n_dev);
     return cudaGetLastError();
 }
 
 cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_wide,
                                const uint32_t* wide, const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair,
                                const UngBox* ub, PrelimOut* out, int2* band_mem, uint64_t band_cap, uint32_t threads,
-                               unsigned long long* cells, unsigned int* failures, cudaStream_t st) {
+                               unsigned long long* cells, unsigned int* failures, cudaStream_t st,
+                               const unsigned int* n_dev) {
     if (!n_wide) return cudaSuccess;
     const int block = 128;
     const int grid = (int)((threads + block - 1) / block);
     k_prelim_wide<<<grid, block, 0, st>>>(L, Q, P, n_wide, wide, idx, hits, hit_pair, ub, out, band_mem, band_cap, cells,
-                                          failures);
+                                          failures, n_dev);
     return cudaGetLastError();
 }
 
@@ -2249,19 +2287,21 @@ struct U64Add {
 __global__ void k_gather_survivors(uint32_t n, const uint32_t* __restrict__ sel, const uint32_t* __restrict__ idx,
                                    const SeedHit* __restrict__ hits, const uint32_t* __restrict__ hit_pair,
                                    const UngBox* __restrict__ ub, const PrelimOut* __restrict__ po,
-                                   SurvivorRec* __restrict__ out) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const uint32_t t = sel[k];
-    const uint32_t i = idx[t];
-    out[k] = SurvivorRec{hit_pair[i], hits[i], ub[i], po[t]};
+                                   SurvivorRec* __restrict__ out, const unsigned int* __restrict__ n_dev) {
+    if (n_dev) n = min(*n_dev, n);  // the count on the device, n the output's capacity
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t t = sel[k];
+        const uint32_t i = idx[t];
+        out[k] = SurvivorRec{hit_pair[i], hits[i], ub[i], po[t]};
+    }
 }
 
 cudaError_t launch_gather_survivors(uint32_t n, const uint32_t* sel, const uint32_t* idx, const SeedHit* hits,
                                     const uint32_t* hit_pair, const UngBox* ub, const PrelimOut* po,
-                                    SurvivorRec* out, cudaStream_t st) {
+                                    SurvivorRec* out, cudaStream_t st, const unsigned int* n_dev) {
     if (!n) return cudaSuccess;
-    k_gather_survivors<<<(n + 255) / 256, 256, 0, st>>>(n, sel, idx, hits, hit_pair, ub, po, out);
+    const uint32_t blocks = (n + 255) / 256;
+    k_gather_survivors<<<blocks < 4096 ? blocks : 4096, 256, 0, st>>>(n, sel, idx, hits, hit_pair, ub, po, out, n_dev);
     return cudaGetLastError();
 }
 
@@ -2272,7 +2312,10 @@ struct FlagEq {
 };
 struct PrelimPass {
     const PrelimOut* p;
-    __host__ __device__ bool operator()(const uint32_t& i) const { return p[i].score != INT32_MIN; }
+    const unsigned int* n_dev;  // records past the device count are stale
+    __host__ __device__ bool operator()(const uint32_t& i) const {
+        return (!n_dev || i < *n_dev) && p[i].score != INT32_MIN;
+    }
 };
 
 cudaError_t launch_select_eq(const uint8_t* flags, uint64_t n, uint8_t want, uint32_t* out, uint32_t* n_out,
@@ -2282,9 +2325,9 @@ cudaError_t launch_select_eq(const uint8_t* flags, uint64_t n, uint8_t want, uin
 }
 
 cudaError_t launch_select_prelim(const PrelimOut* po, uint64_t n, uint32_t* out, uint32_t* n_out, void* temp,
-                                 size_t& temp_bytes, cudaStream_t st) {
+                                 size_t& temp_bytes, cudaStream_t st, const unsigned int* n_dev) {
     thrust::counting_iterator<uint32_t> it(0);
-    return cub::DeviceSelect::If(temp, temp_bytes, it, out, n_out, (int64_t)n, PrelimPass{po}, st);
+    return cub::DeviceSelect::If(temp, temp_bytes, it, out, n_out, (int64_t)n, PrelimPass{po, n_dev}, st);
 }
 
 cudaError_t launch_offsets(const uint32_t* counts, uint64_t n, uint64_t* offs, void* temp, size_t& temp_bytes,

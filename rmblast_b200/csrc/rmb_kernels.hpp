@@ -49,15 +49,24 @@ bool prelim_stream_eligible(const int32_t* matrix256, int32_t gap_open, int32_t 
 size_t prelim_geo_bytes();
 cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
-                               void* geo, int sms, cudaStream_t st);
+                               void* geo, int sms, cudaStream_t st, const unsigned int* n_dev = nullptr);
 // Launch shape of the thread-per-extension DP (from rmb_tune): group of cell steps between
 // row-end blocks (4, 8, 16), resident blocks per SM, widest band a thread keeps, cell budget divisor.
+// Counts a graph-captured chain keeps on the device: the DP's record count (its cell budget then
+// follows on the device) and, for the front-loaded order, the front's length and the order
+// buffer's length (the records past the front are read from its end).
+struct StreamDevCounts {
+    const unsigned int* n = nullptr;
+    const unsigned int* n_front = nullptr;
+    uint64_t order_end = 0;
+};
 struct StreamLaunch {
     int group = 8, blocks_per_sm = 6, window = 60, budget_div = 128;
 };
 cudaError_t launch_prelim_stream(const DevParams* P, uint64_t n, const void* geo, PrelimOut* out, uint32_t* wide,
                                  unsigned int* n_wide, unsigned long long* cells, int sms, cudaStream_t st,
-                                 const uint32_t* order, uint32_t* cells_out, bool plain, const StreamLaunch& cfg);
+                                 const uint32_t* order, uint32_t* cells_out, bool plain, const StreamLaunch& cfg,
+                                 StreamDevCounts dc = StreamDevCounts{});
 // Learned schedule (rmb_sched.cuh).  Raw features of each record (n x SCHED_NF floats); the
 // network's predicted log1p cells of every record and the records in descending predicted cost
 // (order, for launch_prelim_stream; scratch: sched_order_scratch_bytes()); the network on given
@@ -69,10 +78,12 @@ size_t sched_order_scratch_bytes();
 // layout 1: the predicted-costliest ~1/32 of the records first, the rest after in reverse arrival
 // order (temp: sched_front_temp_bytes(n) bytes); 2: all records in descending predicted cost
 size_t sched_front_temp_bytes(uint64_t n);
+// the front-loaded order's front length, on the device, in launch_sched_order's scratch
+const unsigned int* sched_front_count(const void* scratch);
 cudaError_t launch_sched_order(const DevLib& L, const DevQueries& Q, const DevParams* P, uint64_t n,
                                const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair, const UngBox* ub,
                                const uint32_t* pair_hits, const float* params, float* pred, void* scratch,
-                               uint32_t* order, int sms, cudaStream_t st, int layout, void* temp, size_t temp_bytes);
+                               uint32_t* order, int sms, cudaStream_t st, int layout, void* temp, size_t temp_bytes, const unsigned int* n_dev = nullptr);
 cudaError_t launch_sched_predict_features(uint64_t n, const float* feats, const float* params, float* pred, int sms,
                                           cudaStream_t st);
 // Records `list` (the thread kernel's overflow), one warp per extension; dres holds 2 x n_list
@@ -81,11 +92,11 @@ cudaError_t launch_prelim_split(const DevLib& L, const DevQueries& Q, const DevP
                                 const uint32_t* list, const uint32_t* idx, const SeedHit* hits,
                                 const uint32_t* hit_pair, const UngBox* ub, int4* dres, PrelimOut* out,
                                 uint32_t* wide, unsigned int* n_wide, unsigned long long* cells, int sms,
-                                cudaStream_t st);
+                                cudaStream_t st, const unsigned int* n_dev = nullptr);
 cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n_wide,
                                const uint32_t* wide, const uint32_t* idx, const SeedHit* hits, const uint32_t* hit_pair,
                                const UngBox* ub, PrelimOut* out, int2* band_mem, uint64_t band_cap, uint32_t threads,
-                               unsigned long long* cells, unsigned int* failures, cudaStream_t st);
+                               unsigned long long* cells, unsigned int* failures, cudaStream_t st, const unsigned int* n_dev = nullptr);
 cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n, const TbIn* in,
                              TbOut* out, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch, uint64_t per_thread,
                              uint64_t band_cells, uint32_t rows_cap, uint32_t threads, unsigned long long* cells,
@@ -108,13 +119,13 @@ struct SurvivorRec {
 };
 cudaError_t launch_gather_survivors(uint32_t n, const uint32_t* sel, const uint32_t* idx, const SeedHit* hits,
                                     const uint32_t* hit_pair, const UngBox* ub, const PrelimOut* po,
-                                    SurvivorRec* out, cudaStream_t st);
+                                    SurvivorRec* out, cudaStream_t st, const unsigned int* n_dev = nullptr);
 // flags[i] == want  ->  out list of i (order kept); returns the count through *n_out (device).
 cudaError_t launch_select_eq(const uint8_t* flags, uint64_t n, uint8_t want, uint32_t* out, uint32_t* n_out,
                              void* temp, size_t& temp_bytes, cudaStream_t st);
 // prelim score != INT32_MIN -> list of positions.
 cudaError_t launch_select_prelim(const PrelimOut* po, uint64_t n, uint32_t* out, uint32_t* n_out, void* temp,
-                                 size_t& temp_bytes, cudaStream_t st);
+                                 size_t& temp_bytes, cudaStream_t st, const unsigned int* n_dev = nullptr);
 // exclusive sum of counts[0..n) into offs[0..n] (offs[n] = total).
 cudaError_t launch_offsets(const uint32_t* counts, uint64_t n, uint64_t* offs, void* temp, size_t& temp_bytes,
                            cudaStream_t st);

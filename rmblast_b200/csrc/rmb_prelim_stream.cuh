@@ -89,6 +89,10 @@ struct StreamArgs {
     const uint32_t* order = nullptr;  // queue position -> record (a cost order); null: FIFO
     uint32_t* cells_out = nullptr;    // per-record DP cells (UINT32_MAX: passed on), or null
     uint32_t window = STREAM_WINDOW;  // widest band window kept by the thread (<= STREAM_WINDOW)
+    // a front-loaded order: queue positions below n_front read order[p], the others read the
+    // order from its end (order[order_end - 1 - (p - n_front)]), where a partition left them
+    uint32_t n_front = 0xFFFFFFFFu;
+    uint64_t order_end = 0;
 };
 
 // floor(num / d) for 0 <= num <= 8000 and 1 <= d <= 8000: num * ceil(2^32 / d) >> 32 (exact for
@@ -293,7 +297,9 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                 if (phase == 0) {
                     // next record
                     if (next_t >= A.n) { out_of_records = true; break; }
-                    t = A.order ? A.order[next_t] : next_t;
+                    t = !A.order ? next_t
+                        : next_t < A.n_front ? A.order[next_t]
+                                             : A.order[A.order_end - 1 - (uint64_t)(next_t - A.n_front)];
                     next_t = env.take();
                     const uint4* gp = reinterpret_cast<const uint4*>(A.geo + t);
                     const uint4 g0 = gp[0], g1 = gp[1], g2 = gp[2];

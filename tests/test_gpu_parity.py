@@ -557,7 +557,7 @@ def test_config0_full_size_matches_oracle():
 
 def test_config1_full_size_matches_oracle():
     """Config 1 at its full size: all 1,000 chunks of 60 kb (60 Mb) against the 2,000-consensus
-    library, word 11, through the batched pipeline (two lanes, tuned defaults); every one of the
+    library, word 11, through the batched pipeline (tuned defaults, the device chain as a graph); every one of the
     ~25,000 lines against the oracle (about a minute on 16 host cores)."""
     txt, want, res, ctr = _config_case("plain", 1.0)
     assert txt.count("\n") > 20000
@@ -601,7 +601,8 @@ def test_plain_pipeline_matches_oracle(name, scale):
 def test_tune_knobs_leave_output_unchanged(name, scale):
     """The launch knobs (rmb_tune) shape only how the work is laid out: extreme settings of each,
     both dedup paths (the fused bucket-parallel dedup-extension and the extend-then-dedup pair),
-    one and two pipeline lanes, and the autotuner's pick give the oracle's text byte for byte."""
+    one and two pipeline lanes, the device chain as a graph or stage by stage, and the
+    autotuner's pick give the oracle's text byte for byte."""
     qf, dbf, p = synthetic(name, scale, synth.RM_FLAGS)
     s = searcher(p, synth.MATRIX_TEXT, synth.MATRIX_NAME, dbf)
     recs = api.read_fasta(qf)
@@ -612,8 +613,9 @@ def test_tune_knobs_leave_output_unchanged(name, scale):
     default = s.tune()
     assert s.search(enc, ids).tabular(FIELDS) == want
     for knobs in (dict(prelim_group=4), dict(prelim_group=16), dict(prelim_window=16, prelim_budget_div=16),
-                  dict(prelim_blocks_per_sm=1, ungapped_blocks_per_sm=1), dict(prelim_budget_div=4096), dict(lanes=1),
-                  dict(dedup_extend_hits_per_pair=0), dict(dedup_extend_hits_per_pair=-1)):
+                  dict(prelim_blocks_per_sm=1, ungapped_blocks_per_sm=1), dict(prelim_budget_div=4096), dict(lanes=2),
+                  dict(graph=0), dict(graph=2), dict(graph=0, lanes=2), dict(dedup_extend_hits_per_pair=0),
+                  dict(dedup_extend_hits_per_pair=-1)):
         s.set_tune(dict(default, **knobs))
         assert s.search(enc, ids).tabular(FIELDS) == want, knobs
     s.set_tune(default)
