@@ -400,7 +400,7 @@ void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_
         CK(cudaMemsetAsync(W.fails.p, 0, 16, st));
         rec(0);
         if (fused) {
-            CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut, pair0, npairs, W.offs.as<uint64_t>(),
+            CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut, pair0, npairs, nh, W.offs.as<uint64_t>(),
                                    W.hits.as<SeedHit>(), W.ub.as<UngBox>(), W.flags.as<uint8_t>(), W.dd_cells.p,
                                    W.ung_queue.as<unsigned long long>(), C.sms, st));
         } else {
@@ -790,7 +790,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 W.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
                 W.ung_queue.ensure(16);
                 ev.start(st);
-                CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], pair0, npairs,
+                CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], pair0, npairs, nh,
                                        W.offs.as<uint64_t>(), W.hits.as<SeedHit>(), W.ub.as<UngBox>(),
                                        W.flags.as<uint8_t>(), W.dd_cells.p, W.ung_queue.as<unsigned long long>(),
                                        C.sms, st));

@@ -460,15 +460,92 @@ __global__ void __launch_bounds__(128) k_dedup(DevLib L, DevQueries Q, int32_t w
 // in its order per bucket, with the buckets in parallel: for hit-dense pairs (an all-against-
 // all search keeps ~1% of its hits), where extending every hit first wastes most of the work.
 constexpr int DDX_WARPS = 8;
+// a pass whose admitted hits are at most this many extends them one after another with the whole
+// warp (ung_walk_warp); more run one a lane (UngWalk)
+constexpr int DDX_COOP = 6;
 
-__global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQueries Q,
+// Warp-cooperative ungapped X-drop extension: UngWalk's result (left walk, then right walk), 32
+// bases a round.  Every lane calls it with the same arguments and gets the same result.  A round
+// scores 32 consecutive bases and forms the running sum P of the walk and its running maximum M
+// with warp scans.  The sequential walk's sum is P - M_before (M_before: M up to the previous
+// base), so it banks where P > M_before, and it stops at the first base that is past a sequence
+// end or has code 15 on either side, or where it does not bank and P - M_before < xc: xc is
+// -xdrop on the left, and on the right -xdrop until the first bank, then
+// max(-(left score + M_before), -xdrop).  The last bank before the stop is the extension's end,
+// and M_before at the stop its gain.
+__device__ __forceinline__ void ung_walk_warp(const uint8_t* __restrict__ qb, const uint8_t* __restrict__ sb, int32_t qlen,
+                              int32_t slen, int32_t wq, int32_t wsx, int32_t xdrop, const int32_t* mat, int32_t& score,
+                              int32_t& q_beg, int32_t& q_end) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int32_t x = -xdrop;
+    int32_t score0 = 0;
+#pragma unroll 1
+    for (int dir = -1; dir <= 1; dir += 2) {
+        const int32_t q0 = dir < 0 ? wq - 1 : wq, s0 = dir < 0 ? wsx - 1 : wsx;
+        int32_t P = 0, M = 0, best = wq, gain = 0;
+#pragma unroll 1
+        for (int32_t base = 0;; base += 32) {
+            const int32_t qj = q0 + dir * (base + lane), sj = s0 + dir * (base + lane);
+            bool hard = dir < 0 ? (qj < 0 || sj < 0) : (qj >= qlen || sj >= slen);
+            int32_t d = 0;
+            if (!hard) {
+                const uint8_t a = qb[1 + qj], c = sb[1 + sj];
+                hard = a == 15 || c == 15;
+                if (!hard) d = mat[((a & 15) << 4) | (c & 15)];
+            }
+            int32_t p = d;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t v = __shfl_up_sync(FULL, p, o);
+                if (lane >= o) p += v;
+            }
+            p += P;
+            int32_t mx = p;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t v = __shfl_up_sync(FULL, mx, o);
+                if (lane >= o) mx = max(mx, v);
+            }
+            mx = max(mx, M);
+            int32_t mprev = __shfl_up_sync(FULL, mx, 1);
+            if (lane == 0) mprev = M;
+            const bool bank = !hard && p > mprev;
+            const int32_t xc = dir < 0 || mprev <= 0 ? x : max(-(score0 + mprev), x);
+            const bool stop = hard || (!bank && p - mprev < xc);
+            const unsigned sm = __ballot_sync(FULL, stop);
+            const int f = sm ? __ffs((int)sm) - 1 : 32;
+            const unsigned bm = __ballot_sync(FULL, bank) & (f == 32 ? FULL : ((1u << f) - 1u));
+            if (bm) {
+                const int32_t ql = q0 + dir * (base + (31 - __clz((int)bm)));
+                best = dir < 0 ? ql : ql + 1;
+            }
+            if (f < 32) {
+                gain = __shfl_sync(FULL, mprev, f);
+                break;
+            }
+            P = __shfl_sync(FULL, p, 31);
+            M = __shfl_sync(FULL, mx, 31);
+        }
+        if (dir < 0) {
+            q_beg = best;
+            score0 = gain;
+        } else {
+            q_end = best;
+            score = score0 + gain;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, DevQueries Q,
                                                                  const DevParams* __restrict__ P, int32_t ucut,
                                                                  uint64_t pair0, uint64_t n_pairs,
                                                                  const uint64_t* __restrict__ offs,
                                                                  const SeedHit* __restrict__ hits,
                                                                  UngBox* __restrict__ ub, uint8_t* __restrict__ flags,
                                                                  DiagCell* __restrict__ cells,
-                                                                 unsigned long long* __restrict__ queue) {
+                                                                 unsigned long long* __restrict__ queue,
+                                                                 uint32_t glog) {
     __shared__ int32_t mat[256];
     __shared__ uint32_t heads[DDX_WARPS][512];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
@@ -477,12 +554,15 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
     const int lane = threadIdx.x & 31;
     uint32_t* hd = heads[threadIdx.x >> 5];
     const int32_t ws = P->word_size, xdrop = P->xdrop_ungap, window = 1 - ws;
-    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t gmask = (1u << glog) - 1u;
     for (;;) {
-        unsigned long long w = 0;
-        if (lane == 0) w = atomicAdd(queue, 1ull);
-        w = __shfl_sync(FULL, w, 0);
-        if (w >= n_pairs) break;
+        // a unit: one pair's hits in the buckets of one group (bucket & gmask)
+        unsigned long long u_id = 0;
+        if (lane == 0) u_id = atomicAdd(queue, 1ull);
+        u_id = __shfl_sync(FULL, u_id, 0);
+        if (u_id >= (n_pairs << glog)) break;
+        const uint64_t w = u_id >> glog;
+        const uint32_t grp = (uint32_t)u_id & gmask;
         const uint64_t b = offs[w], e = offs[w + 1];
         if (b == e) continue;
         const uint64_t pair = pair0 + w;
@@ -492,13 +572,12 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
         const uint8_t* qf = Q.q + Q.off[qi];
         const uint8_t* qr = Q.qrc + Q.off[qi];
         const uint8_t* sp = L.plus + L.plus_off[si];
-        DiagCell* pool = cells + b;  // at most one cell per hit of the pair
+        DiagCell* pool = cells + b;  // hit i's cell, if it inserts one, is pool[i - b]
         for (int k = lane; k < 512; k += 32) hd[k] = 0;
         __syncwarp();
-        uint32_t occ = 0;  // cells used, the same on every lane
         for (uint64_t r = b; r < e; r += 32) {
             const uint64_t i = r + (uint64_t)lane;
-            const bool have = i < e;
+            bool have = i < e;
             SeedHit h{0, 0};
             int32_t diag = 0;
             uint32_t key = 0, bk = 512u + (uint32_t)lane;  // lanes without a hit: a bucket of their own
@@ -513,6 +592,10 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
                     key = slen - so - (uint32_t)lw;
                 }
                 bk = diag_bucket(diag);
+                if ((bk & gmask) != grp) {  // another unit's bucket
+                    have = false;
+                    bk = 512u + (uint32_t)lane;
+                }
             }
             const unsigned same = __match_any_sync(FULL, bk);
             // Passes over the round's pending hits.  Each looks its diagonal up in the chains as
@@ -545,7 +628,30 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
                     }
                 }
                 UngBox u{};
-                if (ext) {
+                int32_t sc = 0;
+                uint32_t a0 = 0, a1 = 0, c0 = 0, c1 = 0;
+                const unsigned em = __ballot_sync(FULL, ext);
+                if (em && __popc(em) <= DDX_COOP) {
+                    // few extensions: each with the whole warp, one after another
+                    for (unsigned m = em; m; m &= m - 1u) {
+                        const int src = __ffs((int)m) - 1;
+                        const uint32_t hqs = __shfl_sync(FULL, h.qs, src), hs = __shfl_sync(FULL, h.s, src);
+                        const bool minus = hqs >> 31;
+                        const int32_t qo = (int32_t)(hqs & 0x7fffffffu), so = (int32_t)hs;
+                        const int32_t wq = minus ? (int32_t)qlen - 1 - qo : qo;
+                        const int32_t wsx = minus ? (int32_t)slen - 1 - so : so;
+                        int32_t s_, qb_, qe_;
+                        ung_walk_warp(minus ? qr : qf, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_,
+                                      qe_);
+                        if (lane == src) {
+                            sc = s_;
+                            a0 = (uint32_t)qb_;
+                            a1 = (uint32_t)qe_;
+                            c0 = (uint32_t)(wsx - (wq - qb_));
+                            c1 = (uint32_t)(wsx + (qe_ - wq));
+                        }
+                    }
+                } else if (ext) {
                     const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
                     UngWalk walk;
                     if (!(h.qs >> 31)) walk.start(qf, sp, (int32_t)qlen, (int32_t)slen, qo, so, xdrop);
@@ -553,9 +659,9 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
                                     (int32_t)slen - 1 - so, xdrop);
                     while (walk.step(mat) != 2) {
                     }
-                    int32_t sc;
-                    uint32_t a0, a1, c0, c1;
                     walk.result(sc, a0, a1, c0, c1);
+                }
+                if (ext) {
                     u.score = sc;
                     if (!(h.qs >> 31)) {
                         u.q_start = a0; u.q_end = a1; u.s_start = c0; u.s_end = c1;
@@ -576,13 +682,11 @@ __global__ void __launch_bounds__(DDX_WARPS * 32) k_dedup_extend(DevLib L, DevQu
                         if ((int32_t)(key - cl.level) > window) { cl.diag = diag; cl.level = u.store; append = false; break; }
                     }
                 }
-                const unsigned nn = __ballot_sync(FULL, append);
                 if (append) {
-                    const uint32_t idx = occ + (uint32_t)__popc(nn & lt) + 1u;
+                    const uint32_t idx = (uint32_t)(i - b) + 1u;
                     pool[idx - 1] = DiagCell{diag, u.store, head};
                     hd[bk] = idx;
                 }
-                occ += (uint32_t)__popc(nn);
                 __syncwarp();  // this pass's chain updates before the next pass reads them
             }
         }
@@ -2043,16 +2147,21 @@ cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32
 
 size_t diag_cell_bytes() { return sizeof(DiagCell); }
 cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
-                                uint64_t pair0, uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits,
-                                UngBox* ub, uint8_t* flags, void* cells, unsigned long long* queue, int sms,
-                                cudaStream_t st) {
+                                uint64_t pair0, uint64_t n_pairs, uint64_t n_hits, const uint64_t* offs,
+                                const SeedHit* hits, UngBox* ub, uint8_t* flags, void* cells,
+                                unsigned long long* queue, int sms, cudaStream_t st) {
     if (!n_pairs) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    const uint64_t want = (n_pairs + DDX_WARPS - 1) / DDX_WARPS;
+    // few pairs with many hits each (one genome against a small library): each pair's buckets
+    // split into 2^glog groups, one warp a group, until the grid's warps have work
+    uint32_t glog = 0;
+    while (glog < 5 && (n_pairs << glog) < (uint64_t)sms * 48 && n_hits / (n_pairs << glog) >= 1024) ++glog;
+    const uint64_t units = n_pairs << glog;
+    const uint64_t want = (units + DDX_WARPS - 1) / DDX_WARPS;
     const uint64_t cap = (uint64_t)sms * 8;
     k_dedup_extend<<<(unsigned)(want < cap ? want : cap), DDX_WARPS * 32, 0, st>>>(
-        L, Q, P, ucut, pair0, n_pairs, offs, hits, ub, flags, (DiagCell*)cells, queue);
+        L, Q, P, ucut, pair0, n_pairs, offs, hits, ub, flags, (DiagCell*)cells, queue, glog);
     return cudaGetLastError();
 }
 

@@ -30,9 +30,9 @@ uint64_t dedup_threads(int sms);
 // Bucket-parallel diagonal dedup that extends only the hits the hash admits (one warp per pair):
 // flags and boxes as launch_ungapped + launch_dedup give them.
 cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
-                                uint64_t pair0, uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits,
-                                UngBox* ub, uint8_t* flags, void* cells, unsigned long long* queue, int sms,
-                                cudaStream_t st);
+                                uint64_t pair0, uint64_t n_pairs, uint64_t n_hits, const uint64_t* offs,
+                                const SeedHit* hits, UngBox* ub, uint8_t* flags, void* cells,
+                                unsigned long long* queue, int sms, cudaStream_t st);
 size_t diag_cell_bytes();
 cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32_t ucut, uint64_t pair0,
                          uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits, const UngBox* ub, uint8_t* flags,
