@@ -136,6 +136,7 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
     uint8_t a_nx = 0, a0_left = 0, a0_right = 0;
     const int32_t* srow = A.smat;
     uint32_t m = 0, nb = 0, ai = 0, bi = 0, first_b = 0, b_size = 0, last_b = 0, best_a = 0, best_b = 0;
+    uint32_t first_alive = 0xFFFFFFFFu;  // the current row's first live cell
     // scores relative to `origin` (the extension's score 0 until the first rebase)
     int32_t best = 0, prev_best = 0, thr = 0, sc = 0, gap_row = 0, origin = 0;
     // the extension cells of the last row end (gapped.rs:307-319), computed when read: band
@@ -154,7 +155,7 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
         srow = A.smat + (uint32_t)(a_nx & 15) * 16u;
         if (ai + 1 < m) a_nx = abase[(ptrdiff_t)dir * (ptrdiff_t)(ai + 1)];  // next row's residue
         sc = MININT; gap_row = MININT;
-        last_b = first_b; prev_best = best; bi = first_b;
+        last_b = first_b; prev_best = best; bi = first_b; first_alive = 0xFFFFFFFFu;
         rec_cells += b_size - first_b;
     };
     // The residues of the band indices of one aligned word of the column sequence, from the
@@ -197,15 +198,17 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                 const int32_t nxt = cx + srow[w & 15u];
                 const int32_t cell = __vimax3_s32(sc, cy, gap_row);
                 const bool alive = cell >= thr;
-                if (!alive && bi == first_b) ++first_b;
+                if (alive) first_alive = min(first_alive, bi);
                 if (alive) last_b = bi;
                 if (cell > best) best_b = bi;
                 best = max(best, cell);
                 thr = __viaddmax_s32(cell, -xdrop, thr);  // best - xdrop
                 const int32_t open = cell - goe;
-                if (alive) gap_row = __viaddmax_s32(gap_row, -ge, open);
+                // at a dead cell the reference keeps gap_row and the vertical gap; both are then
+                // below the threshold (cell >= each), and so is what is kept here, so they stay dead
+                gap_row = __viaddmax_s32(gap_row, -ge, open);
                 const int32_t ex = alive ? cell : STREAM_FLOOR;
-                const int32_t ey = alive ? __vimax3_s32(cy - ge, open, STREAM_FLOOR) : cy;
+                const int32_t ey = __vimax3_s32(cy - ge, open, STREAM_FLOOR);
                 slot = stream_pack(ex, ey, w);
                 sc = nxt;
                 ++bi;
@@ -217,6 +220,9 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
             // threshold; a MININT sentinel follows while the band has not reached nb.
             if (best > prev_best) best_a = ai + 1;
             ++ai;
+            // the band's first cell: the row's first live cell (gapped.rs:265-268 advance it over
+            // the leading dead ones), b_size when none lived
+            first_b = min(first_alive, b_size);
             const bool empty = first_b >= b_size;
             vlo = last_b + 1;
             uint32_t k = 0;
