@@ -463,6 +463,8 @@ constexpr int DDX_WARPS = 8;
 // a pass whose admitted hits are at most this many extends them one after another with the whole
 // warp (ung_walk_warp); more run one a lane (UngWalk)
 constexpr int DDX_COOP = 6;
+// a pair's hits go to bucket groups of about this many hits each, at most DDX_GMAX groups
+constexpr uint32_t DDX_UNIT_HITS = 8192, DDX_GLOG_MAX = 5, DDX_GMAX = 1u << DDX_GLOG_MAX;
 
 // Warp-cooperative ungapped X-drop extension: UngWalk's result (left walk, then right walk), 32
 // bases a round.  Every lane calls it with the same arguments and gets the same result.  A round
@@ -554,140 +556,158 @@ __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, De
     const int lane = threadIdx.x & 31;
     uint32_t* hd = heads[threadIdx.x >> 5];
     const int32_t ws = P->word_size, xdrop = P->xdrop_ungap, window = 1 - ws;
-    const uint32_t gmask = (1u << glog) - 1u;
+    // A unit is one pair's hits in the buckets of one group (bucket & (G - 1)); a pair with h
+    // hits has G = 2^max(glog, ceil(log2(h / DDX_UNIT_HITS))) groups, at most DDX_GMAX.  Unit
+    // ids run over (group, pair) with the group descending, so the groups of the most split
+    // pairs start first and a hit-heavy pair does not hold the end of the launch; a warp takes 32
+    // ids at a time and runs the ones that exist.
+    const uint64_t n_units = (uint64_t)DDX_GMAX * n_pairs;
     for (;;) {
-        // a unit: one pair's hits in the buckets of one group (bucket & gmask)
-        unsigned long long u_id = 0;
-        if (lane == 0) u_id = atomicAdd(queue, 1ull);
-        u_id = __shfl_sync(FULL, u_id, 0);
-        if (u_id >= (n_pairs << glog)) break;
-        const uint64_t w = u_id >> glog;
-        const uint32_t grp = (uint32_t)u_id & gmask;
-        const uint64_t b = offs[w], e = offs[w + 1];
-        if (b == e) continue;
-        const uint64_t pair = pair0 + w;
-        const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
-        const uint32_t qlen = Q.len[qi], slen = L.len[si];
-        const int32_t lw = Q.lw[qi];
-        const uint8_t* qf = Q.q + Q.off[qi];
-        const uint8_t* qr = Q.qrc + Q.off[qi];
-        const uint8_t* sp = L.plus + L.plus_off[si];
-        DiagCell* pool = cells + b;  // hit i's cell, if it inserts one, is pool[i - b]
-        for (int k = lane; k < 512; k += 32) hd[k] = 0;
-        __syncwarp();
-        for (uint64_t r = b; r < e; r += 32) {
-            const uint64_t i = r + (uint64_t)lane;
-            bool have = i < e;
-            SeedHit h{0, 0};
-            int32_t diag = 0;
-            uint32_t key = 0, bk = 512u + (uint32_t)lane;  // lanes without a hit: a bucket of their own
-            if (have) {
-                h = hits[i];
-                const uint32_t qo = h.qs & 0x7fffffffu, so = h.s;
-                if (!(h.qs >> 31)) {
-                    diag = (int32_t)(so - qo);
-                    key = so;
-                } else {
-                    diag = (int32_t)(slen - 2u * qlen - 1u + (qo - so));
-                    key = slen - so - (uint32_t)lw;
-                }
-                bk = diag_bucket(diag);
-                if ((bk & gmask) != grp) {  // another unit's bucket
-                    have = false;
-                    bk = 512u + (uint32_t)lane;
-                }
-            }
-            const unsigned same = __match_any_sync(FULL, bk);
-            // Passes over the round's pending hits.  Each looks its diagonal up in the chains as
-            // they stand; in each bucket the pending hits before the first one the hash admits are
-            // dropped at once (a dropped hit changes no chain, so the lookups of the ones after it
-            // stay right), the first admitted one is extended and inserted, and the bucket's hits
-            // after it wait for the next pass.  A run of dropped hits on one repeat's diagonal
-            // takes one pass instead of one turn each.
-            bool pending = have;
-            while (__any_sync(FULL, pending)) {
-                uint32_t head = 0;
-                bool admitted = false;
-                if (pending) {
-                    head = hd[bk];
-                    uint32_t last = 0;
-                    for (uint32_t c = head; c; c = pool[c - 1].next)
-                        if (pool[c - 1].diag == diag) { last = pool[c - 1].level; break; }
-                    admitted = key >= last;
-                }
-                const unsigned adm = __ballot_sync(FULL, pending && admitted) & same;
-                const int first = adm ? __ffs((int)adm) - 1 : 32;
-                bool ext = false;
-                if (pending) {
-                    if (lane < first) {
-                        flags[i] = 0;
-                        pending = false;
-                    } else if (lane == first) {
-                        ext = true;
-                        pending = false;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(queue, 32ull);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= n_units) break;
+        const uint64_t id = base + (uint64_t)lane;
+        uint64_t wl = 0;
+        uint32_t gl = glog, gr = 0;
+        bool valid = false;
+        if (id < n_units) {
+            gr = DDX_GMAX - 1u - (uint32_t)(id / n_pairs);
+            wl = id % n_pairs;
+            const uint64_t hp = offs[wl + 1] - offs[wl];
+            while (gl < DDX_GLOG_MAX && hp > ((uint64_t)DDX_UNIT_HITS << gl)) ++gl;
+            valid = hp != 0 && gr < (1u << gl);
+        }
+        for (unsigned vm = __ballot_sync(FULL, valid); vm; vm &= vm - 1u) {
+            const int src = __ffs((int)vm) - 1;
+            const uint64_t w = __shfl_sync(FULL, (unsigned long long)wl, src);
+            const uint32_t grp = __shfl_sync(FULL, gr, src);
+            const uint32_t gmask = (1u << __shfl_sync(FULL, gl, src)) - 1u;
+            const uint64_t b = offs[w], e = offs[w + 1];
+            const uint64_t pair = pair0 + w;
+            const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
+            const uint32_t qlen = Q.len[qi], slen = L.len[si];
+            const int32_t lw = Q.lw[qi];
+            const uint8_t* qf = Q.q + Q.off[qi];
+            const uint8_t* qr = Q.qrc + Q.off[qi];
+            const uint8_t* sp = L.plus + L.plus_off[si];
+            DiagCell* pool = cells + b;  // hit i's cell, if it inserts one, is pool[i - b]
+            for (int k = lane; k < 512; k += 32) hd[k] = 0;
+            __syncwarp();
+            for (uint64_t r = b; r < e; r += 32) {
+                const uint64_t i = r + (uint64_t)lane;
+                bool have = i < e;
+                SeedHit h{0, 0};
+                int32_t diag = 0;
+                uint32_t key = 0, bk = 512u + (uint32_t)lane;  // lanes without a hit: a bucket of their own
+                if (have) {
+                    h = hits[i];
+                    const uint32_t qo = h.qs & 0x7fffffffu, so = h.s;
+                    if (!(h.qs >> 31)) {
+                        diag = (int32_t)(so - qo);
+                        key = so;
+                    } else {
+                        diag = (int32_t)(slen - 2u * qlen - 1u + (qo - so));
+                        key = slen - so - (uint32_t)lw;
+                    }
+                    bk = diag_bucket(diag);
+                    if ((bk & gmask) != grp) {  // another unit's bucket
+                        have = false;
+                        bk = 512u + (uint32_t)lane;
                     }
                 }
-                UngBox u{};
-                int32_t sc = 0;
-                uint32_t a0 = 0, a1 = 0, c0 = 0, c1 = 0;
-                const unsigned em = __ballot_sync(FULL, ext);
-                if (em && __popc(em) <= DDX_COOP) {
-                    // few extensions: each with the whole warp, one after another
-                    for (unsigned m = em; m; m &= m - 1u) {
-                        const int src = __ffs((int)m) - 1;
-                        const uint32_t hqs = __shfl_sync(FULL, h.qs, src), hs = __shfl_sync(FULL, h.s, src);
-                        const bool minus = hqs >> 31;
-                        const int32_t qo = (int32_t)(hqs & 0x7fffffffu), so = (int32_t)hs;
-                        const int32_t wq = minus ? (int32_t)qlen - 1 - qo : qo;
-                        const int32_t wsx = minus ? (int32_t)slen - 1 - so : so;
-                        int32_t s_, qb_, qe_;
-                        ung_walk_warp(minus ? qr : qf, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_,
-                                      qe_);
-                        if (lane == src) {
-                            sc = s_;
-                            a0 = (uint32_t)qb_;
-                            a1 = (uint32_t)qe_;
-                            c0 = (uint32_t)(wsx - (wq - qb_));
-                            c1 = (uint32_t)(wsx + (qe_ - wq));
+                const unsigned same = __match_any_sync(FULL, bk);
+                // Passes over the round's pending hits.  Each looks its diagonal up in the chains as
+                // they stand; in each bucket the pending hits before the first one the hash admits are
+                // dropped at once (a dropped hit changes no chain, so the lookups of the ones after it
+                // stay right), the first admitted one is extended and inserted, and the bucket's hits
+                // after it wait for the next pass.  A run of dropped hits on one repeat's diagonal
+                // takes one pass instead of one turn each.
+                bool pending = have;
+                while (__any_sync(FULL, pending)) {
+                    uint32_t head = 0;
+                    bool admitted = false;
+                    if (pending) {
+                        head = hd[bk];
+                        uint32_t last = 0;
+                        for (uint32_t c = head; c; c = pool[c - 1].next)
+                            if (pool[c - 1].diag == diag) { last = pool[c - 1].level; break; }
+                        admitted = key >= last;
+                    }
+                    const unsigned adm = __ballot_sync(FULL, pending && admitted) & same;
+                    const int first = adm ? __ffs((int)adm) - 1 : 32;
+                    bool ext = false;
+                    if (pending) {
+                        if (lane < first) {
+                            flags[i] = 0;
+                            pending = false;
+                        } else if (lane == first) {
+                            ext = true;
+                            pending = false;
                         }
                     }
-                } else if (ext) {
-                    const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
-                    UngWalk walk;
-                    if (!(h.qs >> 31)) walk.start(qf, sp, (int32_t)qlen, (int32_t)slen, qo, so, xdrop);
-                    else walk.start(qr, sp, (int32_t)qlen, (int32_t)slen, (int32_t)qlen - 1 - qo,
-                                    (int32_t)slen - 1 - so, xdrop);
-                    while (walk.step(mat) != 2) {
+                    UngBox u{};
+                    int32_t sc = 0;
+                    uint32_t a0 = 0, a1 = 0, c0 = 0, c1 = 0;
+                    const unsigned em = __ballot_sync(FULL, ext);
+                    if (em && __popc(em) <= DDX_COOP) {
+                        // few extensions: each with the whole warp, one after another
+                        for (unsigned m = em; m; m &= m - 1u) {
+                            const int src = __ffs((int)m) - 1;
+                            const uint32_t hqs = __shfl_sync(FULL, h.qs, src), hs = __shfl_sync(FULL, h.s, src);
+                            const bool minus = hqs >> 31;
+                            const int32_t qo = (int32_t)(hqs & 0x7fffffffu), so = (int32_t)hs;
+                            const int32_t wq = minus ? (int32_t)qlen - 1 - qo : qo;
+                            const int32_t wsx = minus ? (int32_t)slen - 1 - so : so;
+                            int32_t s_, qb_, qe_;
+                            ung_walk_warp(minus ? qr : qf, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_,
+                                          qe_);
+                            if (lane == src) {
+                                sc = s_;
+                                a0 = (uint32_t)qb_;
+                                a1 = (uint32_t)qe_;
+                                c0 = (uint32_t)(wsx - (wq - qb_));
+                                c1 = (uint32_t)(wsx + (qe_ - wq));
+                            }
+                        }
+                    } else if (ext) {
+                        const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
+                        UngWalk walk;
+                        if (!(h.qs >> 31)) walk.start(qf, sp, (int32_t)qlen, (int32_t)slen, qo, so, xdrop);
+                        else walk.start(qr, sp, (int32_t)qlen, (int32_t)slen, (int32_t)qlen - 1 - qo,
+                                        (int32_t)slen - 1 - so, xdrop);
+                        while (walk.step(mat) != 2) {
+                        }
+                        walk.result(sc, a0, a1, c0, c1);
                     }
-                    walk.result(sc, a0, a1, c0, c1);
-                }
-                if (ext) {
-                    u.score = sc;
-                    if (!(h.qs >> 31)) {
-                        u.q_start = a0; u.q_end = a1; u.s_start = c0; u.s_end = c1;
-                        u.store = sc >= ucut ? c1 : h.s + (uint32_t)ws;
-                    } else {
-                        u.q_start = qlen - a1; u.q_end = qlen - a0; u.s_start = slen - c1; u.s_end = slen - c0;
-                        u.store = sc >= ucut ? c1 : key + (uint32_t)ws;
+                    if (ext) {
+                        u.score = sc;
+                        if (!(h.qs >> 31)) {
+                            u.q_start = a0; u.q_end = a1; u.s_start = c0; u.s_end = c1;
+                            u.store = sc >= ucut ? c1 : h.s + (uint32_t)ws;
+                        } else {
+                            u.q_start = qlen - a1; u.q_end = qlen - a0; u.s_start = slen - c1; u.s_end = slen - c0;
+                            u.store = sc >= ucut ? c1 : key + (uint32_t)ws;
+                        }
+                        ub[i] = u;
+                        flags[i] = sc >= ucut ? 3 : 1;
                     }
-                    ub[i] = u;
-                    flags[i] = sc >= ucut ? 3 : 1;
-                }
-                bool append = false;
-                if (ext) {
-                    append = true;
-                    for (uint32_t c = head; c; c = pool[c - 1].next) {
-                        DiagCell& cl = pool[c - 1];
-                        if (cl.diag == diag) { cl.level = u.store; append = false; break; }
-                        if ((int32_t)(key - cl.level) > window) { cl.diag = diag; cl.level = u.store; append = false; break; }
+                    bool append = false;
+                    if (ext) {
+                        append = true;
+                        for (uint32_t c = head; c; c = pool[c - 1].next) {
+                            DiagCell& cl = pool[c - 1];
+                            if (cl.diag == diag) { cl.level = u.store; append = false; break; }
+                            if ((int32_t)(key - cl.level) > window) { cl.diag = diag; cl.level = u.store; append = false; break; }
+                        }
                     }
+                    if (append) {
+                        const uint32_t idx = (uint32_t)(i - b) + 1u;
+                        pool[idx - 1] = DiagCell{diag, u.store, head};
+                        hd[bk] = idx;
+                    }
+                    __syncwarp();  // this pass's chain updates before the next pass reads them
                 }
-                if (append) {
-                    const uint32_t idx = (uint32_t)(i - b) + 1u;
-                    pool[idx - 1] = DiagCell{diag, u.store, head};
-                    hd[bk] = idx;
-                }
-                __syncwarp();  // this pass's chain updates before the next pass reads them
             }
         }
     }
@@ -2153,10 +2173,10 @@ cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevP
     if (!n_pairs) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    // few pairs with many hits each (one genome against a small library): each pair's buckets
-    // split into 2^glog groups, one warp a group, until the grid's warps have work
+    // few pairs with many hits each (one genome against a small library): every pair's buckets
+    // split into at least 2^glog groups, one warp a group, until the grid's warps have work
     uint32_t glog = 0;
-    while (glog < 5 && (n_pairs << glog) < (uint64_t)sms * 48 && n_hits / (n_pairs << glog) >= 1024) ++glog;
+    while (glog < DDX_GLOG_MAX && (n_pairs << glog) < (uint64_t)sms * 48 && n_hits / (n_pairs << glog) >= 1024) ++glog;
     const uint64_t units = n_pairs << glog;
     const uint64_t want = (units + DDX_WARPS - 1) / DDX_WARPS;
     const uint64_t cap = (uint64_t)sms * 8;
