@@ -155,7 +155,7 @@ struct Work {
     DBuf pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo,
         n_wide, band, sel, surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over,
-        tb_ooff, tb_ops2, ung_queue;
+        tb_ooff, tb_ops2, ung_queue, dd_units;
     DBuf sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
     // the device chain as a CUDA graph (chain_graph): its executable, its timing events and the
     // pinned block its counts come back in
@@ -174,7 +174,7 @@ struct Work {
                        &lut_vals2, &lut_counts, &counts, &offs, &hits, &hit_pair, &ub, &flags, &dd_scratch, &dd_cells,
                        &ung_idx, &n_sel, &po, &wide, &wide2, &dres, &geo, &n_wide, &band, &sel, &surv, &cells, &fails,
                        &temp, &tb_in, &tb_out, &tb_ops, &tb_scratch, &stage, &stage_start, &stage_over, &tb_ooff,
-                       &tb_ops2, &ung_queue, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
+                       &tb_ops2, &ung_queue, &dd_units, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
         for (DBuf* b : all) b->release();
         if (st) cudaStreamDestroy(st);
         st = nullptr;
@@ -358,6 +358,7 @@ void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_
     W.dd_cells.ensure(n1 * diag_cell_bytes());
     W.ung_queue.ensure(16);
     if (!fused) W.dd_scratch.ensure(dedup_threads(C.sms) * 1024 * 4);
+    else W.dd_units.ensure(dedup_units_bytes(npairs, nh, C.sms));
     W.ung_idx.ensure(n1 * 4);
     W.n_sel.ensure(16);   // [0] ungapped records, [1] survivors
     W.n_wide.ensure(16);  // [0] records the thread kernel passed on, [1] its queue, [2] those the warp kernel did
@@ -402,7 +403,7 @@ void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_
         if (fused) {
             CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut, pair0, npairs, nh, W.offs.as<uint64_t>(),
                                    W.hits.as<SeedHit>(), W.ub.as<UngBox>(), W.flags.as<uint8_t>(), W.dd_cells.p,
-                                   W.ung_queue.as<unsigned long long>(), C.sms, st));
+                                   W.ung_queue.as<unsigned long long>(), W.dd_units.p, C.sms, st));
         } else {
             CK(launch_ungapped(C.L, Q, C.d_params.as<DevParams>(), ucut, nh, W.hits.as<SeedHit>(),
                                W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), C.sms, st,
@@ -497,7 +498,7 @@ void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_
     ctr.gpu_ms_prelim += ms(1, 5);
     ctr.gpu_ms_prelim_main += ms(2, 3);
     ctr.so_cells_main += main_cells;
-    ctr.launches += (fused ? 1 : 2) + 1 + 1 + (learned ? 3 : 0) + 1 + 2 + 1 + 1;
+    ctr.launches += 2 + 1 + 1 + (learned ? 3 : 0) + 1 + 2 + 1 + 1;
     ctr.ungapped += nu;
     ctr.prelim_dp += nu;
     if (nw > wcap || nw2 || nsv > scap) {
@@ -789,13 +790,14 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 W.flags.ensure(nh + 1);
                 W.dd_cells.ensure(std::max<uint64_t>(nh, 1) * diag_cell_bytes());
                 W.ung_queue.ensure(16);
+                W.dd_units.ensure(dedup_units_bytes(npairs, nh, C.sms));
                 ev.start(st);
                 CK(launch_dedup_extend(C.L, Q, C.d_params.as<DevParams>(), ucut[qb], pair0, npairs, nh,
                                        W.offs.as<uint64_t>(), W.hits.as<SeedHit>(), W.ub.as<UngBox>(),
                                        W.flags.as<uint8_t>(), W.dd_cells.p, W.ung_queue.as<unsigned long long>(),
-                                       C.sms, st));
+                                       W.dd_units.p, C.sms, st));
                 ev.stop(st);
-                ctr.launches += 1;
+                ctr.launches += 2;
             } else {
                 ev.start(st);
                 W.ung_queue.ensure(16);

@@ -539,6 +539,33 @@ __device__ __forceinline__ void ung_walk_warp(const uint8_t* __restrict__ qb, co
     }
 }
 
+// The fused dedup's units: a pair with h > 0 hits gets G = 2^gl groups, gl the smallest at or
+// above glog with h <= DDX_UNIT_HITS << gl (at most DDX_GLOG_MAX).  Pairs with G > 1 list their
+// groups in `heavy` (pair | group << 32 | gl << 40), the others themselves in `light`.
+__global__ void k_dedup_units(uint64_t n_pairs, const uint64_t* __restrict__ offs, uint32_t glog, DedupUnits units) {
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t hp = offs[p + 1] - offs[p];
+        uint32_t gl = glog;
+        while (gl < DDX_GLOG_MAX && hp > ((uint64_t)DDX_UNIT_HITS << gl)) ++gl;
+        const bool light = hp != 0 && gl == 0;
+        const unsigned am = __activemask();
+        const unsigned lm = __ballot_sync(am, light);
+        const int lead = __ffs((int)am) - 1, lane = threadIdx.x & 31;
+        unsigned int lb = 0;
+        if (lane == lead && lm) lb = atomicAdd(&units.counts[1], (unsigned)__popc(lm));
+        lb = __shfl_sync(am, lb, lead);
+        if (light) units.light[lb + __popc(lm & ((1u << lane) - 1u))] = (uint32_t)p;
+        if (hp != 0 && gl > 0) {
+            const unsigned int hb = atomicAdd(&units.counts[0], 1u << gl);
+            for (uint32_t g = 0; g < (1u << gl); ++g)
+                if (hb + g < units.heavy_cap)  // never false: heavy_cap bounds the sum of the G
+                    units.heavy[hb + g] = (unsigned long long)p | ((unsigned long long)g << 32) |
+                                          ((unsigned long long)gl << 40);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, DevQueries Q,
                                                                  const DevParams* __restrict__ P, int32_t ucut,
                                                                  uint64_t pair0, uint64_t n_pairs,
@@ -547,7 +574,7 @@ __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, De
                                                                  UngBox* __restrict__ ub, uint8_t* __restrict__ flags,
                                                                  DiagCell* __restrict__ cells,
                                                                  unsigned long long* __restrict__ queue,
-                                                                 uint32_t glog) {
+                                                                 DedupUnits units) {
     __shared__ int32_t mat[256];
     __shared__ uint32_t heads[DDX_WARPS][512];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
@@ -556,33 +583,27 @@ __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, De
     const int lane = threadIdx.x & 31;
     uint32_t* hd = heads[threadIdx.x >> 5];
     const int32_t ws = P->word_size, xdrop = P->xdrop_ungap, window = 1 - ws;
-    // A unit is one pair's hits in the buckets of one group (bucket & (G - 1)); a pair with h
-    // hits has G = 2^max(glog, ceil(log2(h / DDX_UNIT_HITS))) groups, at most DDX_GMAX.  Unit
-    // ids run over (group, pair) with the group descending, so the groups of the most split
-    // pairs start first and a hit-heavy pair does not hold the end of the launch; a warp takes 32
-    // ids at a time and runs the ones that exist.
-    const uint64_t n_units = (uint64_t)DDX_GMAX * n_pairs;
+    // A unit is one pair's hits in the buckets of one group (bucket & (G - 1)).  The units of the
+    // pairs split into groups come first (units.heavy, a pair's groups one after another), then
+    // one unit for each other pair with hits (units.light), so a hit-heavy pair's groups start
+    // early and run side by side instead of holding the end of the launch.
+    const unsigned int n_heavy = units.counts[0], n_units = n_heavy + units.counts[1];
     for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(queue, 32ull);
-        base = __shfl_sync(FULL, base, 0);
-        if (base >= n_units) break;
-        const uint64_t id = base + (uint64_t)lane;
-        uint64_t wl = 0;
-        uint32_t gl = glog, gr = 0;
-        bool valid = false;
-        if (id < n_units) {
-            gr = DDX_GMAX - 1u - (uint32_t)(id / n_pairs);
-            wl = id % n_pairs;
-            const uint64_t hp = offs[wl + 1] - offs[wl];
-            while (gl < DDX_GLOG_MAX && hp > ((uint64_t)DDX_UNIT_HITS << gl)) ++gl;
-            valid = hp != 0 && gr < (1u << gl);
+        unsigned long long u_id = 0;
+        if (lane == 0) u_id = atomicAdd(queue, 1ull);
+        u_id = __shfl_sync(FULL, u_id, 0);
+        if (u_id >= n_units) break;
+        uint64_t w;
+        uint32_t grp = 0, gmask = 0;
+        if (u_id < n_heavy) {
+            const unsigned long long v = units.heavy[u_id];
+            w = (uint32_t)v;
+            grp = (uint32_t)(v >> 32) & 0xffu;
+            gmask = (1u << ((uint32_t)(v >> 40) & 0xffu)) - 1u;
+        } else {
+            w = units.light[u_id - n_heavy];
         }
-        for (unsigned vm = __ballot_sync(FULL, valid); vm; vm &= vm - 1u) {
-            const int src = __ffs((int)vm) - 1;
-            const uint64_t w = __shfl_sync(FULL, (unsigned long long)wl, src);
-            const uint32_t grp = __shfl_sync(FULL, gr, src);
-            const uint32_t gmask = (1u << __shfl_sync(FULL, gl, src)) - 1u;
+        {
             const uint64_t b = offs[w], e = offs[w + 1];
             const uint64_t pair = pair0 + w;
             const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
@@ -2166,22 +2187,45 @@ cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32
 }
 
 size_t diag_cell_bytes() { return sizeof(DiagCell); }
-cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
-                                uint64_t pair0, uint64_t n_pairs, uint64_t n_hits, const uint64_t* offs,
-                                const SeedHit* hits, UngBox* ub, uint8_t* flags, void* cells,
-                                unsigned long long* queue, int sms, cudaStream_t st) {
-    if (!n_pairs) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
-    if (e != cudaSuccess) return e;
+uint32_t dedup_glog(uint64_t n_pairs, uint64_t n_hits, int sms) {
     // few pairs with many hits each (one genome against a small library): every pair's buckets
     // split into at least 2^glog groups, one warp a group, until the grid's warps have work
     uint32_t glog = 0;
-    while (glog < DDX_GLOG_MAX && (n_pairs << glog) < (uint64_t)sms * 48 && n_hits / (n_pairs << glog) >= 1024) ++glog;
+    while (glog < DDX_GLOG_MAX && n_pairs && (n_pairs << glog) < (uint64_t)sms * 48 &&
+           n_hits / (n_pairs << glog) >= 1024)
+        ++glog;
+    return glog;
+}
+
+size_t dedup_units_bytes(uint64_t n_pairs, uint64_t n_hits, int sms) {
+    // a pair split past glog has G < 2 h / DDX_UNIT_HITS, so the groups of all pairs with G > 1
+    // number at most n_pairs 2^glog + 2 n_hits / DDX_UNIT_HITS
+    const uint64_t heavy = (n_pairs << dedup_glog(n_pairs, n_hits, sms)) + n_hits / (DDX_UNIT_HITS / 2) + 1;
+    return 16 + heavy * 8 + n_pairs * 4 + 16;
+}
+
+cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
+                                uint64_t pair0, uint64_t n_pairs, uint64_t n_hits, const uint64_t* offs,
+                                const SeedHit* hits, UngBox* ub, uint8_t* flags, void* cells,
+                                unsigned long long* queue, void* units_buf, int sms, cudaStream_t st) {
+    if (!n_pairs) return cudaSuccess;
+    const uint32_t glog = dedup_glog(n_pairs, n_hits, sms);
+    const uint64_t heavy_cap = (n_pairs << glog) + n_hits / (DDX_UNIT_HITS / 2) + 1;
+    DedupUnits du;
+    du.counts = (unsigned int*)units_buf;
+    du.heavy = (unsigned long long*)((char*)units_buf + 16);
+    du.light = (uint32_t*)(du.heavy + heavy_cap);
+    du.heavy_cap = heavy_cap;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(du.counts, 0, 16, st);
+    if (e != cudaSuccess) return e;
+    const uint64_t bb = (n_pairs + 255) / 256;
+    k_dedup_units<<<(unsigned)(bb < 4096 ? bb : 4096), 256, 0, st>>>(n_pairs, offs, glog, du);
     const uint64_t units = n_pairs << glog;
     const uint64_t want = (units + DDX_WARPS - 1) / DDX_WARPS;
     const uint64_t cap = (uint64_t)sms * 8;
     k_dedup_extend<<<(unsigned)(want < cap ? want : cap), DDX_WARPS * 32, 0, st>>>(
-        L, Q, P, ucut, pair0, n_pairs, offs, hits, ub, flags, (DiagCell*)cells, queue, glog);
+        L, Q, P, ucut, pair0, n_pairs, offs, hits, ub, flags, (DiagCell*)cells, queue, du);
     return cudaGetLastError();
 }
 

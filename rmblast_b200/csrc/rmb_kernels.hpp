@@ -29,10 +29,12 @@ cudaError_t launch_ungapped(const DevLib& L, const DevQueries& Q, const DevParam
 uint64_t dedup_threads(int sms);
 // Bucket-parallel diagonal dedup that extends only the hits the hash admits (one warp per pair):
 // flags and boxes as launch_ungapped + launch_dedup give them.
+// device bytes of the fused dedup's unit lists (units_buf below) for a pair range
+size_t dedup_units_bytes(uint64_t n_pairs, uint64_t n_hits, int sms);
 cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevParams* P, int32_t ucut,
                                 uint64_t pair0, uint64_t n_pairs, uint64_t n_hits, const uint64_t* offs,
                                 const SeedHit* hits, UngBox* ub, uint8_t* flags, void* cells,
-                                unsigned long long* queue, int sms, cudaStream_t st);
+                                unsigned long long* queue, void* units_buf, int sms, cudaStream_t st);
 size_t diag_cell_bytes();
 cudaError_t launch_dedup(const DevLib& L, const DevQueries& Q, int32_t ws, int32_t ucut, uint64_t pair0,
                          uint64_t n_pairs, const uint64_t* offs, const SeedHit* hits, const UngBox* ub, uint8_t* flags,
@@ -55,6 +57,14 @@ cudaError_t launch_prelim_prep(const DevLib& L, const DevQueries& Q, const DevPa
 // Counts a graph-captured chain keeps on the device: the DP's record count (its cell budget then
 // follows on the device) and, for the front-loaded order, the front's length and the order
 // buffer's length (the records past the front are read from its end).
+// The fused dedup's work units (built on the device from the pair offsets).
+struct DedupUnits {
+    unsigned long long* heavy = nullptr;  // groups of the split pairs: pair | group << 32 | log2 G << 40
+    uint32_t* light = nullptr;            // pairs with hits kept whole
+    unsigned int* counts = nullptr;       // [0] heavy entries, [1] light entries
+    uint64_t heavy_cap = 0;
+};
+
 struct StreamDevCounts {
     const unsigned int* n = nullptr;
     const unsigned int* n_front = nullptr;

@@ -20,7 +20,7 @@
 //    and the end-of-row extension cells (gapped.rs:307-319), are not written: a row computes
 //    them from (vlo, nvirt, ext_val) when it reads them, a few predicated operations a cell
 //    (cheaper than a loop in the row end, which runs divergently).  The MININT sentinel
-//    (gapped.rs:325-330) is written at the row end as a clamped entry (below).
+//    (gapped.rs:325-330) is read the same way, as the virtual index after them.
 //  - An entry is 32 bits: bits 0-3 the column residue, bits 4-17 the cell and bits 18-31 the
 //    vertical gap, both as 14-bit values relative to the extension's origin and clamped below at
 //    FLOOR.  The DP runs in the same frame, so entries are read and written without conversion.
@@ -251,14 +251,13 @@ __host__ __device__ __forceinline__ unsigned long long prelim_stream_thread(cons
                     origin += d; best = 0; thr -= d; gap_row -= d;
                 }
                 while (filled < b_size) fill_word();
-                nvirt = k;
+                // the k extension cells and the sentinel after them are read as computed values:
+                // the sentinel's (index nbs, k past vlo) vertical gap ext_val - k * ge - goe is
+                // below the threshold like the reference's MININT (k = 0: then gap_row is below
+                // it, or the band's end cell did not live), and its diagonal feeds no cell (it
+                // is the row's last)
+                nvirt = k + 1u;
                 ext_val = gap_row;
-                {
-                    // the sentinel; with nbs = nb + 1 (no sentinel) the store lands past the band,
-                    // on a slot no live index shares (window <= STREAM_WINDOW), and is never read
-                    uint32_t& e = env.at(nbs);
-                    e = stream_pack(STREAM_FLOOR, STREAM_FLOOR, e);
-                }
                 new_row();
             }
         }
