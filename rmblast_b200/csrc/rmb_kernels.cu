@@ -463,8 +463,8 @@ constexpr int DDX_WARPS = 8;
 // a pass whose admitted hits are at most this many extends them one after another with the whole
 // warp (ung_walk_warp); more run one a lane (UngWalk)
 constexpr int DDX_COOP = 6;
-// a pair's hits go to bucket groups of about this many hits each, at most DDX_GMAX groups
-constexpr uint32_t DDX_UNIT_HITS = 8192, DDX_GLOG_MAX = 5, DDX_GMAX = 1u << DDX_GLOG_MAX;
+// a hit-heavy pair's hits go to at most 2^DDX_GLOG_MAX bucket groups
+constexpr uint32_t DDX_GLOG_MAX = 5;
 
 // Warp-cooperative ungapped X-drop extension: UngWalk's result (left walk, then right walk), 32
 // bases a round.  Every lane calls it with the same arguments and gets the same result.  A round
@@ -540,14 +540,15 @@ __device__ __forceinline__ void ung_walk_warp(const uint8_t* __restrict__ qb, co
 }
 
 // The fused dedup's units: a pair with h > 0 hits gets G = 2^gl groups, gl the smallest at or
-// above glog with h <= DDX_UNIT_HITS << gl (at most DDX_GLOG_MAX).  Pairs with G > 1 list their
+// above glog with h <= unit_hits << gl (at most DDX_GLOG_MAX).  Pairs with G > 1 list their
 // groups in `heavy` (pair | group << 32 | gl << 40), the others themselves in `light`.
-__global__ void k_dedup_units(uint64_t n_pairs, const uint64_t* __restrict__ offs, uint32_t glog, DedupUnits units) {
+__global__ void k_dedup_units(uint64_t n_pairs, const uint64_t* __restrict__ offs, uint32_t glog, uint64_t unit_hits,
+                              DedupUnits units) {
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs;
          p += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t hp = offs[p + 1] - offs[p];
         uint32_t gl = glog;
-        while (gl < DDX_GLOG_MAX && hp > ((uint64_t)DDX_UNIT_HITS << gl)) ++gl;
+        while (gl < DDX_GLOG_MAX && hp > (unit_hits << gl)) ++gl;
         const bool light = hp != 0 && gl == 0;
         const unsigned am = __activemask();
         const unsigned lm = __ballot_sync(am, light);
@@ -583,8 +584,10 @@ __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, De
     const int lane = threadIdx.x & 31;
     uint32_t* hd = heads[threadIdx.x >> 5];
     const int32_t ws = P->word_size, xdrop = P->xdrop_ungap, window = 1 - ws;
-    // A unit is one pair's hits in the buckets of one group (bucket & (G - 1)).  The units of the
-    // pairs split into groups come first (units.heavy, a pair's groups one after another), then
+    // A unit is one pair's hits in the buckets of one group (bucket & (G - 1)).  A pair is split
+    // when it holds more than a warp's share of the launch's hits (each group reads all the
+    // pair's hits and runs its passes with fewer lanes, so splitting only pays where one pair
+    // would hold the end of the launch).  The units of the pairs split into groups come first (units.heavy, a pair's groups one after another), then
     // one unit for each other pair with hits (units.light), so a hit-heavy pair's groups start
     // early and run side by side instead of holding the end of the launch.
     const unsigned int n_heavy = units.counts[0], n_units = n_heavy + units.counts[1];
@@ -2197,10 +2200,17 @@ uint32_t dedup_glog(uint64_t n_pairs, uint64_t n_hits, int sms) {
     return glog;
 }
 
+// hits a unit may hold before its pair is split: a warp's share of the launch's hits
+uint64_t dedup_unit_hits(uint64_t n_hits, int sms) {
+    const uint64_t share = n_hits / ((uint64_t)sms * 32);
+    return share > 2048 ? share : 2048;
+}
+
 size_t dedup_units_bytes(uint64_t n_pairs, uint64_t n_hits, int sms) {
-    // a pair split past glog has G < 2 h / DDX_UNIT_HITS, so the groups of all pairs with G > 1
-    // number at most n_pairs 2^glog + 2 n_hits / DDX_UNIT_HITS
-    const uint64_t heavy = (n_pairs << dedup_glog(n_pairs, n_hits, sms)) + n_hits / (DDX_UNIT_HITS / 2) + 1;
+    // a pair split past glog has G < 2 h / unit_hits, so the groups of all pairs with G > 1
+    // number at most n_pairs 2^glog + 2 n_hits / unit_hits
+    const uint64_t heavy =
+        (n_pairs << dedup_glog(n_pairs, n_hits, sms)) + 2 * n_hits / dedup_unit_hits(n_hits, sms) + 1;
     return 16 + heavy * 8 + n_pairs * 4 + 16;
 }
 
@@ -2210,7 +2220,8 @@ cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevP
                                 unsigned long long* queue, void* units_buf, int sms, cudaStream_t st) {
     if (!n_pairs) return cudaSuccess;
     const uint32_t glog = dedup_glog(n_pairs, n_hits, sms);
-    const uint64_t heavy_cap = (n_pairs << glog) + n_hits / (DDX_UNIT_HITS / 2) + 1;
+    const uint64_t unit_hits = dedup_unit_hits(n_hits, sms);
+    const uint64_t heavy_cap = (n_pairs << glog) + 2 * n_hits / unit_hits + 1;
     DedupUnits du;
     du.counts = (unsigned int*)units_buf;
     du.heavy = (unsigned long long*)((char*)units_buf + 16);
@@ -2220,7 +2231,7 @@ cudaError_t launch_dedup_extend(const DevLib& L, const DevQueries& Q, const DevP
     if (e == cudaSuccess) e = cudaMemsetAsync(du.counts, 0, 16, st);
     if (e != cudaSuccess) return e;
     const uint64_t bb = (n_pairs + 255) / 256;
-    k_dedup_units<<<(unsigned)(bb < 4096 ? bb : 4096), 256, 0, st>>>(n_pairs, offs, glog, du);
+    k_dedup_units<<<(unsigned)(bb < 4096 ? bb : 4096), 256, 0, st>>>(n_pairs, offs, glog, unit_hits, du);
     const uint64_t units = n_pairs << glog;
     const uint64_t want = (units + DDX_WARPS - 1) / DDX_WARPS;
     const uint64_t cap = (uint64_t)sms * 8;
