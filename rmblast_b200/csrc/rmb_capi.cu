@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <future>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -313,7 +314,8 @@ struct PairPrelims {
 
 bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
-                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps);
+                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps,
+                  std::future<void>* defer = nullptr);
 
 // The per-query end of a search: E-values and bit scores (rmstats RmStats for the query's length
 // against the whole database), the --evalue reap (main.rs:1224-1226, before masklevel), then
@@ -631,6 +633,9 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         std::vector<uint64_t> hpvoff(nb), hcsoff(nb), hposoff(nb), hzero(nb, 0);
         std::vector<uint32_t> hqlen(qlen + qb, qlen + qe);
         std::vector<int32_t> hlw(lw_all.begin() + qb, lw_all.begin() + qe);
+        // the batched pipeline's host Phase 2b of the last range, running while the next one's
+        // kernels do (declared here: it reads hqlen and writes out_hits)
+        std::future<void> pending;
         uint64_t npv = 0, ncs = 0, npos = 0;
         for (uint32_t i = 0; i < nb; ++i) {
             hpvoff[i] = npv;
@@ -1117,11 +1122,14 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             }
 
             // ---- traceback DP and host Phase 2b of every prelim
-            if (traceback_2b(C, W, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps)) {
+            if (pending.valid()) pending.get();
+            if (traceback_2b(C, W, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps,
+                             P.pipeline != 1 && !taps ? &pending : nullptr)) {
                 tapped = true;
                 continue;
             }
         }
+        if (pending.valid()) pending.get();
         if (tapped || collect) return;
         t0 = std::chrono::steady_clock::now();
         parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
@@ -1158,10 +1166,13 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
 // Traceback DP on the device and the host Phase 2b (engine.rs:1438-1762) of the prelims of
 // (query, subject) pairs; pair = local query * n_subjects + subject over the queries of Q, whose
 // lengths are hqlen and host copies qhost(local).  Hits go to out[local query].  Returns true
-// when the traceback stage tap took the results instead.
+// when the traceback stage tap took the results instead.  With `defer`, the host Phase 2b runs
+// on a thread of its own and *defer holds it: the caller waits for it before the next call that
+// writes the same queries' hits, and before it reads them.
 bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
-                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps) {
+                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps,
+                  std::future<void>* defer) {
     const uint32_t ns = (uint32_t)C.ids.size();
     const size_t np = pair_ids.size();
     cudaStream_t st = W.st;
@@ -1287,37 +1298,42 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
         }
 
         // ---- host Phase 2b per pair, then per query
-        t0 = std::chrono::steady_clock::now();
-        std::vector<std::vector<Hit>> pair_hits(np);
-        // the reverse complement of each query with prelims, once
-        std::vector<uint32_t> uq;
-        for (size_t k = 0; k < np; ++k) uq.push_back(pair_ids[k] / ns);
-        std::sort(uq.begin(), uq.end());
-        uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
-        std::vector<std::vector<uint8_t>> qrcs(uq.size());
-        parallel_for(uq.size(), [&](size_t j) { qrcs[j] = revcomp_full(qhost(uq[j]), hqlen[uq[j]] + 2); });
-        parallel_for(np, [&](size_t k) {
-            const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
-            const uint8_t* qs = qhost(qi);
-            const std::vector<uint8_t>& qrc = qrcs[std::lower_bound(uq.begin(), uq.end(), qi) - uq.begin()];
-            SubjectView v;
-            v.align = C.h_align.data() + C.plus_off[si];
-            v.align_rc = C.h_align_rc.data() + C.plus_off[si];
-            v.n_mask = C.mask_off[si] >= 0 ? C.h_mask.data() + C.mask_off[si] : nullptr;
-            v.n_mask_rc = C.mask_off[si] >= 0 ? C.h_mask_rc.data() + C.mask_off[si] : nullptr;
-            v.len = C.slen[si];
-            std::vector<TbResult> tr(tres.begin() + pre_off[k], tres.begin() + pre_off[k + 1]);
-            pair_hits[k] = phase2b_filter(prelims[k], tr, qs, qrc.data(), hqlen[qi], v, si, C.gp);
-        });
-        for (size_t k = 0; k < np; ++k) {
-            const uint32_t qi = pair_ids[k] / ns;
-            auto& dst = out[qi];
-            for (auto& h : pair_hits[k]) {
-                h.q_len = hqlen[qi];
-                dst.push_back(std::move(h));
+        auto phase2b = [&C, &ctr, ns, np, out, hqlen, qhost, pair_ids, prelims = std::move(prelims),
+                        tres = std::move(tres), pre_off = std::move(pre_off)]() mutable {
+            const auto t2 = std::chrono::steady_clock::now();
+            std::vector<std::vector<Hit>> pair_hits(np);
+            // the reverse complement of each query with prelims, once
+            std::vector<uint32_t> uq;
+            for (size_t k = 0; k < np; ++k) uq.push_back(pair_ids[k] / ns);
+            std::sort(uq.begin(), uq.end());
+            uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
+            std::vector<std::vector<uint8_t>> qrcs(uq.size());
+            parallel_for(uq.size(), [&](size_t j) { qrcs[j] = revcomp_full(qhost(uq[j]), hqlen[uq[j]] + 2); });
+            parallel_for(np, [&](size_t k) {
+                const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
+                const uint8_t* qs = qhost(qi);
+                const std::vector<uint8_t>& qrc = qrcs[std::lower_bound(uq.begin(), uq.end(), qi) - uq.begin()];
+                SubjectView v;
+                v.align = C.h_align.data() + C.plus_off[si];
+                v.align_rc = C.h_align_rc.data() + C.plus_off[si];
+                v.n_mask = C.mask_off[si] >= 0 ? C.h_mask.data() + C.mask_off[si] : nullptr;
+                v.n_mask_rc = C.mask_off[si] >= 0 ? C.h_mask_rc.data() + C.mask_off[si] : nullptr;
+                v.len = C.slen[si];
+                std::vector<TbResult> tr(tres.begin() + pre_off[k], tres.begin() + pre_off[k + 1]);
+                pair_hits[k] = phase2b_filter(prelims[k], tr, qs, qrc.data(), hqlen[qi], v, si, C.gp);
+            });
+            for (size_t k = 0; k < np; ++k) {
+                const uint32_t qi = pair_ids[k] / ns;
+                auto& dst = out[qi];
+                for (auto& h : pair_hits[k]) {
+                    h.q_len = hqlen[qi];
+                    dst.push_back(std::move(h));
+                }
             }
-        }
-        ctr.ms_host_2b += ms_since(t0);
+            ctr.ms_host_2b += ms_since(t2);
+        };
+        if (defer) *defer = std::async(std::launch::async, std::move(phase2b));
+        else phase2b();
     }
     (void)nb;
     return false;
