@@ -375,7 +375,7 @@ def main():
         return {"value": timed_bases * world / (ms * 1e-3) / 1e6, "ms_per_step": ms, "prelim_ms": kc["gpu_ms_prelim"],
                 "gcups_computed": kc["so_cells"] / (kc["gpu_ms_prelim"] * 1e-3) / 1e9 if kc["gpu_ms_prelim"] else None,
                 "stage_ms": {key: round(kc[key], 3) for key in ("gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
-                                                              "gpu_ms_prelim", "gpu_ms_traceback")}}
+                                                              "gpu_ms_prelim", "gpu_ms_sched", "gpu_ms_traceback")}}
 
     # ---- the measured arm: autotuned launch knobs (batched pipeline), resident, then end to end
     s = searcher(args.pipeline, args.schedule)
@@ -435,9 +435,10 @@ def main():
                                      if k["gpu_ms_traceback"] > 0 else None),
         "scan_roofline": scan_roofline(sum(len(enc[b]) for b in timed) / args.steps, db, k, peaks),
         # device time per stage on one lane (the kernels alone), and the lanes' sum in the timed run
+        # (gpu_ms_sched: the learned order's features, network and order, a part of gpu_ms_prelim)
         "stage_ms": {key: round(k[key], 3) for key in ("gpu_ms_lookup", "gpu_ms_scan", "gpu_ms_ungapped",
-                                                      "gpu_ms_dedup", "gpu_ms_prelim", "gpu_ms_traceback",
-                                                      "ms_host_2a", "ms_host_2b")},
+                                                      "gpu_ms_dedup", "gpu_ms_prelim", "gpu_ms_sched",
+                                                      "gpu_ms_traceback", "ms_host_2a", "ms_host_2b")},
         "lanes": knobs.get("lanes", 1),
         # wall-clock per stage on the host (device work, syncs and host steps together)
         "wall_ms": {k: round(c[k], 3) for k in ("ms_lookup", "ms_scan", "ms_ungapped", "ms_dedup", "ms_prelim_dp",

@@ -180,6 +180,9 @@ typedef struct rmb_counters {
     uint64_t so_cells_main;
     /* DUST masking of the query set (once per uploaded query set, when dust = 1) */
     double gpu_ms_dust;
+    /* the learned record order (schedule 1 or 2): features, network and order, a part of
+     * gpu_ms_prelim */
+    double gpu_ms_sched;
 } rmb_counters;
 
 /* Results of rmb_search_batch, in the reference's output order per query

@@ -56,7 +56,8 @@ class _Counters(C.Structure):
         (n, C.c_double) for n in ("ms_lookup", "ms_scan", "ms_ungapped", "ms_dedup", "ms_prelim_dp", "ms_host_2a",
                                   "ms_traceback", "ms_host_2b", "gpu_ms_scan", "gpu_ms_ungapped", "gpu_ms_dedup",
                                   "gpu_ms_prelim", "gpu_ms_traceback", "gpu_ms_lookup")] + [("launches", C.c_uint64)] + [
-        ("gpu_ms_prelim_main", C.c_double), ("so_cells_main", C.c_uint64), ("gpu_ms_dust", C.c_double)]
+        ("gpu_ms_prelim_main", C.c_double), ("so_cells_main", C.c_uint64), ("gpu_ms_dust", C.c_double),
+        ("gpu_ms_sched", C.c_double)]
 
 
 class _Results(C.Structure):

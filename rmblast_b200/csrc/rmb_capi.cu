@@ -161,7 +161,7 @@ struct Work {
     // the device chain as a CUDA graph (chain_graph): its executable, its timing events and the
     // pinned block its counts come back in
     cudaGraphExec_t exec = nullptr;
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[7] = {};
     HostBuf hcount;
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -421,6 +421,7 @@ void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_
         CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), n1, W.ung_idx.as<uint32_t>(), W.hits.as<SeedHit>(),
                               W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(), W.geo.p, C.sms, st, nu_dev));
         const uint32_t* order = nullptr;
+        rec(6);
         if (learned) {
             CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), n1, W.ung_idx.as<uint32_t>(),
                                   W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
@@ -499,6 +500,7 @@ void chain_graph(rmb_ctx& C, Work& W, const DevQueries& Q, int32_t ucut, uint64_
     ctr.gpu_ms_dedup += ms(0, 1);
     ctr.gpu_ms_prelim += ms(1, 5);
     ctr.gpu_ms_prelim_main += ms(2, 3);
+    if (learned) ctr.gpu_ms_sched += ms(6, 2);
     ctr.so_cells_main += main_cells;
     ctr.launches += 2 + 1 + 1 + (learned ? 3 : 0) + 1 + 2 + 1 + 1;
     ctr.ungapped += nu;
@@ -577,6 +579,7 @@ void add_counters(rmb_counters& a, const rmb_counters& b) {
     a.launches += b.launches;
     a.gpu_ms_prelim_main += b.gpu_ms_prelim_main; a.so_cells_main += b.so_cells_main;
     a.gpu_ms_dust += b.gpu_ms_dust;
+    a.gpu_ms_sched += b.gpu_ms_sched;
 }
 
 // The search of a set of single-chunk queries.  ucut_override: per-query ungapped cutoffs (the
@@ -923,7 +926,8 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             CK(cudaMemsetAsync(W.cells.p, 0, 16, st));
             CK(cudaMemsetAsync(W.fails.p, 0, 16, st));
             ev.start(st);
-            EvTimer ev_main;
+            EvTimer ev_main, es;  // es: the learned order's kernels
+            bool es_used = false;
             if (C.prelim_stream) {
                 W.geo.ensure(std::max<uint64_t>(nu, 1) * prelim_geo_bytes());
                 CK(launch_prelim_prep(C.L, Q, C.d_params.as<DevParams>(), nu, W.ung_idx.as<uint32_t>(),
@@ -948,11 +952,14 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                     W.sched_scratch.ensure(sched_order_scratch_bytes());
                     size_t tb = C.p.schedule == 1 ? sched_front_temp_bytes(nu) : 0;
                     if (tb) W.temp.ensure(tb);
+                    es.start(st);
+                    es_used = true;
                     CK(launch_sched_order(C.L, Q, C.d_params.as<DevParams>(), nu, W.ung_idx.as<uint32_t>(),
                                           W.hits.as<SeedHit>(), W.hit_pair.as<uint32_t>(), W.ub.as<UngBox>(),
                                           W.counts.as<uint32_t>(), C.sched_params.as<float>(),
                                           W.sched_pred.as<float>(), W.sched_scratch.p, W.sched_order.as<uint32_t>(),
                                           C.sms, st, C.p.schedule, W.temp.p, tb));
+                    es.stop(st);
                     order = W.sched_order.as<uint32_t>();
                     ctr.launches += 3;
                 }
@@ -1003,6 +1010,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
                 ctr.gpu_ms_prelim_main += ev_main.ms();
                 ctr.so_cells_main += main_cells;
             }
+            if (es_used) ctr.gpu_ms_sched += es.ms();
             DBuf* wide_list = &W.wide;
             if (nw && C.prelim_stream) {
                 // records whose band window outgrew the thread ring: the warp kernel's 256-cell rings
