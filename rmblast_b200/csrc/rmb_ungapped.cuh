@@ -28,12 +28,12 @@ struct UngWalk {
         sum = 0; score = 0; xc = x; best = wq;
     }
 
-    // One base.  Returns 0 while walking, 1 when the left walk ended (the right one starts at
-    // the seed), 2 when the right walk ended (the extension is done).
-    __host__ __device__ __forceinline__ int step(const int32_t* mat) {
-        bool stop = q == qlim || s == slim;
+    // One base: the walk's step on query base a and subject base c at (q, s), or its end when
+    // at_end (q or s at its limit).  Returns 0 while walking, 1 when the left walk ended (the
+    // right one starts at the seed), 2 when the right walk ended (the extension is done).
+    __host__ __device__ __forceinline__ int on_base(bool at_end, uint8_t a, uint8_t c, const int32_t* mat) {
+        bool stop = at_end;
         if (!stop) {
-            const uint8_t a = qb[1 + q], c = sb[1 + s];
             if (a == 15 || c == 15) {
                 stop = true;
             } else {
@@ -60,6 +60,32 @@ struct UngWalk {
             return 1;
         }
         return 2;
+    }
+
+    // One base, as on_base.
+    __host__ __device__ __forceinline__ int step(const int32_t* mat) {
+        const bool end = q == qlim || s == slim;
+        return on_base(end, end ? (uint8_t)15 : qb[1 + q], end ? (uint8_t)15 : sb[1 + s], mat);
+    }
+
+    // Up to four bases, their loads issued together (the walk's next positions do not depend on
+    // its sums): the same as calling step() until it returns nonzero, at most four times; returns
+    // what the last call would have.
+    __host__ __device__ __forceinline__ int step4(const int32_t* mat) {
+        uint8_t a[4], c[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int32_t qj = q + dir * j, sj = s + dir * j;
+            const bool in = dir < 0 ? (qj > qlim && sj > slim) : (qj < qlim && sj < slim);
+            a[j] = in ? qb[1 + qj] : (uint8_t)15;
+            c[j] = in ? sb[1 + sj] : (uint8_t)15;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = on_base(q == qlim || s == slim, a[j], c[j], mat);
+            if (r) return r;
+        }
+        return 0;
     }
 
     // After step() returned 2: the extension in the walk's frame.
