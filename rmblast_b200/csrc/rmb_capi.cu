@@ -156,7 +156,7 @@ struct Work {
     DBuf pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo,
         n_wide, band, sel, surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over,
-        tb_ooff, tb_ops2, ung_queue, dd_units;
+        tb_ooff, tb_ops2, ung_queue, dd_units, tb_half;
     DBuf sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
     // the device chain as a CUDA graph (chain_graph): its executable, its timing events and the
     // pinned block its counts come back in
@@ -175,7 +175,7 @@ struct Work {
                        &lut_vals2, &lut_counts, &counts, &offs, &hits, &hit_pair, &ub, &flags, &dd_scratch, &dd_cells,
                        &ung_idx, &n_sel, &po, &wide, &wide2, &dres, &geo, &n_wide, &band, &sel, &surv, &cells, &fails,
                        &temp, &tb_in, &tb_out, &tb_ops, &tb_scratch, &stage, &stage_start, &stage_over, &tb_ooff,
-                       &tb_ops2, &ung_queue, &dd_units, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
+                       &tb_ops2, &ung_queue, &dd_units, &tb_half, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
         for (DBuf* b : all) b->release();
         if (st) cudaStreamDestroy(st);
         st = nullptr;
@@ -1223,19 +1223,23 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 const uint32_t rows_cap = qmax + 2;
                 const uint64_t per_thread = ((band_cells * 8 + (uint64_t)rows_cap * 8 + trace_cap) + 255) & ~255ull;
                 const uint64_t budget = 8ull << 30;
-                // one warp per scratch slot, blocks of 8 warps
-                uint32_t threads = (uint32_t)std::min<uint64_t>(todo.size(), std::max<uint64_t>(8, budget / per_thread));
+                // one warp per scratch slot (two items, the left and the right extension, per
+                // prelim), blocks of 8 warps
+                uint32_t threads =
+                    (uint32_t)std::min<uint64_t>(2 * todo.size(), std::max<uint64_t>(8, budget / per_thread));
                 threads = (threads + 7) / 8 * 8;
                 upload(W.tb_in, chunk_in, st);
                 W.tb_out.ensure(todo.size() * sizeof(TbOut));
-                W.tb_ops.ensure(todo.size() * (uint64_t)ops_cap * 4);
+                W.tb_half.ensure(2 * todo.size() * sizeof(TbHalf));
+                W.tb_ops.ensure(2 * todo.size() * (uint64_t)ops_cap * 4);
                 W.tb_scratch.ensure((uint64_t)threads * per_thread);
                 CK(cudaMemsetAsync(W.cells.p, 0, 8, st));
                 EvTimer et;
                 et.start(st);
-                ctr.launches += 1;
+                ctr.launches += 2;
                 CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), W.tb_in.as<TbIn>(),
-                                    W.tb_out.as<TbOut>(), W.tb_ops.as<uint32_t>(), ops_cap, W.tb_scratch.as<uint8_t>(),
+                                    W.tb_out.as<TbOut>(), W.tb_half.as<TbHalf>(), W.tb_ops.as<uint32_t>(), ops_cap,
+                                    W.tb_scratch.as<uint8_t>(),
                                     per_thread, band_cells, rows_cap, threads, W.cells.as<unsigned long long>(), st));
                 et.stop(st);
                 std::vector<TbOut> to(todo.size());
@@ -1251,7 +1255,8 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 if (!ops.empty()) {
                     upload(W.tb_ooff, ooff, st);
                     W.tb_ops2.ensure(ops.size() * 4);
-                    CK(launch_gather_ops((uint32_t)todo.size(), W.tb_ops.as<uint32_t>(), ops_cap, W.tb_out.as<TbOut>(),
+                    // the merged script of prelim i sits in ops slot 2 i
+                    CK(launch_gather_ops((uint32_t)todo.size(), W.tb_ops.as<uint32_t>(), 2 * ops_cap, W.tb_out.as<TbOut>(),
                                          W.tb_ooff.as<uint64_t>(), W.tb_ops2.as<uint32_t>(), C.sms, st));
                     CK(cudaMemcpyAsync(ops.data(), W.tb_ops2.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
                     CK(cudaStreamSynchronize(st));

@@ -80,5 +80,12 @@ struct TbOut {
     uint32_t n_ops;
     uint32_t need;    // scratch bytes a retry needs (status 2)
 };
+// One extension's traceback (left or right of the improved seed).
+struct TbHalf {
+    int32_t status;  // 0 ok, 2 scratch overflow, 3 walk failure
+    int32_t score;
+    uint32_t a_len, b_len, n_ops, need;
+    uint32_t tq, ts;  // the improved seed (DP frame)
+};
 
 }  // namespace rmb

@@ -1986,10 +1986,13 @@ __device__ int align_ex_tb_warp(const uint8_t* __restrict__ a, const uint8_t* __
     return st;
 }
 
-// One prelim per warp: improve_seed, the two warp DPs, script merge and gap pruning.
+// One extension of a prelim per warp: item 2t is prelim t's left extension, item 2t + 1 its right
+// one (both from the improved seed, independent of each other), so a long alignment's two DPs
+// run side by side on two warps; k_traceback_join then merges the two scripts.  Each item's ops
+// go to its own ops_cap slot; `half` gets its status, score, extents and op count.
 __global__ void __launch_bounds__(256) k_traceback_warp(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                          uint32_t n, const TbIn* __restrict__ in,
-                                                         TbOut* __restrict__ out, uint32_t* __restrict__ ops_out,
+                                                         TbHalf* __restrict__ half, uint32_t* __restrict__ ops_out,
                                                          uint32_t ops_cap, uint8_t* __restrict__ scratch,
                                                          uint64_t per_warp, uint64_t band_cells, uint32_t rows_cap,
                                                          unsigned long long* __restrict__ cells_total) {
@@ -2007,7 +2010,9 @@ __global__ void __launch_bounds__(256) k_traceback_warp(DevLib L, DevQueries Q, 
     S.trace = base + band_cells * sizeof(int2) + (uint64_t)rows_cap * sizeof(uint2);
     S.trace_cap = per_warp - band_cells * sizeof(int2) - (uint64_t)rows_cap * sizeof(uint2);
     uint64_t cells = 0;
-    for (uint64_t t = warp; t < n; t += nwarps) {
+    for (uint64_t k = warp; k < 2ull * n; k += nwarps) {
+        const uint64_t t = k >> 1;
+        const bool right = k & 1;
         const TbIn h = in[t];
         const uint32_t qi = h.pair / L.n, si = h.pair % L.n;
         const uint32_t qa = Q.len[qi], sa = L.len[si];
@@ -2021,74 +2026,94 @@ __global__ void __launch_bounds__(256) k_traceback_warp(DevLib L, DevQueries Q, 
         const uint32_t tq = plus ? nq : qa - 1 - nq, ts = plus ? ns : sa - 1 - ns;
         const uint8_t* qa_ = (plus ? Q.q : Q.qrc) + Q.off[qi] + 1;
         const uint8_t* sa_ = L.align + L.plus_off[si] + 1;
-        uint32_t* ops = ops_out + t * (uint64_t)ops_cap;
-        TbOut o{0, 0, 0, 0, 0, 0, 0, 0};
+        uint32_t* ops = ops_out + k * (uint64_t)ops_cap;
         uint64_t need = 0;
-        int32_t ls, rs = 0;
-        uint32_t la, lb, ra = 0, rb = 0, nl = 0, nr = 0;
-        int st = align_ex_tb_warp<true>(qa_, sa_, tq + 1, ts + 1, P->gap_open, P->gap_extend, P->xdrop_gap_final, mat,
-                                        S, ls, la, lb, ops, ops_cap, nl, cells, need);
-        if (st == 0) {
+        int32_t sc = 0;
+        uint32_t a = 0, b = 0, nops = 0;
+        int st = 0;
+        if (!right) {
+            st = align_ex_tb_warp<true>(qa_, sa_, tq + 1, ts + 1, P->gap_open, P->gap_extend, P->xdrop_gap_final, mat,
+                                        S, sc, a, b, ops, ops_cap, nops, cells, need);
+        } else {
             const uint32_t rq = tq + 1, rsd = ts + 1;
             const uint32_t rm = qa > rq ? qa - rq : 0, rn = sa > rsd ? sa - rsd : 0;
             if (rm > 0 && rn > 0)
                 st = align_ex_tb_warp<false>(qa_ + rq, sa_ + rsd, rm, rn, P->gap_open, P->gap_extend,
-                                             P->xdrop_gap_final, mat, S, rs, ra, rb, ops + nl, ops_cap - nl, nr, cells,
-                                             need);
+                                             P->xdrop_gap_final, mat, S, sc, a, b, ops, ops_cap, nops, cells, need);
         }
-        if (lane != 0) continue;
-        if (st != 0) {
-            o.status = st == 3 ? 3 : 2;
-            o.need = (uint32_t)min(need, (uint64_t)0xffffffffu);
-            out[t] = o;
-            continue;
-        }
-        for (uint32_t i = 0, j = nr ? nr - 1 : 0; i < j; ++i, --j) {
-            const uint32_t tmp = ops[nl + i];
-            ops[nl + i] = ops[nl + j];
-            ops[nl + j] = tmp;
-        }
-        uint32_t nops = nl;
-        for (uint32_t i = 0; i < nr; ++i) {
-            const uint32_t v = ops[nl + i];
-            if (nops > 0 && (ops[nops - 1] >> 30) == (v >> 30)) ops[nops - 1] += v & 0x3fffffffu;
-            else ops[nops++] = v;
-        }
-        int32_t total = ls + rs;
-        uint32_t q_start = tq + 1 - la, s_start = ts + 1 - lb, q_end = tq + 1 + ra, s_end = ts + 1 + rb;
-        uint32_t first = 0;
-        while (first < nops && (ops[first] >> 30) != 0) {
-            const uint32_t op = ops[first] >> 30, cnt = ops[first] & 0x3fffffffu;
-            total += P->gap_open + (int32_t)cnt * P->gap_extend;
-            if (op == 1) s_start += cnt;
-            else q_start += cnt;
-            ++first;
-        }
-        while (nops > first && (ops[nops - 1] >> 30) != 0) {
-            const uint32_t op = ops[nops - 1] >> 30, cnt = ops[nops - 1] & 0x3fffffffu;
-            total += P->gap_open + (int32_t)cnt * P->gap_extend;
-            if (op == 1) s_end -= cnt;
-            else q_end -= cnt;
-            --nops;
-        }
-        if (first) {
-            for (uint32_t i = first; i < nops; ++i) ops[i - first] = ops[i];
-            nops -= first;
-        }
-        if (total < 0) {
-            o.status = 1;
-            out[t] = o;
-            continue;
-        }
-        o.score = total;
-        o.q0 = q_start;
-        o.q1 = q_end;
-        o.s0 = s_start;
-        o.s1 = s_end;
-        o.n_ops = nops;
-        out[t] = o;
+        if (lane == 0)
+            half[k] = TbHalf{st, sc, a, b, nops, (uint32_t)min(need, (uint64_t)0xffffffffu), tq, ts};
     }
     if (lane == 0 && cells) atomicAdd(cells_total, (unsigned long long)cells);
+}
+
+// One prelim per thread: its two extensions' scripts merged (the right one reversed after the
+// left one, runs of one op joined), the end gaps pruned, and the box and score of the whole
+// alignment (engine.rs:2953-3039).  The merged script goes to the left item's ops slot.
+__global__ void k_traceback_join(const DevParams* __restrict__ P, uint32_t n, const TbHalf* __restrict__ half,
+                                 uint32_t* __restrict__ ops_out, uint32_t ops_cap, TbOut* __restrict__ out) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const TbHalf lh = half[2 * t], rh = half[2 * t + 1];
+    TbOut o{0, 0, 0, 0, 0, 0, 0, 0};
+    if (lh.status != 0 || rh.status != 0) {
+        o.status = lh.status == 3 || rh.status == 3 ? 3 : 2;
+        o.need = max(lh.status ? lh.need : 0u, rh.status ? rh.need : 0u);
+        out[t] = o;
+        return;
+    }
+    uint32_t* ops = ops_out + 2 * t * (uint64_t)ops_cap;
+    const uint32_t* rops = ops_out + (2 * t + 1) * (uint64_t)ops_cap;
+    const uint32_t nl = lh.n_ops, nr = rh.n_ops;
+    const uint32_t tq = lh.tq, ts = lh.ts;
+    uint32_t nops = nl;
+    for (uint32_t i = 0; i < nr; ++i) {
+        const uint32_t v = rops[nr - 1 - i];
+        if (nops > 0 && (ops[nops - 1] >> 30) == (v >> 30)) {
+            ops[nops - 1] += v & 0x3fffffffu;
+        } else {
+            if (nops >= ops_cap) {  // the joined script does not fit the slot: again with larger slots
+                o.status = 2;
+                out[t] = o;
+                return;
+            }
+            ops[nops++] = v;
+        }
+    }
+    int32_t total = lh.score + rh.score;
+    uint32_t q_start = tq + 1 - lh.a_len, s_start = ts + 1 - lh.b_len, q_end = tq + 1 + rh.a_len,
+             s_end = ts + 1 + rh.b_len;
+    uint32_t first = 0;
+    while (first < nops && (ops[first] >> 30) != 0) {
+        const uint32_t op = ops[first] >> 30, cnt = ops[first] & 0x3fffffffu;
+        total += P->gap_open + (int32_t)cnt * P->gap_extend;
+        if (op == 1) s_start += cnt;
+        else q_start += cnt;
+        ++first;
+    }
+    while (nops > first && (ops[nops - 1] >> 30) != 0) {
+        const uint32_t op = ops[nops - 1] >> 30, cnt = ops[nops - 1] & 0x3fffffffu;
+        total += P->gap_open + (int32_t)cnt * P->gap_extend;
+        if (op == 1) s_end -= cnt;
+        else q_end -= cnt;
+        --nops;
+    }
+    if (first) {
+        for (uint32_t i = first; i < nops; ++i) ops[i - first] = ops[i];
+        nops -= first;
+    }
+    if (total < 0) {
+        o.status = 1;
+        out[t] = o;
+        return;
+    }
+    o.score = total;
+    o.q0 = q_start;
+    o.q1 = q_end;
+    o.s0 = s_start;
+    o.s1 = s_end;
+    o.n_ops = nops;
+    out[t] = o;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -2441,16 +2466,20 @@ cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevPa
 }
 
 cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n, const TbIn* in,
-                             TbOut* out, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch, uint64_t per_thread,
-                             uint64_t band_cells, uint32_t rows_cap, uint32_t threads, unsigned long long* cells,
-                             cudaStream_t st) {
-    // `threads` scratch slots of `per_thread` bytes: one warp per slot
+                             TbOut* out, TbHalf* half, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch,
+                             uint64_t per_thread, uint64_t band_cells, uint32_t rows_cap, uint32_t threads,
+                             unsigned long long* cells, cudaStream_t st) {
+    // `threads` scratch slots of `per_thread` bytes: one warp per slot, two items per prelim;
+    // ops: 2 n slots of ops_cap, the merged script of prelim t in slot 2 t
     if (!n) return cudaSuccess;
     const int block = 256;
     const uint32_t warps = threads;
     const int grid = (int)((warps * 32 + block - 1) / block);
-    k_traceback_warp<<<grid, block, 0, st>>>(L, Q, P, n, in, out, ops, ops_cap, scratch, per_thread, band_cells,
+    k_traceback_warp<<<grid, block, 0, st>>>(L, Q, P, n, in, half, ops, ops_cap, scratch, per_thread, band_cells,
                                              rows_cap, cells);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_traceback_join<<<(n + 127) / 128, 128, 0, st>>>(P, n, half, ops, ops_cap, out);
     return cudaGetLastError();
 }
 
