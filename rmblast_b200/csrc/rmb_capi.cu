@@ -1225,8 +1225,10 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 const uint64_t budget = 8ull << 30;
                 // one warp per scratch slot (two items, the left and the right extension, per
                 // prelim), blocks of 8 warps
-                uint32_t threads =
-                    (uint32_t)std::min<uint64_t>(2 * todo.size(), std::max<uint64_t>(8, budget / per_thread));
+                // (the plain pipeline: one prelim per warp, its two extensions in turn)
+                const bool whole = C.p.pipeline == 1;
+                uint32_t threads = (uint32_t)std::min<uint64_t>((whole ? 1 : 2) * todo.size(),
+                                                                std::max<uint64_t>(8, budget / per_thread));
                 threads = (threads + 7) / 8 * 8;
                 upload(W.tb_in, chunk_in, st);
                 W.tb_out.ensure(todo.size() * sizeof(TbOut));
@@ -1240,7 +1242,8 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), W.tb_in.as<TbIn>(),
                                     W.tb_out.as<TbOut>(), W.tb_half.as<TbHalf>(), W.tb_ops.as<uint32_t>(), ops_cap,
                                     W.tb_scratch.as<uint8_t>(),
-                                    per_thread, band_cells, rows_cap, threads, W.cells.as<unsigned long long>(), st));
+                                    per_thread, band_cells, rows_cap, threads, W.cells.as<unsigned long long>(), whole,
+                                    st));
                 et.stop(st);
                 std::vector<TbOut> to(todo.size());
                 CK(cudaMemcpyAsync(to.data(), W.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));

@@ -1989,19 +1989,23 @@ __device__ int align_ex_tb_warp(const uint8_t* __restrict__ a, const uint8_t* __
 // One extension of a prelim per warp: item 2t is prelim t's left extension, item 2t + 1 its right
 // one (both from the improved seed, independent of each other), so a long alignment's two DPs
 // run side by side on two warps; k_traceback_join then merges the two scripts.  Each item's ops
-// go to its own ops_cap slot; `half` gets its status, score, extents and op count.
+// go to its own ops_cap slot; `half` gets its status, score, extents and op count.  With `whole`
+// a warp takes a prelim's two items one after the other (one prelim per warp, the plain
+// pipeline's work unit).
 __global__ void __launch_bounds__(256) k_traceback_warp(DevLib L, DevQueries Q, const DevParams* __restrict__ P,
                                                          uint32_t n, const TbIn* __restrict__ in,
                                                          TbHalf* __restrict__ half, uint32_t* __restrict__ ops_out,
                                                          uint32_t ops_cap, uint8_t* __restrict__ scratch,
                                                          uint64_t per_warp, uint64_t band_cells, uint32_t rows_cap,
-                                                         unsigned long long* __restrict__ cells_total) {
+                                                         unsigned long long* __restrict__ cells_total, bool whole) {
     __shared__ int32_t mat[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) mat[i] = P->matrix[i];
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    // item sequence of this warp: k = warp, warp + nwarps, ...; or, whole, 2w, 2w + 1, 2(w + nwarps), ...
+    const uint64_t k_first = whole ? 2 * warp : warp, k_stride = whole ? 2 * nwarps : nwarps;
     uint8_t* base = scratch + warp * per_warp;
     TbScratch S;
     S.band = (int2*)base;
@@ -2010,7 +2014,8 @@ __global__ void __launch_bounds__(256) k_traceback_warp(DevLib L, DevQueries Q, 
     S.trace = base + band_cells * sizeof(int2) + (uint64_t)rows_cap * sizeof(uint2);
     S.trace_cap = per_warp - band_cells * sizeof(int2) - (uint64_t)rows_cap * sizeof(uint2);
     uint64_t cells = 0;
-    for (uint64_t k = warp; k < 2ull * n; k += nwarps) {
+    for (uint64_t k0 = k_first; k0 < 2ull * n; k0 += k_stride)
+    for (uint64_t k = k0; k < (whole ? k0 + 2 : k0 + 1); ++k) {
         const uint64_t t = k >> 1;
         const bool right = k & 1;
         const TbIn h = in[t];
@@ -2468,7 +2473,7 @@ cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevPa
 cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n, const TbIn* in,
                              TbOut* out, TbHalf* half, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch,
                              uint64_t per_thread, uint64_t band_cells, uint32_t rows_cap, uint32_t threads,
-                             unsigned long long* cells, cudaStream_t st) {
+                             unsigned long long* cells, bool whole, cudaStream_t st) {
     // `threads` scratch slots of `per_thread` bytes: one warp per slot, two items per prelim;
     // ops: 2 n slots of ops_cap, the merged script of prelim t in slot 2 t
     if (!n) return cudaSuccess;
@@ -2476,7 +2481,7 @@ cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevPara
     const uint32_t warps = threads;
     const int grid = (int)((warps * 32 + block - 1) / block);
     k_traceback_warp<<<grid, block, 0, st>>>(L, Q, P, n, in, half, ops, ops_cap, scratch, per_thread, band_cells,
-                                             rows_cap, cells);
+                                             rows_cap, cells, whole);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_traceback_join<<<(n + 127) / 128, 128, 0, st>>>(P, n, half, ops, ops_cap, out);

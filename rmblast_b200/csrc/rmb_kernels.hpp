@@ -110,7 +110,7 @@ cudaError_t launch_prelim_wide(const DevLib& L, const DevQueries& Q, const DevPa
 cudaError_t launch_traceback(const DevLib& L, const DevQueries& Q, const DevParams* P, uint32_t n, const TbIn* in,
                              TbOut* out, TbHalf* half, uint32_t* ops, uint32_t ops_cap, uint8_t* scratch,
                              uint64_t per_thread, uint64_t band_cells, uint32_t rows_cap, uint32_t threads,
-                             unsigned long long* cells, cudaStream_t st);
+                             unsigned long long* cells, bool whole, cudaStream_t st);
 // The ops of the finished items of a traceback launch, packed at the host-computed offsets off[i]
 // (items with status 2 are skipped), so only the ops in use cross to the host.
 cudaError_t launch_gather_ops(uint32_t n, const uint32_t* ops, uint32_t ops_cap, const TbOut* out, const uint64_t* off,
