@@ -315,7 +315,7 @@ struct PairPrelims {
 bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
                   std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps,
-                  std::future<void>* defer = nullptr);
+                  std::future<double>* defer = nullptr);
 
 // The per-query end of a search: E-values and bit scores (rmstats RmStats for the query's length
 // against the whole database), the --evalue reap (main.rs:1224-1226, before masklevel), then
@@ -628,7 +628,11 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         qb = qe;
     }
     CK(cudaStreamSynchronize(st));  // the lanes start after the query set's own work (upload, DUST)
-    auto sub_batch = [&](Work& W, uint32_t qb, uint32_t qe, rmb_counters& ctr) {
+    // With `tail`, the sub-batch's last host steps (the pending Phase 2b, masklevel and the hit
+    // order) run on a thread of their own, *tail holding them (their host ms and hits), so the
+    // next sub-batch's kernels start at once.
+    using Tail = std::future<std::pair<double, uint64_t>>;
+    auto sub_batch = [&](Work& W, uint32_t qb, uint32_t qe, rmb_counters& ctr, Tail* tail) {
         cudaStream_t st = W.st;
         const uint32_t nb = qe - qb;
         auto t0 = std::chrono::steady_clock::now();
@@ -638,7 +642,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         std::vector<int32_t> hlw(lw_all.begin() + qb, lw_all.begin() + qe);
         // the batched pipeline's host Phase 2b of the last range, running while the next one's
         // kernels do (declared here: it reads hqlen and writes out_hits)
-        std::future<void> pending;
+        std::future<double> pending;
         uint64_t npv = 0, ncs = 0, npos = 0;
         for (uint32_t i = 0; i < nb; ++i) {
             hpvoff[i] = npv;
@@ -1130,14 +1134,25 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             }
 
             // ---- traceback DP and host Phase 2b of every prelim
-            if (pending.valid()) pending.get();
+            if (pending.valid()) ctr.ms_host_2b += pending.get();
             if (traceback_2b(C, W, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps,
                              P.pipeline != 1 && !taps ? &pending : nullptr)) {
                 tapped = true;
                 continue;
             }
         }
-        if (pending.valid()) pending.get();
+        if (tail && !tapped && !collect) {
+            *tail = std::async(std::launch::async, [&C, &out_hits, qb, nb, hqlen, pending = std::move(pending)]() mutable {
+                double ms = pending.valid() ? pending.get() : 0.0;
+                const auto t3 = std::chrono::steady_clock::now();
+                parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
+                uint64_t finals = 0;
+                for (uint32_t i = 0; i < nb; ++i) finals += out_hits[qb + i].size();
+                return std::make_pair(ms + ms_since(t3), finals);
+            });
+            return;
+        }
+        if (pending.valid()) ctr.ms_host_2b += pending.get();
         if (tapped || collect) return;
         t0 = std::chrono::steady_clock::now();
         parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
@@ -1145,7 +1160,22 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         ctr.ms_host_2b += ms_since(t0);
     };
     if (lanes == 1) {
-        for (auto& sb : subs) sub_batch(C.work[0], sb.first, sb.second, ctr);
+        // the batched pipeline: each sub-batch's host tail beside the next one's kernels
+        const bool overlap = P.pipeline != 1 && !taps && !collect;
+        Tail last;
+        auto join = [&]() {
+            if (!last.valid()) return;
+            const auto r = last.get();
+            ctr.ms_host_2b += r.first;
+            ctr.finals += r.second;
+        };
+        for (auto& sb : subs) {
+            Tail next;
+            sub_batch(C.work[0], sb.first, sb.second, ctr, overlap ? &next : nullptr);
+            join();
+            last = std::move(next);
+        }
+        join();
         return;
     }
     // lane k takes sub-batches k, k + 2, ... in order; lane 1 on a host thread of its own
@@ -1154,14 +1184,14 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
     std::thread t1([&]() {
         try {
             CK(cudaSetDevice(C.p.device));
-            for (size_t i = 1; i < subs.size(); i += 2) sub_batch(C.work[1], subs[i].first, subs[i].second, c1);
+            for (size_t i = 1; i < subs.size(); i += 2) sub_batch(C.work[1], subs[i].first, subs[i].second, c1, nullptr);
         } catch (...) {
             err1 = std::current_exception();
         }
     });
     std::exception_ptr err0;
     try {
-        for (size_t i = 0; i < subs.size(); i += 2) sub_batch(C.work[0], subs[i].first, subs[i].second, ctr);
+        for (size_t i = 0; i < subs.size(); i += 2) sub_batch(C.work[0], subs[i].first, subs[i].second, ctr, nullptr);
     } catch (...) {
         err0 = std::current_exception();
     }
@@ -1175,12 +1205,12 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
 // (query, subject) pairs; pair = local query * n_subjects + subject over the queries of Q, whose
 // lengths are hqlen and host copies qhost(local).  Hits go to out[local query].  Returns true
 // when the traceback stage tap took the results instead.  With `defer`, the host Phase 2b runs
-// on a thread of its own and *defer holds it: the caller waits for it before the next call that
-// writes the same queries' hits, and before it reads them.
+// on a thread of its own and *defer holds it (its host ms): the caller waits for it before the
+// next call that writes the same queries' hits, and before it reads them.
 bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
                   std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps,
-                  std::future<void>* defer) {
+                  std::future<double>* defer) {
     const uint32_t ns = (uint32_t)C.ids.size();
     const size_t np = pair_ids.size();
     cudaStream_t st = W.st;
@@ -1314,7 +1344,7 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
         }
 
         // ---- host Phase 2b per pair, then per query
-        auto phase2b = [&C, &ctr, ns, np, out, hqlen, qhost, pair_ids, prelims = std::move(prelims),
+        auto phase2b = [&C, ns, np, out, hqlen, qhost, pair_ids, prelims = std::move(prelims),
                         tres = std::move(tres), pre_off = std::move(pre_off)]() mutable {
             const auto t2 = std::chrono::steady_clock::now();
             std::vector<std::vector<Hit>> pair_hits(np);
@@ -1346,10 +1376,10 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                     dst.push_back(std::move(h));
                 }
             }
-            ctr.ms_host_2b += ms_since(t2);
+            return ms_since(t2);
         };
         if (defer) *defer = std::async(std::launch::async, std::move(phase2b));
-        else phase2b();
+        else ctr.ms_host_2b += phase2b();
     }
     (void)nb;
     return false;
