@@ -295,8 +295,9 @@ __device__ __forceinline__ void extend_ungapped(const uint8_t* query, int64_t q_
 // not wait for the longest walk of the warp.  Same arithmetic as extend_ungapped + the box of
 // engine.rs:1165-1170 / 1244-1261.
 // 16 steps a round: the walks at the default size run hundreds of bases, so fewer refills pay
-// for the idle steps after a walk ends (8 measured 49-50 ms, 16 47 ms a step); the steps go four
-// bases at a time (UngWalk::step4), the eight byte loads of four bases issued together
+// for the idle steps after a walk ends (8 measured 49-50 ms, 16 47 ms a step).  Four bases a
+// step with their loads issued together measured slower, on this kernel (27 -> 32 ms a step on
+// config 3's workload) and in the fused dedup's lane walks
 constexpr int UNG_GROUP = 16;
 // QUEUE: a persistent grid whose lanes take hits from a grid-wide queue as their walks end (the
 // batched pipeline); otherwise one hit per thread, thread i taking hit i (the plain pipeline).
@@ -353,8 +354,8 @@ __global__ void __launch_bounds__(256) k_ungapped(DevLib L, DevQueries Q, const 
         }
         if (!__any_sync(FULL, phase == 1)) break;
 #pragma unroll
-        for (int g = 0; g < UNG_GROUP / 4; ++g) {
-            if (phase == 1 && walk.step4(mat) == 2) {
+        for (int g = 0; g < UNG_GROUP; ++g) {
+            if (phase == 1 && walk.step(mat) == 2) {
                 // the box in the record frame, and the value the diagonal hash stores
                 int32_t sc;
                 uint32_t a, b, c, d;
@@ -701,7 +702,7 @@ __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, De
                         if (!(h.qs >> 31)) walk.start(qf, sp, (int32_t)qlen, (int32_t)slen, qo, so, xdrop);
                         else walk.start(qr, sp, (int32_t)qlen, (int32_t)slen, (int32_t)qlen - 1 - qo,
                                         (int32_t)slen - 1 - so, xdrop);
-                        while (walk.step4(mat) != 2) {
+                        while (walk.step(mat) != 2) {
                         }
                         walk.result(sc, a0, a1, c0, c1);
                     }

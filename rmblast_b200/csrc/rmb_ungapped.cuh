@@ -68,26 +68,6 @@ struct UngWalk {
         return on_base(end, end ? (uint8_t)15 : qb[1 + q], end ? (uint8_t)15 : sb[1 + s], mat);
     }
 
-    // Up to four bases, their loads issued together (the walk's next positions do not depend on
-    // its sums): the same as calling step() until it returns nonzero, at most four times; returns
-    // what the last call would have.
-    __host__ __device__ __forceinline__ int step4(const int32_t* mat) {
-        uint8_t a[4], c[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int32_t qj = q + dir * j, sj = s + dir * j;
-            const bool in = dir < 0 ? (qj > qlim && sj > slim) : (qj < qlim && sj < slim);
-            a[j] = in ? qb[1 + qj] : (uint8_t)15;
-            c[j] = in ? sb[1 + sj] : (uint8_t)15;
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = on_base(q == qlim || s == slim, a[j], c[j], mat);
-            if (r) return r;
-        }
-        return 0;
-    }
-
     // After step() returned 2: the extension in the walk's frame.
     __host__ __device__ __forceinline__ void result(int32_t& sc, uint32_t& q0, uint32_t& q1, uint32_t& s0,
                                                     uint32_t& s1) const {

@@ -46,24 +46,21 @@ int main(int argc, char** argv) {
         const int qo = q0 + (int)(rng() % seg), so = s0 + (qo - q0);
         const rmbo::UngappedResult want =
             rmbo::extend_ungapped(qw.data(), qw.size(), sw.data(), sw.size(), (uint32_t)qo, (uint32_t)so, mat, xdrop);
-        // one base a call (step), then four (step4): both must give the oracle's extension
-        for (int four = 0; four < 2; ++four) {
-            rmb::UngWalk w;
-            w.start(qw.data(), sw.data(), ql, sl, qo, so, xdrop);
-            int r;
-            do {
-                r = four ? w.step4(flat) : w.step(flat);
-                ++steps;
-            } while (r != 2);
-            int32_t sc;
-            uint32_t a, b, c, d;
-            w.result(sc, a, b, c, d);
-            if (sc != want.score || a != want.q_start || b != want.q_end || c != want.s_start || d != want.s_end) {
-                if (bad < 5)
-                    fprintf(stderr, "hit %d (%s): want %d %u-%u %u-%u got %d %u-%u %u-%u\n", k, four ? "step4" : "step",
-                            want.score, want.q_start, want.q_end, want.s_start, want.s_end, sc, a, b, c, d);
-                ++bad;
-            }
+        rmb::UngWalk w;
+        w.start(qw.data(), sw.data(), ql, sl, qo, so, xdrop);
+        int r;
+        do {
+            r = w.step(flat);
+            ++steps;
+        } while (r != 2);
+        int32_t sc;
+        uint32_t a, b, c, d;
+        w.result(sc, a, b, c, d);
+        if (sc != want.score || a != want.q_start || b != want.q_end || c != want.s_start || d != want.s_end) {
+            if (bad < 5)
+                fprintf(stderr, "hit %d: want %d %u-%u %u-%u got %d %u-%u %u-%u\n", k, want.score, want.q_start,
+                        want.q_end, want.s_start, want.s_end, sc, a, b, c, d);
+            ++bad;
         }
     }
     printf("hits %d bad %d steps %llu\n", n, bad, steps);
