@@ -709,7 +709,8 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             return;
         }
         ctr.ms_lookup += ms_since(t0);
-        auto qhost = [&](uint32_t local) { return QH.host.data() + QH.off[qb + local]; };
+        // by value: a deferred Phase 2b may call it after this sub-batch's body has returned
+        auto qhost = [&QH, qb](uint32_t local) { return QH.host.data() + QH.off[qb + local]; };
 
         // ---- scan: one pass that counts and stages the hits per warp, offsets, then the hits in
         // pair order (pair ids are local to the sub-batch)
@@ -1344,7 +1345,10 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
         }
 
         // ---- host Phase 2b per pair, then per query
-        auto phase2b = [&C, ns, np, out, hqlen, qhost, pair_ids, prelims = std::move(prelims),
+        // everything it reads is owned by it or outlives the caller's sub-batch (it may still run
+        // after the sub-batch body has returned, held by the sub-batch's host tail)
+        auto phase2b = [&C, ns, np, out, hqlen = std::vector<uint32_t>(hqlen, hqlen + nb), qhost, pair_ids,
+                        prelims = std::move(prelims),
                         tres = std::move(tres), pre_off = std::move(pre_off)]() mutable {
             const auto t2 = std::chrono::steady_clock::now();
             std::vector<std::vector<Hit>> pair_hits(np);
