@@ -150,30 +150,19 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
             const uint32_t* pv = Q.pv + Q.pv_off[qi];
             const uint32_t* cs = Q.cell_start + Q.cs_off[qi];
             const uint32_t* cq = Q.cell_q + Q.cq_off[qi];
-            // the word and its presence bit of a lane's position, loaded one round ahead, so
-            // those two dependent loads overlap the round before
-            uint32_t idx_c = 0, pvw_c = 0;
-            if (lane < npos) {
-                idx_c = kmer_at(pk, lane * step, v.lw);
-                pvw_c = __ldg(pv + (idx_c >> 5));
-            }
             for (uint32_t k0 = 0; k0 < npos; k0 += 32) {
                 // lane l looks up position k0 + l; its lookup cell's entries b .. b + cnt are
                 // then spread over the warp, one entry a lane, in (position, entry) order
                 const uint32_t k = k0 + lane;
                 uint32_t cnt = 0, b = 0, p = 0;
-                const uint32_t kn = k + 32;
-                uint32_t idx_n = 0;
-                if (kn < npos) idx_n = kmer_at(pk, kn * step, v.lw);
                 if (k < npos) {
                     p = k * step;
-                    if (pvw_c & (1u << (idx_c & 31))) {
-                        b = __ldg(cs + idx_c);
-                        cnt = __ldg(cs + idx_c + 1) - b;
+                    const uint32_t idx = kmer_at(pk, p, v.lw);
+                    if (__ldg(pv + (idx >> 5)) & (1u << (idx & 31))) {
+                        b = __ldg(cs + idx);
+                        cnt = __ldg(cs + idx + 1) - b;
                     }
                 }
-                uint32_t pvw_n = 0;
-                if (kn < npos) pvw_n = __ldg(pv + (idx_n >> 5));
                 uint32_t incl = cnt;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
@@ -213,8 +202,6 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
                 }
                 __syncwarp();
                 total += chunk;
-                idx_c = idx_n;
-                pvw_c = pvw_n;
             }
         }
         if (MODE != SCAN_WRITE && lane == 0) counts[w] = total;
