@@ -1230,6 +1230,11 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 tin.push_back(TbIn{pair_ids[k], p.strand, p.q_seed, p.s_seed, p.q_start, p.q_end, p.s_start, p.s_end});
         }
         std::vector<TbResult> tres(tin.size());
+        // each finished item's script stays packed in its round's ops until Phase 2b unpacks it
+        // (in parallel, per pair): round, offset and count per item
+        std::vector<std::vector<uint32_t>> rounds_ops;
+        std::vector<uint32_t> raw_round(tin.size(), 0), raw_n(tin.size(), 0);
+        std::vector<uint64_t> raw_off(tin.size(), 0);
         if (!tin.empty()) {
             uint32_t qmax = 0;
             for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
@@ -1297,6 +1302,7 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                     ctr.launches += 1;
                 }
                 std::vector<uint32_t> again;
+                const uint32_t round_id = (uint32_t)rounds_ops.size();
                 for (size_t i = 0; i < todo.size(); ++i) {
                     const TbOut& o = to[i];
                     if (o.status == 2) { again.push_back(todo[i]); continue; }
@@ -1308,12 +1314,11 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                     r.q1 = o.q1;
                     r.s0 = o.s0;
                     r.s1 = o.s1;
-                    r.script.clear();
-                    for (uint32_t k = 0; k < o.n_ops; ++k) {
-                        const uint32_t v = ops[ooff[i] + k];
-                        r.script.push_back(RunOp{(uint8_t)(v >> 30), v & 0x3fffffffu});
-                    }
+                    raw_round[todo[i]] = round_id;
+                    raw_off[todo[i]] = ooff[i];
+                    raw_n[todo[i]] = o.n_ops;
                 }
+                rounds_ops.push_back(std::move(ops));
                 if (again.size() == todo.size()) {  // nothing finished: grow the caps
                     trace_cap *= 4;
                     ops_cap *= 4;
@@ -1327,7 +1332,16 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
         }
         ctr.tb_dp += tin.size();
         ctr.ms_traceback += ms_since(t0);
+        // item k's script from its round's packed ops (op << 30 | count)
+        auto unpack = [](const std::vector<std::vector<uint32_t>>& rops, uint32_t rd, uint64_t off, uint32_t n,
+                         Script& out) {
+            out.clear();
+            if (!n) return;
+            const uint32_t* v = rops[rd].data() + off;
+            for (uint32_t j = 0; j < n; ++j) out.push_back(RunOp{(uint8_t)(v[j] >> 30), v[j] & 0x3fffffffu});
+        };
         if (taps && taps->tracebacks) {
+            for (size_t k = 0; k < tin.size(); ++k) unpack(rounds_ops, raw_round[k], raw_off[k], raw_n[k], tres[k].script);
             for (size_t k = 0; k < tin.size(); ++k) {
                 const TbResult& r = tres[k];
                 uint32_t h = 2166136261u;  // FNV-1a over the run-length ops
@@ -1349,7 +1363,9 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
         // after the sub-batch body has returned, held by the sub-batch's host tail)
         auto phase2b = [&C, ns, np, out, hqlen = std::vector<uint32_t>(hqlen, hqlen + nb), qhost, pair_ids,
                         prelims = std::move(prelims),
-                        tres = std::move(tres), pre_off = std::move(pre_off)]() mutable {
+                        tres = std::move(tres), pre_off = std::move(pre_off), rounds_ops = std::move(rounds_ops),
+                        raw_round = std::move(raw_round), raw_off = std::move(raw_off), raw_n = std::move(raw_n),
+                        unpack]() mutable {
             const auto t2 = std::chrono::steady_clock::now();
             std::vector<std::vector<Hit>> pair_hits(np);
             // the reverse complement of each query with prelims, once
@@ -1370,6 +1386,8 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 v.n_mask_rc = C.mask_off[si] >= 0 ? C.h_mask_rc.data() + C.mask_off[si] : nullptr;
                 v.len = C.slen[si];
                 std::vector<TbResult> tr(tres.begin() + pre_off[k], tres.begin() + pre_off[k + 1]);
+                for (uint64_t j = pre_off[k]; j < pre_off[k + 1]; ++j)
+                    unpack(rounds_ops, raw_round[j], raw_off[j], raw_n[j], tr[j - pre_off[k]].script);
                 pair_hits[k] = phase2b_filter(prelims[k], tr, qs, qrc.data(), hqlen[qi], v, si, C.gp);
             });
             for (size_t k = 0; k < np; ++k) {
