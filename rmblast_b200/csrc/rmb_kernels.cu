@@ -462,94 +462,81 @@ __global__ void __launch_bounds__(128) k_dedup(DevLib L, DevQueries Q, int32_t w
 // in its order per bucket, with the buckets in parallel: for hit-dense pairs (an all-against-
 // all search keeps ~1% of its hits), where extending every hit first wastes most of the work.
 constexpr int DDX_WARPS = 8;
-// a pass whose admitted hits are at most this many extends them side by side on segments of the
-// warp's lanes (ung_walk_seg); more run one a lane (UngWalk)
-constexpr int DDX_COOP = 16;
+// a pass whose admitted hits are at most this many extends them one after another with the whole
+// warp (ung_walk_warp); more run one a lane (UngWalk)
+constexpr int DDX_COOP = 6;
 // a hit-heavy pair's hits go to at most 2^DDX_GLOG_MAX bucket groups
 constexpr uint32_t DDX_GLOG_MAX = 5;
 
-// Ungapped X-drop extension by a segment of W consecutive lanes (UngWalk's result: left walk,
-// then right walk), W bases a round; the warp's 32 / W segments run one walk each (`has`: the
-// segment has one).  Every lane of the warp calls it; a segment's lanes pass the same walk and
-// get the same result.  A round scores W consecutive bases and forms the running sum P of the
-// walk and its running maximum M with segment scans.  The sequential walk's sum is P - M_before
-// (M_before: M up to the previous base), so it banks where P > M_before, and it stops at the first
-// base that is past a sequence end or has code 15 on either side, or where it does not bank and
-// P - M_before < xc: xc is -xdrop on the left, and on the right -xdrop until the first bank, then
-// max(-(left score + M_before), -xdrop).  The last bank before the stop is the extension's end, and
-// M_before at the stop its gain (checked against the one-lane walk on random walks at every W).
-template <int W>
-__device__ __forceinline__ void ung_walk_seg(bool has, const uint8_t* __restrict__ qb, const uint8_t* __restrict__ sb,
-                                             int32_t qlen, int32_t slen, int32_t wq, int32_t wsx, int32_t xdrop,
-                                             const int32_t* mat, int32_t& score, int32_t& q_beg, int32_t& q_end) {
+// Warp-cooperative ungapped X-drop extension: UngWalk's result (left walk, then right walk), 32
+// bases a round.  Every lane calls it with the same arguments and gets the same result.  A round
+// scores 32 consecutive bases and forms the running sum P of the walk and its running maximum M
+// with warp scans.  The sequential walk's sum is P - M_before (M_before: M up to the previous
+// base), so it banks where P > M_before, and it stops at the first base that is past a sequence
+// end or has code 15 on either side, or where it does not bank and P - M_before < xc: xc is
+// -xdrop on the left, and on the right -xdrop until the first bank, then
+// max(-(left score + M_before), -xdrop).  The last bank before the stop is the extension's end,
+// and M_before at the stop its gain.
+__device__ __forceinline__ void ung_walk_warp(const uint8_t* __restrict__ qb, const uint8_t* __restrict__ sb, int32_t qlen,
+                              int32_t slen, int32_t wq, int32_t wsx, int32_t xdrop, const int32_t* mat, int32_t& score,
+                              int32_t& q_beg, int32_t& q_end) {
     const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, sl = lane & (W - 1), sbase = lane & ~(W - 1);
-    const unsigned wmask = W == 32 ? FULL : ((1u << W) - 1u);
+    const int lane = threadIdx.x & 31;
     const int32_t x = -xdrop;
-    int32_t score0 = 0, P = 0, M = 0, best = wq, base = 0, dir = -1;
-    bool active = has;
-    score = 0;
-    q_beg = wq;
-    q_end = wq;
+    int32_t score0 = 0;
 #pragma unroll 1
-    while (__any_sync(FULL, active)) {
+    for (int dir = -1; dir <= 1; dir += 2) {
         const int32_t q0 = dir < 0 ? wq - 1 : wq, s0 = dir < 0 ? wsx - 1 : wsx;
-        const int32_t qj = q0 + dir * (base + sl), sj = s0 + dir * (base + sl);
-        bool hard = !active || (dir < 0 ? (qj < 0 || sj < 0) : (qj >= qlen || sj >= slen));
-        int32_t d = 0;
-        if (!hard) {
-            const uint8_t a = qb[1 + qj], c = sb[1 + sj];
-            hard = a == 15 || c == 15;
-            if (!hard) d = mat[((a & 15) << 4) | (c & 15)];
-        }
-        int32_t p = d;
+        int32_t P = 0, M = 0, best = wq, gain = 0;
+#pragma unroll 1
+        for (int32_t base = 0;; base += 32) {
+            const int32_t qj = q0 + dir * (base + lane), sj = s0 + dir * (base + lane);
+            bool hard = dir < 0 ? (qj < 0 || sj < 0) : (qj >= qlen || sj >= slen);
+            int32_t d = 0;
+            if (!hard) {
+                const uint8_t a = qb[1 + qj], c = sb[1 + sj];
+                hard = a == 15 || c == 15;
+                if (!hard) d = mat[((a & 15) << 4) | (c & 15)];
+            }
+            int32_t p = d;
 #pragma unroll
-        for (int o = 1; o < W; o <<= 1) {
-            const int32_t v = __shfl_up_sync(FULL, p, o, W);
-            if (sl >= o) p += v;
-        }
-        p += P;
-        int32_t mx = p;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t v = __shfl_up_sync(FULL, p, o);
+                if (lane >= o) p += v;
+            }
+            p += P;
+            int32_t mx = p;
 #pragma unroll
-        for (int o = 1; o < W; o <<= 1) {
-            const int32_t v = __shfl_up_sync(FULL, mx, o, W);
-            if (sl >= o) mx = max(mx, v);
-        }
-        mx = max(mx, M);
-        int32_t mprev = __shfl_up_sync(FULL, mx, 1, W);
-        if (sl == 0) mprev = M;
-        const bool bank = !hard && p > mprev;
-        const int32_t xc = dir < 0 || mprev <= 0 ? x : max(-(score0 + mprev), x);
-        const bool stop = hard || (!bank && p - mprev < xc);
-        const unsigned sm = (__ballot_sync(FULL, stop) >> sbase) & wmask;
-        const int f = sm ? __ffs((int)sm) - 1 : W;
-        const unsigned bm = ((__ballot_sync(FULL, bank) >> sbase) & wmask) & (f == 32 ? FULL : ((1u << f) - 1u));
-        const int32_t gain = __shfl_sync(FULL, mprev, f < W ? f : 0, W);
-        const int32_t Pn = __shfl_sync(FULL, p, W - 1, W), Mn = __shfl_sync(FULL, mx, W - 1, W);
-        if (active) {
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t v = __shfl_up_sync(FULL, mx, o);
+                if (lane >= o) mx = max(mx, v);
+            }
+            mx = max(mx, M);
+            int32_t mprev = __shfl_up_sync(FULL, mx, 1);
+            if (lane == 0) mprev = M;
+            const bool bank = !hard && p > mprev;
+            const int32_t xc = dir < 0 || mprev <= 0 ? x : max(-(score0 + mprev), x);
+            const bool stop = hard || (!bank && p - mprev < xc);
+            const unsigned sm = __ballot_sync(FULL, stop);
+            const int f = sm ? __ffs((int)sm) - 1 : 32;
+            const unsigned bm = __ballot_sync(FULL, bank) & (f == 32 ? FULL : ((1u << f) - 1u));
             if (bm) {
                 const int32_t ql = q0 + dir * (base + (31 - __clz((int)bm)));
                 best = dir < 0 ? ql : ql + 1;
             }
-            if (f < W) {
-                if (dir < 0) {
-                    q_beg = best;
-                    score0 = gain;
-                    dir = 1;
-                    base = 0;
-                    P = 0;
-                    M = 0;
-                    best = wq;
-                } else {
-                    q_end = best;
-                    score = score0 + gain;
-                    active = false;
-                }
-            } else {
-                P = Pn;
-                M = Mn;
-                base += W;
+            if (f < 32) {
+                gain = __shfl_sync(FULL, mprev, f);
+                break;
             }
+            P = __shfl_sync(FULL, p, 31);
+            M = __shfl_sync(FULL, mx, 31);
+        }
+        if (dir < 0) {
+            q_beg = best;
+            score0 = gain;
+        } else {
+            q_end = best;
+            score = score0 + gain;
         }
     }
 }
@@ -689,44 +676,25 @@ __global__ void __launch_bounds__(DDX_WARPS * 32, 4) k_dedup_extend(DevLib L, De
                     int32_t sc = 0;
                     uint32_t a0 = 0, a1 = 0, c0 = 0, c1 = 0;
                     const unsigned em = __ballot_sync(FULL, ext);
-                    const int ne = __popc(em);
-                    if (ne > 0 && ne <= DDX_COOP) {
-                        // the pass's extensions side by side, each on a segment of W lanes: W = 32
-                        // for one, 16 for two, ... 2 for up to 16
-                        int wseg = 32;
-                        while (wseg > 2 && 32 / wseg < ne) wseg >>= 1;
-                        const int seg = lane / wseg;
-                        const bool has = seg < ne;
-                        unsigned m = em;
-                        for (int k = 0; k < seg && m; ++k) m &= m - 1u;
-                        const int src = has ? __ffs((int)m) - 1 : 0;
-                        const uint32_t hqs = __shfl_sync(FULL, h.qs, src), hs = __shfl_sync(FULL, h.s, src);
-                        const bool minus = hqs >> 31;
-                        const int32_t qo = (int32_t)(hqs & 0x7fffffffu), so = (int32_t)hs;
-                        const int32_t wq = minus ? (int32_t)qlen - 1 - qo : qo;
-                        const int32_t wsx = minus ? (int32_t)slen - 1 - so : so;
-                        const uint8_t* qw = minus ? qr : qf;
-                        int32_t s_ = 0, qb_ = 0, qe_ = 0;
-                        switch (wseg) {
-                            case 32: ung_walk_seg<32>(has, qw, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_, qe_); break;
-                            case 16: ung_walk_seg<16>(has, qw, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_, qe_); break;
-                            case 8: ung_walk_seg<8>(has, qw, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_, qe_); break;
-                            case 4: ung_walk_seg<4>(has, qw, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_, qe_); break;
-                            default: ung_walk_seg<2>(has, qw, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_, qe_); break;
-                        }
-                        // each extending lane takes its segment's result (segment = its rank in em)
-                        const int from = ext ? __popc(em & ((1u << lane) - 1u)) * wseg : lane;
-                        const int32_t rs = __shfl_sync(FULL, s_, from), rb = __shfl_sync(FULL, qb_, from),
-                                      re = __shfl_sync(FULL, qe_, from);
-                        if (ext) {
-                            const int32_t oq = (int32_t)(h.qs & 0x7fffffffu), os = (int32_t)h.s;
-                            const int32_t mq = (h.qs >> 31) ? (int32_t)qlen - 1 - oq : oq;
-                            const int32_t ms = (h.qs >> 31) ? (int32_t)slen - 1 - os : os;
-                            sc = rs;
-                            a0 = (uint32_t)rb;
-                            a1 = (uint32_t)re;
-                            c0 = (uint32_t)(ms - (mq - rb));
-                            c1 = (uint32_t)(ms + (re - mq));
+                    if (em && __popc(em) <= DDX_COOP) {
+                        // few extensions: each with the whole warp, one after another
+                        for (unsigned m = em; m; m &= m - 1u) {
+                            const int src = __ffs((int)m) - 1;
+                            const uint32_t hqs = __shfl_sync(FULL, h.qs, src), hs = __shfl_sync(FULL, h.s, src);
+                            const bool minus = hqs >> 31;
+                            const int32_t qo = (int32_t)(hqs & 0x7fffffffu), so = (int32_t)hs;
+                            const int32_t wq = minus ? (int32_t)qlen - 1 - qo : qo;
+                            const int32_t wsx = minus ? (int32_t)slen - 1 - so : so;
+                            int32_t s_, qb_, qe_;
+                            ung_walk_warp(minus ? qr : qf, sp, (int32_t)qlen, (int32_t)slen, wq, wsx, xdrop, mat, s_, qb_,
+                                          qe_);
+                            if (lane == src) {
+                                sc = s_;
+                                a0 = (uint32_t)qb_;
+                                a1 = (uint32_t)qe_;
+                                c0 = (uint32_t)(wsx - (wq - qb_));
+                                c1 = (uint32_t)(wsx + (qe_ - wq));
+                            }
                         }
                     } else if (ext) {
                         const int32_t qo = (int32_t)(h.qs & 0x7fffffffu), so = (int32_t)h.s;
