@@ -153,10 +153,15 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 // while the other's kernels do, and the kernels of both fill each other's launch tails.
 struct Work {
     cudaStream_t st = nullptr;
+    // the batched pipeline's traceback of a range, beside the lane's next kernels; tb_mu keeps
+    // one traceback at a time on the lane's traceback buffers (a sub-batch's last one can still
+    // run when the next sub-batch's first starts)
+    cudaStream_t st2 = nullptr;
+    std::mutex tb_mu;
     DBuf pv, pv_off, cs, cs_off, cq, cq_off, pos_off, lut_keys, lut_vals, lut_keys2, lut_vals2, lut_counts;
     DBuf counts, offs, hits, hit_pair, ub, flags, dd_scratch, dd_cells, ung_idx, n_sel, po, wide, wide2, dres, geo,
         n_wide, band, sel, surv, cells, fails, temp, tb_in, tb_out, tb_ops, tb_scratch, stage, stage_start, stage_over,
-        tb_ooff, tb_ops2, ung_queue, dd_units, tb_half;
+        tb_ooff, tb_ops2, ung_queue, dd_units, tb_half, tb_cells;
     DBuf sched_pred, sched_order, sched_scratch, sched_feat, sched_cells;
     // the device chain as a CUDA graph (chain_graph): its executable, its timing events and the
     // pinned block its counts come back in
@@ -175,9 +180,11 @@ struct Work {
                        &lut_vals2, &lut_counts, &counts, &offs, &hits, &hit_pair, &ub, &flags, &dd_scratch, &dd_cells,
                        &ung_idx, &n_sel, &po, &wide, &wide2, &dres, &geo, &n_wide, &band, &sel, &surv, &cells, &fails,
                        &temp, &tb_in, &tb_out, &tb_ops, &tb_scratch, &stage, &stage_start, &stage_over, &tb_ooff,
-                       &tb_ops2, &ung_queue, &dd_units, &tb_half, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
+                       &tb_ops2, &ung_queue, &dd_units, &tb_half, &tb_cells, &sched_pred, &sched_order, &sched_scratch, &sched_feat, &sched_cells};
         for (DBuf* b : all) b->release();
         if (st) cudaStreamDestroy(st);
+        if (st2) cudaStreamDestroy(st2);
+        st2 = nullptr;
         st = nullptr;
     }
 };
@@ -315,7 +322,7 @@ struct PairPrelims {
 bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
                   const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
                   std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps,
-                  std::future<double>* defer = nullptr);
+                  std::future<rmb_counters>* defer = nullptr);
 
 // The per-query end of a search: E-values and bit scores (rmstats RmStats for the query's length
 // against the whole database), the --evalue reap (main.rs:1224-1226, before masklevel), then
@@ -631,7 +638,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
     // With `tail`, the sub-batch's last host steps (the pending Phase 2b, masklevel and the hit
     // order) run on a thread of their own, *tail holding them (their host ms and hits), so the
     // next sub-batch's kernels start at once.
-    using Tail = std::future<std::pair<double, uint64_t>>;
+    using Tail = std::future<rmb_counters>;
     auto sub_batch = [&](Work& W, uint32_t qb, uint32_t qe, rmb_counters& ctr, Tail* tail) {
         cudaStream_t st = W.st;
         const uint32_t nb = qe - qb;
@@ -640,9 +647,9 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         std::vector<uint64_t> hpvoff(nb), hcsoff(nb), hposoff(nb), hzero(nb, 0);
         std::vector<uint32_t> hqlen(qlen + qb, qlen + qe);
         std::vector<int32_t> hlw(lw_all.begin() + qb, lw_all.begin() + qe);
-        // the batched pipeline's host Phase 2b of the last range, running while the next one's
-        // kernels do (declared here: it reads hqlen and writes out_hits)
-        std::future<double> pending;
+        // the batched pipeline's traceback and host Phase 2b of the last range, running while the
+        // next one's kernels do (it writes out_hits; its counters come back with it)
+        std::future<rmb_counters> pending;
         uint64_t npv = 0, ncs = 0, npos = 0;
         for (uint32_t i = 0; i < nb; ++i) {
             hpvoff[i] = npv;
@@ -1135,7 +1142,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
             }
 
             // ---- traceback DP and host Phase 2b of every prelim
-            if (pending.valid()) ctr.ms_host_2b += pending.get();
+            if (pending.valid()) add_counters(ctr, pending.get());
             if (traceback_2b(C, W, Q, hqlen.data(), nb, qhost, pair_ids, prelims, out_hits.data() + qb, ctr, taps,
                              P.pipeline != 1 && !taps ? &pending : nullptr)) {
                 tapped = true;
@@ -1144,16 +1151,17 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         }
         if (tail && !tapped && !collect) {
             *tail = std::async(std::launch::async, [&C, &out_hits, qb, nb, hqlen, pending = std::move(pending)]() mutable {
-                double ms = pending.valid() ? pending.get() : 0.0;
+                rmb_counters c{};
+                if (pending.valid()) c = pending.get();
                 const auto t3 = std::chrono::steady_clock::now();
                 parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
-                uint64_t finals = 0;
-                for (uint32_t i = 0; i < nb; ++i) finals += out_hits[qb + i].size();
-                return std::make_pair(ms + ms_since(t3), finals);
+                for (uint32_t i = 0; i < nb; ++i) c.finals += out_hits[qb + i].size();
+                c.ms_host_2b += ms_since(t3);
+                return c;
             });
             return;
         }
-        if (pending.valid()) ctr.ms_host_2b += pending.get();
+        if (pending.valid()) add_counters(ctr, pending.get());
         if (tapped || collect) return;
         t0 = std::chrono::steady_clock::now();
         parallel_for(nb, [&](size_t i) { finish_query(C, out_hits[qb + i], hqlen[i]); });
@@ -1165,10 +1173,7 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         const bool overlap = P.pipeline != 1 && !taps && !collect;
         Tail last;
         auto join = [&]() {
-            if (!last.valid()) return;
-            const auto r = last.get();
-            ctr.ms_host_2b += r.first;
-            ctr.finals += r.second;
+            if (last.valid()) add_counters(ctr, last.get());
         };
         for (auto& sb : subs) {
             Tail next;
@@ -1205,17 +1210,23 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
 // Traceback DP on the device and the host Phase 2b (engine.rs:1438-1762) of the prelims of
 // (query, subject) pairs; pair = local query * n_subjects + subject over the queries of Q, whose
 // lengths are hqlen and host copies qhost(local).  Hits go to out[local query].  Returns true
-// when the traceback stage tap took the results instead.  With `defer`, the host Phase 2b runs
-// on a thread of its own and *defer holds it (its host ms): the caller waits for it before the
-// next call that writes the same queries' hits, and before it reads them.
-bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen, uint32_t nb,
-                  const std::function<const uint8_t*(uint32_t)>& qhost, const std::vector<uint32_t>& pair_ids,
-                  std::vector<std::vector<Prelim>>& prelims, std::vector<Hit>* out, rmb_counters& ctr, Taps* taps,
-                  std::future<double>* defer) {
+// when the traceback stage tap took the results instead.  With `defer` (no taps), the whole step,
+// the traceback kernels on the lane's second stream and the host Phase 2b, runs on a thread of
+// its own and *defer holds it (its counters): the caller waits for it before the next call (the
+// traceback buffers and the hits of the same queries) and before it reads the hits.
+bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqlen_in, uint32_t nb,
+                  const std::function<const uint8_t*(uint32_t)>& qhost_in, const std::vector<uint32_t>& pair_ids_in,
+                  std::vector<std::vector<Prelim>>& prelims_in, std::vector<Hit>* out, rmb_counters& ctr_in,
+                  Taps* taps, std::future<rmb_counters>* defer) {
+  // everything the job reads is owned by it or outlives the caller's sub-batch
+  auto job = [&C, &W, Q, nb, out, taps, hq = std::vector<uint32_t>(hqlen_in, hqlen_in + nb), qhost = qhost_in,
+              pair_ids = pair_ids_in, prelims = std::move(prelims_in)](rmb_counters& ctr,
+                                                                      cudaStream_t st) mutable -> bool {
+    const uint32_t* hqlen = hq.data();
     const uint32_t ns = (uint32_t)C.ids.size();
     const size_t np = pair_ids.size();
-    cudaStream_t st = W.st;
     unsigned long long cells = 0;
+    std::unique_lock<std::mutex> tb_lock(W.tb_mu);  // the lane's traceback buffers, until the results are back
     auto t0 = std::chrono::steady_clock::now();
     {
         // ---- traceback DP of every prelim (GPU), with retries for scratch overflow
@@ -1271,19 +1282,20 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                 W.tb_half.ensure(2 * todo.size() * sizeof(TbHalf));
                 W.tb_ops.ensure(2 * todo.size() * (uint64_t)ops_cap * 4);
                 W.tb_scratch.ensure((uint64_t)threads * per_thread);
-                CK(cudaMemsetAsync(W.cells.p, 0, 8, st));
+                W.tb_cells.ensure(8);
+                CK(cudaMemsetAsync(W.tb_cells.p, 0, 8, st));
                 EvTimer et;
                 et.start(st);
                 ctr.launches += 2;
                 CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), W.tb_in.as<TbIn>(),
                                     W.tb_out.as<TbOut>(), W.tb_half.as<TbHalf>(), W.tb_ops.as<uint32_t>(), ops_cap,
                                     W.tb_scratch.as<uint8_t>(),
-                                    per_thread, band_cells, rows_cap, threads, W.cells.as<unsigned long long>(), whole,
-                                    st));
+                                    per_thread, band_cells, rows_cap, threads, W.tb_cells.as<unsigned long long>(),
+                                    whole, st));
                 et.stop(st);
                 std::vector<TbOut> to(todo.size());
                 CK(cudaMemcpyAsync(to.data(), W.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(&cells, W.cells.p, 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&cells, W.tb_cells.p, 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 ctr.gpu_ms_traceback += et.ms();
                 // only the ops of the finished items come back, packed
@@ -1331,6 +1343,7 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
             }
         }
         ctr.tb_dp += tin.size();
+        tb_lock.unlock();  // the results are on the host
         ctr.ms_traceback += ms_since(t0);
         // item k's script from its round's packed ops (op << 30 | count)
         auto unpack = [](const std::vector<std::vector<uint32_t>>& rops, uint32_t rd, uint64_t off, uint32_t n,
@@ -1400,11 +1413,22 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
             }
             return ms_since(t2);
         };
-        if (defer) *defer = std::async(std::launch::async, std::move(phase2b));
-        else ctr.ms_host_2b += phase2b();
+        ctr.ms_host_2b += phase2b();
     }
-    (void)nb;
     return false;
+  };
+  if (defer) {
+      const int dev = C.p.device;
+      cudaStream_t st2 = W.st2;
+      *defer = std::async(std::launch::async, [job = std::move(job), dev, st2]() mutable {
+          CK(cudaSetDevice(dev));
+          rmb_counters c{};
+          job(c, st2);
+          return c;
+      });
+      return false;
+  }
+  return job(ctr_in, W.st);
 }
 
 int fail_out(const std::exception& e, char* err, size_t errlen, int code) {
@@ -1457,7 +1481,10 @@ int rmb_ctx_create(const rmb_params* params, const int32_t scores[256], const do
         if (prop.major < 10) throw Fail(RMB_EINVAL, "this library is built for sm_100a (B200)");
         C->sms = prop.multiProcessorCount;
         CK(cudaStreamCreateWithFlags(&C->st, cudaStreamNonBlocking));
-        for (Work& w : C->work) CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking));
+        for (Work& w : C->work) {
+            CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithFlags(&w.st2, cudaStreamNonBlocking));
+        }
         DevParams dp{};
         dp.gap_open = p.gap_open;
         dp.gap_extend = p.gap_extend;
