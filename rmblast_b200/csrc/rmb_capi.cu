@@ -727,12 +727,12 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         W.offs.ensure((npairs + 1) * 8);
         W.stage_start.ensure(npairs * 4);
         W.stage.ensure(scan_stage_entries(npairs, C.sms) * sizeof(SeedHit));
-        W.stage_over.ensure(4);
+        W.stage_over.ensure(16);  // the overflow flag and the scan's pair queue
         CK(cudaMemsetAsync(W.counts.p, 0, (npairs + 1) * 4, st));
-        CK(cudaMemsetAsync(W.stage_over.p, 0, 4, st));
+        CK(cudaMemsetAsync(W.stage_over.p, 0, 16, st));
         ev.start(st);
         CK(launch_scan_stage(C.L, Q, P.word_size, npairs, W.counts.as<uint32_t>(), W.stage_start.as<uint32_t>(),
-                             W.stage.as<SeedHit>(), W.stage_over.as<unsigned int>(), C.sms, st));
+                             W.stage.as<SeedHit>(), W.stage_over.as<unsigned int>(), C.sms, st, P.pipeline != 1));
         size_t tb = 0;
         CK(launch_offsets(W.counts.as<uint32_t>(), npairs + 1, W.offs.as<uint64_t>(), nullptr, tb, st));
         W.temp.ensure(tb);

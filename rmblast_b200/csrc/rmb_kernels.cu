@@ -119,7 +119,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
                                                uint32_t* counts, const uint64_t* offs, SeedHit* hits,
                                                uint32_t* hit_pair, uint32_t* stage_start, uint32_t stage_cap,
-                                               unsigned int* stage_over) {
+                                               unsigned int* stage_over, unsigned long long* pair_queue) {
     constexpr bool WRITE = MODE != SCAN_COUNT;
     // per warp: each lane's first candidate index, lookup-cell start and scan position
     __shared__ uint32_t s_first[8][32], s_cell[8][32], s_pos[8][32];
@@ -129,7 +129,20 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
     const uint32_t stage0 = MODE == SCAN_STAGE ? (uint32_t)warp * stage_cap : 0u;  // this warp's stretch
     uint32_t cursor = 0;                                                            // entries of it used
     bool fits = true;
-    for (uint64_t w = warp; w < n_pairs; w += nwarps) {
+    // pairs by warp stride, or, with pair_queue, the next pair off a grid-wide counter as a warp
+    // finishes one (subject lengths vary 100-fold, so fixed strides leave warps idle at the end)
+    uint64_t w_next = warp;
+    auto next_pair = [&]() -> uint64_t {
+        if (pair_queue) {
+            unsigned long long x = 0;
+            if (lane == 0) x = atomicAdd(pair_queue, 1ull);
+            return __shfl_sync(0xffffffffu, x, 0);
+        }
+        const uint64_t r = w_next;
+        w_next += nwarps;
+        return r;
+    };
+    for (uint64_t w = next_pair(); w < n_pairs; w = next_pair()) {
         const uint64_t pair = pair0 + w;
         const uint32_t qi = (uint32_t)(pair / L.n), si = (uint32_t)(pair % L.n);
         const uint32_t qlen = Q.len[qi], slen = L.len[si];
@@ -2161,10 +2174,10 @@ cudaError_t launch_scan(bool write, const DevLib& L, const DevQueries& Q, int32_
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
     if (write)
         k_scan<SCAN_WRITE><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair, nullptr,
-                                                   0, nullptr);
+                                                   0, nullptr, nullptr);
     else
         k_scan<SCAN_COUNT><<<grid, block, 0, st>>>(L, Q, ws, pair0, n_pairs, counts, offs, hits, hit_pair, nullptr,
-                                                   0, nullptr);
+                                                   0, nullptr, nullptr);
     return cudaGetLastError();
 }
 
@@ -2174,11 +2187,14 @@ uint64_t scan_stage_entries(uint64_t n_pairs, int sms) {
 
 cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t n_pairs, uint32_t* counts,
                               uint32_t* stage_start, SeedHit* stage, unsigned int* stage_over, int sms,
-                              cudaStream_t st) {
+                              cudaStream_t st, bool queue) {
+    // stage_over: [0] the overflow flag, [2..3] the pair queue (both zeroed by the caller); without
+    // `queue` the warps take pairs by stride (the plain pipeline)
     const int block = 256;
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
     k_scan<SCAN_STAGE><<<grid, block, 0, st>>>(L, Q, ws, 0, n_pairs, counts, nullptr, stage, nullptr, stage_start,
-                                               SCAN_STAGE_PER_WARP, stage_over);
+                                               SCAN_STAGE_PER_WARP, stage_over,
+                                               queue ? reinterpret_cast<unsigned long long*>(stage_over + 2) : nullptr);
     return cudaGetLastError();
 }
 

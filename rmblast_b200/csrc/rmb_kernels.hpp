@@ -18,7 +18,7 @@ constexpr uint32_t SCAN_STAGE_PER_WARP = 32768;
 uint64_t scan_stage_entries(uint64_t n_pairs, int sms);
 cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, uint64_t n_pairs, uint32_t* counts,
                               uint32_t* stage_start, SeedHit* stage, unsigned int* stage_over, int sms,
-                              cudaStream_t st);
+                              cudaStream_t st, bool queue);
 cudaError_t launch_scan_gather(uint64_t pair0, uint64_t n_pairs, const uint32_t* counts, const uint64_t* offs,
                                const uint32_t* stage_start, const SeedHit* stage, SeedHit* hits, uint32_t* hit_pair,
                                int sms, cudaStream_t st);
