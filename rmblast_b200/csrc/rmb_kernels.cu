@@ -114,6 +114,7 @@ __device__ __forceinline__ bool exact_extend(const PairView& v, uint32_t q0c, ui
 //               from warp * stage_cap), the pair's first entry in stage_start; if a stretch runs
 //               out, *stage_over is set and the batch takes the SCAN_WRITE pass instead.
 enum { SCAN_COUNT = 0, SCAN_WRITE = 1, SCAN_STAGE = 2 };
+constexpr uint32_t SCAN_QUEUE_RUN = 8;
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
@@ -129,14 +130,18 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
     const uint32_t stage0 = MODE == SCAN_STAGE ? (uint32_t)warp * stage_cap : 0u;  // this warp's stretch
     uint32_t cursor = 0;                                                            // entries of it used
     bool fits = true;
-    // pairs by warp stride, or, with pair_queue, the next pair off a grid-wide counter as a warp
-    // finishes one (subject lengths vary 100-fold, so fixed strides leave warps idle at the end)
-    uint64_t w_next = warp;
+    // pairs by warp stride, or, with pair_queue, the next run of SCAN_QUEUE_RUN consecutive pairs
+    // off a grid-wide counter as a warp finishes one (subject lengths vary 100-fold, so fixed
+    // strides leave warps idle at the end; a run's pairs share their query's tables in L1)
+    uint64_t w_next = warp, run_end = 0;
     auto next_pair = [&]() -> uint64_t {
         if (pair_queue) {
+            if (w_next < run_end) return w_next++;
             unsigned long long x = 0;
-            if (lane == 0) x = atomicAdd(pair_queue, 1ull);
-            return __shfl_sync(0xffffffffu, x, 0);
+            if (lane == 0) x = atomicAdd(pair_queue, (unsigned long long)SCAN_QUEUE_RUN);
+            w_next = __shfl_sync(0xffffffffu, x, 0);
+            run_end = w_next + SCAN_QUEUE_RUN;
+            return w_next++;
         }
         const uint64_t r = w_next;
         w_next += nwarps;
