@@ -2197,11 +2197,11 @@ cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, 
     // `queue` the warps take pairs by stride (the plain pipeline)
     const int block = 256;
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
-    // the queue pays where a warp gets few pairs (its strides' lengths then vary the most); with
+    // the queue pays where a warp gets few pairs (under 64: its strides' lengths vary the most); with
     // many pairs a warp, fixed strides balance and keep a block's warps on one query's tables in
     // L1 (measured: config 3's sub-batches 54 -> 41 ms with the queue, config 1's 2 M pairs
     // 75 -> 115 ms)
-    const bool use_queue = queue && n_pairs < (uint64_t)grid * (block / 32) * 32;
+    const bool use_queue = queue && n_pairs < (uint64_t)grid * (block / 32) * 64;
     k_scan<SCAN_STAGE><<<grid, block, 0, st>>>(L, Q, ws, 0, n_pairs, counts, nullptr, stage, nullptr, stage_start,
                                                SCAN_STAGE_PER_WARP, stage_over,
                                                use_queue ? reinterpret_cast<unsigned long long*>(stage_over + 2) : nullptr);
