@@ -315,7 +315,7 @@ __device__ __forceinline__ void extend_ungapped(const uint8_t* query, int64_t q_
 // 16 steps a round: the walks at the default size run hundreds of bases, so fewer refills pay
 // for the idle steps after a walk ends (8 measured 49-50 ms, 16 47 ms a step).  Four bases a
 // step with their loads issued together measured slower, on this kernel (27 -> 32 ms a step on
-// config 3's workload) and in the fused dedup's lane walks
+// 1,000 queries of 1-200 kb) and in the fused dedup's lane walks
 constexpr int UNG_GROUP = 16;
 // QUEUE: a persistent grid whose lanes take hits from a grid-wide queue as their walks end (the
 // batched pipeline); otherwise one hit per thread, thread i taking hit i (the plain pipeline).
@@ -2199,8 +2199,8 @@ cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, 
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
     // the queue pays where a warp gets few pairs (under 64: its strides' lengths vary the most); with
     // many pairs a warp, fixed strides balance and keep a block's warps on one query's tables in
-    // L1 (measured: config 3's sub-batches 54 -> 41 ms with the queue, config 1's 2 M pairs
-    // 75 -> 115 ms)
+    // L1 (measured: sub-batches of ~150 queries of 1-200 kb, 54 -> 41 ms with the queue; 1,000
+    // queries of 60 kb, 2 M pairs, 75 -> 115 ms)
     const bool use_queue = queue && n_pairs < (uint64_t)grid * (block / 32) * 64;
     k_scan<SCAN_STAGE><<<grid, block, 0, st>>>(L, Q, ws, 0, n_pairs, counts, nullptr, stage, nullptr, stage_start,
                                                SCAN_STAGE_PER_WARP, stage_over,
