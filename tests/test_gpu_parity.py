@@ -546,8 +546,8 @@ def _config_case(name: str, scale: float, **kw):
     return txt, want, res, ctr
 
 
-def test_config0_full_size_matches_oracle():
-    """Config 0 at its full size: the 100 kb genome with 300 planted copies against 50 consensi,
+def test_small_workload_full_size_matches_oracle():
+    """The small workload at its full size: the 100 kb genome with 300 planted copies against 50 consensi,
     word 7, every line against the oracle."""
     txt, want, res, ctr = _config_case("small", 1.0)
     assert txt == want
@@ -555,8 +555,8 @@ def test_config0_full_size_matches_oracle():
     assert res.counters["ungapped"] == ctr["ungapped"]
 
 
-def test_config1_full_size_matches_oracle():
-    """Config 1 at its full size: all 1,000 chunks of 60 kb (60 Mb) against the 2,000-consensus
+def test_plain_workload_full_size_matches_oracle():
+    """The plain workload at its full size: all 1,000 chunks of 60 kb (60 Mb) against the 2,000-consensus
     library, word 11, through the batched pipeline (tuned defaults, the device chain as a graph); every one of the
     ~25,000 lines against the oracle (about a minute on 16 host cores)."""
     txt, want, res, ctr = _config_case("plain", 1.0)
@@ -565,8 +565,8 @@ def test_config1_full_size_matches_oracle():
     assert res.counters["ungapped"] == ctr["ungapped"] and res.counters["prelims"] >= ctr["prelims"]
 
 
-def test_config1_fifty_chunks_matches_oracle():
-    """Config 1's shape at 50 of its 1,000 chunks of 60 kb (3 Mb) against the 2,000-consensus
+def test_plain_workload_fifty_chunks_matches_oracle():
+    """The plain workload's shape at 50 of its 1,000 chunks of 60 kb (3 Mb) against the 2,000-consensus
     library, word 11."""
     txt, want, res, ctr = _config_case("plain", 0.05)
     assert txt.count("\n") > 500
@@ -575,8 +575,8 @@ def test_config1_fifty_chunks_matches_oracle():
 
 
 @pytest.mark.parametrize("schedule", [1, 2])
-def test_config3_learned_order_matches_oracle(schedule):
-    """Config 3: chunks of 1-200 kb through the batched pipeline with the learned record order
+def test_batched_workload_learned_order_matches_oracle(schedule):
+    """The batched workload: chunks of 1-200 kb through the batched pipeline with the learned record order
     (the committed network; front-loaded and full cost order), every line against the oracle."""
     txt, want, res, ctr = _config_case("batched", 0.005, schedule=schedule)
     assert txt.count("\n") > 500
