@@ -1218,217 +1218,217 @@ bool traceback_2b(rmb_ctx& C, Work& W, const DevQueries& Q, const uint32_t* hqle
                   const std::function<const uint8_t*(uint32_t)>& qhost_in, const std::vector<uint32_t>& pair_ids_in,
                   std::vector<std::vector<Prelim>>& prelims_in, std::vector<Hit>* out, rmb_counters& ctr_in,
                   Taps* taps, std::future<rmb_counters>* defer) {
-  // everything the job reads is owned by it or outlives the caller's sub-batch
-  auto job = [&C, &W, Q, nb, out, taps, hq = std::vector<uint32_t>(hqlen_in, hqlen_in + nb), qhost = qhost_in,
-              pair_ids = pair_ids_in, prelims = std::move(prelims_in)](rmb_counters& ctr,
-                                                                      cudaStream_t st) mutable -> bool {
-    const uint32_t* hqlen = hq.data();
-    const uint32_t ns = (uint32_t)C.ids.size();
-    const size_t np = pair_ids.size();
-    unsigned long long cells = 0;
-    std::unique_lock<std::mutex> tb_lock(W.tb_mu);  // the lane's traceback buffers, until the results are back
-    auto t0 = std::chrono::steady_clock::now();
-    {
-        // ---- traceback DP of every prelim (GPU), with retries for scratch overflow
-        uint64_t n_pre = 0;
-        for (auto& v : prelims) n_pre += v.size();
-        std::vector<TbIn> tin;
-        tin.reserve(n_pre);
-        std::vector<uint64_t> pre_off(np + 1, 0);
-        for (size_t k = 0; k < np; ++k) {
-            pre_off[k + 1] = pre_off[k] + prelims[k].size();
-            for (const Prelim& p : prelims[k])
-                tin.push_back(TbIn{pair_ids[k], p.strand, p.q_seed, p.s_seed, p.q_start, p.q_end, p.s_start, p.s_end});
-        }
-        std::vector<TbResult> tres(tin.size());
-        // each finished item's script stays packed in its round's ops until Phase 2b unpacks it
-        // (in parallel, per pair): round, offset and count per item
-        std::vector<std::vector<uint32_t>> rounds_ops;
-        std::vector<uint32_t> raw_round(tin.size(), 0), raw_n(tin.size(), 0);
-        std::vector<uint64_t> raw_off(tin.size(), 0);
-        if (!tin.empty()) {
-            uint32_t qmax = 0;
-            for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
-            // batched: largest prelim boxes first (warps take items round-robin, so the long
-            // alignments start in the first wave instead of stretching the end of the launch);
-            // plain: in arrival order
-            std::vector<uint32_t> todo(tin.size());
-            for (uint32_t i = 0; i < todo.size(); ++i) todo[i] = i;
-            auto box = [&](uint32_t i) {
-                return (uint64_t)(tin[i].q_end - tin[i].q_start) + (uint64_t)(tin[i].s_end - tin[i].s_start);
-            };
-            if (C.p.pipeline != 1)
-                std::stable_sort(todo.begin(), todo.end(), [&](uint32_t x, uint32_t y) { return box(x) > box(y); });
-            uint64_t trace_cap = 1ull << 20;
-            uint32_t ops_cap = 1024;
-            int rounds = 0;
-            while (!todo.empty()) {
-                if (++rounds > 12) throw Fail(RMB_ENOMEM, "traceback scratch kept overflowing");
-                std::vector<TbIn> chunk_in(todo.size());
-                for (size_t i = 0; i < todo.size(); ++i) chunk_in[i] = tin[todo[i]];
-                const uint64_t band_cells = (uint64_t)C.max_slen + 2;
-                const uint32_t rows_cap = qmax + 2;
-                const uint64_t per_thread = ((band_cells * 8 + (uint64_t)rows_cap * 8 + trace_cap) + 255) & ~255ull;
-                const uint64_t budget = 8ull << 30;
-                // one warp per scratch slot (two items, the left and the right extension, per
-                // prelim), blocks of 8 warps
-                // (the plain pipeline: one prelim per warp, its two extensions in turn)
-                const bool whole = C.p.pipeline == 1;
-                uint32_t threads = (uint32_t)std::min<uint64_t>((whole ? 1 : 2) * todo.size(),
-                                                                std::max<uint64_t>(8, budget / per_thread));
-                threads = (threads + 7) / 8 * 8;
-                upload(W.tb_in, chunk_in, st);
-                W.tb_out.ensure(todo.size() * sizeof(TbOut));
-                W.tb_half.ensure(2 * todo.size() * sizeof(TbHalf));
-                W.tb_ops.ensure(2 * todo.size() * (uint64_t)ops_cap * 4);
-                W.tb_scratch.ensure((uint64_t)threads * per_thread);
-                W.tb_cells.ensure(8);
-                CK(cudaMemsetAsync(W.tb_cells.p, 0, 8, st));
-                EvTimer et;
-                et.start(st);
-                ctr.launches += 2;
-                CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), W.tb_in.as<TbIn>(),
-                                    W.tb_out.as<TbOut>(), W.tb_half.as<TbHalf>(), W.tb_ops.as<uint32_t>(), ops_cap,
-                                    W.tb_scratch.as<uint8_t>(),
-                                    per_thread, band_cells, rows_cap, threads, W.tb_cells.as<unsigned long long>(),
-                                    whole, st));
-                et.stop(st);
-                std::vector<TbOut> to(todo.size());
-                CK(cudaMemcpyAsync(to.data(), W.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(&cells, W.tb_cells.p, 8, cudaMemcpyDeviceToHost, st));
-                CK(cudaStreamSynchronize(st));
-                ctr.gpu_ms_traceback += et.ms();
-                // only the ops of the finished items come back, packed
-                std::vector<uint64_t> ooff(todo.size() + 1, 0);
-                for (size_t i = 0; i < todo.size(); ++i)
-                    ooff[i + 1] = ooff[i] + (to[i].status == 2 ? 0 : to[i].n_ops);
-                std::vector<uint32_t> ops(ooff.back());
-                if (!ops.empty()) {
-                    upload(W.tb_ooff, ooff, st);
-                    W.tb_ops2.ensure(ops.size() * 4);
-                    // the merged script of prelim i sits in ops slot 2 i
-                    CK(launch_gather_ops((uint32_t)todo.size(), W.tb_ops.as<uint32_t>(), 2 * ops_cap, W.tb_out.as<TbOut>(),
-                                         W.tb_ooff.as<uint64_t>(), W.tb_ops2.as<uint32_t>(), C.sms, st));
-                    CK(cudaMemcpyAsync(ops.data(), W.tb_ops2.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
-                    CK(cudaStreamSynchronize(st));
-                    ctr.launches += 1;
-                }
-                std::vector<uint32_t> again;
-                const uint32_t round_id = (uint32_t)rounds_ops.size();
-                for (size_t i = 0; i < todo.size(); ++i) {
-                    const TbOut& o = to[i];
-                    if (o.status == 2) { again.push_back(todo[i]); continue; }
-                    if (o.status == 3) throw Fail(RMB_ECUDA, "traceback walk did not reach the origin");
-                    TbResult& r = tres[todo[i]];
-                    r.status = o.status;
-                    r.score = o.score;
-                    r.q0 = o.q0;
-                    r.q1 = o.q1;
-                    r.s0 = o.s0;
-                    r.s1 = o.s1;
-                    raw_round[todo[i]] = round_id;
-                    raw_off[todo[i]] = ooff[i];
-                    raw_n[todo[i]] = o.n_ops;
-                }
-                rounds_ops.push_back(std::move(ops));
-                if (again.size() == todo.size()) {  // nothing finished: grow the caps
-                    trace_cap *= 4;
-                    ops_cap *= 4;
-                } else if (!again.empty()) {
-                    trace_cap *= 4;
-                    ops_cap *= 4;
-                }
-                ctr.tb_cells += cells;
-                todo.swap(again);
-            }
-        }
-        ctr.tb_dp += tin.size();
-        tb_lock.unlock();  // the results are on the host
-        ctr.ms_traceback += ms_since(t0);
-        // item k's script from its round's packed ops (op << 30 | count)
-        auto unpack = [](const std::vector<std::vector<uint32_t>>& rops, uint32_t rd, uint64_t off, uint32_t n,
-                         Script& out) {
-            out.clear();
-            if (!n) return;
-            const uint32_t* v = rops[rd].data() + off;
-            for (uint32_t j = 0; j < n; ++j) out.push_back(RunOp{(uint8_t)(v[j] >> 30), v[j] & 0x3fffffffu});
-        };
-        if (taps && taps->tracebacks) {
-            for (size_t k = 0; k < tin.size(); ++k) unpack(rounds_ops, raw_round[k], raw_off[k], raw_n[k], tres[k].script);
-            for (size_t k = 0; k < tin.size(); ++k) {
-                const TbResult& r = tres[k];
-                uint32_t h = 2166136261u;  // FNV-1a over the run-length ops
-                for (const RunOp& o : r.script) {
-                    const uint32_t v = ((uint32_t)o.op << 30) | o.n;
-                    for (int b = 0; b < 4; ++b) h = (h ^ ((v >> (8 * b)) & 0xffu)) * 16777619u;
-                }
-                const bool ok = r.status == 0;
-                taps->tracebacks->insert(taps->tracebacks->end(),
-                                         {tin[k].strand, ok ? 0u : 1u, ok ? (uint32_t)r.score : 0u, ok ? r.q0 : 0u,
-                                          ok ? r.q1 : 0u, ok ? r.s0 : 0u, ok ? r.s1 : 0u,
-                                          ok ? (uint32_t)r.script.size() : 0u, ok ? h : 2166136261u});
-            }
-            return true;
-        }
-
-        // ---- host Phase 2b per pair, then per query
-        // everything it reads is owned by it or outlives the caller's sub-batch (it may still run
-        // after the sub-batch body has returned, held by the sub-batch's host tail)
-        auto phase2b = [&C, ns, np, out, hqlen = std::vector<uint32_t>(hqlen, hqlen + nb), qhost, pair_ids,
-                        prelims = std::move(prelims),
-                        tres = std::move(tres), pre_off = std::move(pre_off), rounds_ops = std::move(rounds_ops),
-                        raw_round = std::move(raw_round), raw_off = std::move(raw_off), raw_n = std::move(raw_n),
-                        unpack]() mutable {
-            const auto t2 = std::chrono::steady_clock::now();
-            std::vector<std::vector<Hit>> pair_hits(np);
-            // the reverse complement of each query with prelims, once
-            std::vector<uint32_t> uq;
-            for (size_t k = 0; k < np; ++k) uq.push_back(pair_ids[k] / ns);
-            std::sort(uq.begin(), uq.end());
-            uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
-            std::vector<std::vector<uint8_t>> qrcs(uq.size());
-            parallel_for(uq.size(), [&](size_t j) { qrcs[j] = revcomp_full(qhost(uq[j]), hqlen[uq[j]] + 2); });
-            parallel_for(np, [&](size_t k) {
-                const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
-                const uint8_t* qs = qhost(qi);
-                const std::vector<uint8_t>& qrc = qrcs[std::lower_bound(uq.begin(), uq.end(), qi) - uq.begin()];
-                SubjectView v;
-                v.align = C.h_align.data() + C.plus_off[si];
-                v.align_rc = C.h_align_rc.data() + C.plus_off[si];
-                v.n_mask = C.mask_off[si] >= 0 ? C.h_mask.data() + C.mask_off[si] : nullptr;
-                v.n_mask_rc = C.mask_off[si] >= 0 ? C.h_mask_rc.data() + C.mask_off[si] : nullptr;
-                v.len = C.slen[si];
-                std::vector<TbResult> tr(tres.begin() + pre_off[k], tres.begin() + pre_off[k + 1]);
-                for (uint64_t j = pre_off[k]; j < pre_off[k + 1]; ++j)
-                    unpack(rounds_ops, raw_round[j], raw_off[j], raw_n[j], tr[j - pre_off[k]].script);
-                pair_hits[k] = phase2b_filter(prelims[k], tr, qs, qrc.data(), hqlen[qi], v, si, C.gp);
-            });
+    // everything the job reads is owned by it or outlives the caller's sub-batch
+    auto job = [&C, &W, Q, nb, out, taps, hq = std::vector<uint32_t>(hqlen_in, hqlen_in + nb), qhost = qhost_in,
+                pair_ids = pair_ids_in, prelims = std::move(prelims_in)](rmb_counters& ctr,
+                                                                          cudaStream_t st) mutable -> bool {
+        const uint32_t* hqlen = hq.data();
+        const uint32_t ns = (uint32_t)C.ids.size();
+        const size_t np = pair_ids.size();
+        unsigned long long cells = 0;
+        std::unique_lock<std::mutex> tb_lock(W.tb_mu);  // the lane's traceback buffers, until the results are back
+        auto t0 = std::chrono::steady_clock::now();
+        {
+            // ---- traceback DP of every prelim (GPU), with retries for scratch overflow
+            uint64_t n_pre = 0;
+            for (auto& v : prelims) n_pre += v.size();
+            std::vector<TbIn> tin;
+            tin.reserve(n_pre);
+            std::vector<uint64_t> pre_off(np + 1, 0);
             for (size_t k = 0; k < np; ++k) {
-                const uint32_t qi = pair_ids[k] / ns;
-                auto& dst = out[qi];
-                for (auto& h : pair_hits[k]) {
-                    h.q_len = hqlen[qi];
-                    dst.push_back(std::move(h));
+                pre_off[k + 1] = pre_off[k] + prelims[k].size();
+                for (const Prelim& p : prelims[k])
+                    tin.push_back(TbIn{pair_ids[k], p.strand, p.q_seed, p.s_seed, p.q_start, p.q_end, p.s_start, p.s_end});
+            }
+            std::vector<TbResult> tres(tin.size());
+            // each finished item's script stays packed in its round's ops until Phase 2b unpacks it
+            // (in parallel, per pair): round, offset and count per item
+            std::vector<std::vector<uint32_t>> rounds_ops;
+            std::vector<uint32_t> raw_round(tin.size(), 0), raw_n(tin.size(), 0);
+            std::vector<uint64_t> raw_off(tin.size(), 0);
+            if (!tin.empty()) {
+                uint32_t qmax = 0;
+                for (uint32_t i = 0; i < nb; ++i) qmax = std::max(qmax, hqlen[i]);
+                // batched: largest prelim boxes first (warps take items round-robin, so the long
+                // alignments start in the first wave instead of stretching the end of the launch);
+                // plain: in arrival order
+                std::vector<uint32_t> todo(tin.size());
+                for (uint32_t i = 0; i < todo.size(); ++i) todo[i] = i;
+                auto box = [&](uint32_t i) {
+                    return (uint64_t)(tin[i].q_end - tin[i].q_start) + (uint64_t)(tin[i].s_end - tin[i].s_start);
+                };
+                if (C.p.pipeline != 1)
+                    std::stable_sort(todo.begin(), todo.end(), [&](uint32_t x, uint32_t y) { return box(x) > box(y); });
+                uint64_t trace_cap = 1ull << 20;
+                uint32_t ops_cap = 1024;
+                int rounds = 0;
+                while (!todo.empty()) {
+                    if (++rounds > 12) throw Fail(RMB_ENOMEM, "traceback scratch kept overflowing");
+                    std::vector<TbIn> chunk_in(todo.size());
+                    for (size_t i = 0; i < todo.size(); ++i) chunk_in[i] = tin[todo[i]];
+                    const uint64_t band_cells = (uint64_t)C.max_slen + 2;
+                    const uint32_t rows_cap = qmax + 2;
+                    const uint64_t per_thread = ((band_cells * 8 + (uint64_t)rows_cap * 8 + trace_cap) + 255) & ~255ull;
+                    const uint64_t budget = 8ull << 30;
+                    // one warp per scratch slot (two items, the left and the right extension, per
+                    // prelim), blocks of 8 warps
+                    // (the plain pipeline: one prelim per warp, its two extensions in turn)
+                    const bool whole = C.p.pipeline == 1;
+                    uint32_t threads = (uint32_t)std::min<uint64_t>((whole ? 1 : 2) * todo.size(),
+                                                                    std::max<uint64_t>(8, budget / per_thread));
+                    threads = (threads + 7) / 8 * 8;
+                    upload(W.tb_in, chunk_in, st);
+                    W.tb_out.ensure(todo.size() * sizeof(TbOut));
+                    W.tb_half.ensure(2 * todo.size() * sizeof(TbHalf));
+                    W.tb_ops.ensure(2 * todo.size() * (uint64_t)ops_cap * 4);
+                    W.tb_scratch.ensure((uint64_t)threads * per_thread);
+                    W.tb_cells.ensure(8);
+                    CK(cudaMemsetAsync(W.tb_cells.p, 0, 8, st));
+                    EvTimer et;
+                    et.start(st);
+                    ctr.launches += 2;
+                    CK(launch_traceback(C.L, Q, C.d_params.as<DevParams>(), (uint32_t)todo.size(), W.tb_in.as<TbIn>(),
+                                        W.tb_out.as<TbOut>(), W.tb_half.as<TbHalf>(), W.tb_ops.as<uint32_t>(), ops_cap,
+                                        W.tb_scratch.as<uint8_t>(),
+                                        per_thread, band_cells, rows_cap, threads, W.tb_cells.as<unsigned long long>(),
+                                        whole, st));
+                    et.stop(st);
+                    std::vector<TbOut> to(todo.size());
+                    CK(cudaMemcpyAsync(to.data(), W.tb_out.p, to.size() * sizeof(TbOut), cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(&cells, W.tb_cells.p, 8, cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    ctr.gpu_ms_traceback += et.ms();
+                    // only the ops of the finished items come back, packed
+                    std::vector<uint64_t> ooff(todo.size() + 1, 0);
+                    for (size_t i = 0; i < todo.size(); ++i)
+                        ooff[i + 1] = ooff[i] + (to[i].status == 2 ? 0 : to[i].n_ops);
+                    std::vector<uint32_t> ops(ooff.back());
+                    if (!ops.empty()) {
+                        upload(W.tb_ooff, ooff, st);
+                        W.tb_ops2.ensure(ops.size() * 4);
+                        // the merged script of prelim i sits in ops slot 2 i
+                        CK(launch_gather_ops((uint32_t)todo.size(), W.tb_ops.as<uint32_t>(), 2 * ops_cap, W.tb_out.as<TbOut>(),
+                                             W.tb_ooff.as<uint64_t>(), W.tb_ops2.as<uint32_t>(), C.sms, st));
+                        CK(cudaMemcpyAsync(ops.data(), W.tb_ops2.p, ops.size() * 4, cudaMemcpyDeviceToHost, st));
+                        CK(cudaStreamSynchronize(st));
+                        ctr.launches += 1;
+                    }
+                    std::vector<uint32_t> again;
+                    const uint32_t round_id = (uint32_t)rounds_ops.size();
+                    for (size_t i = 0; i < todo.size(); ++i) {
+                        const TbOut& o = to[i];
+                        if (o.status == 2) { again.push_back(todo[i]); continue; }
+                        if (o.status == 3) throw Fail(RMB_ECUDA, "traceback walk did not reach the origin");
+                        TbResult& r = tres[todo[i]];
+                        r.status = o.status;
+                        r.score = o.score;
+                        r.q0 = o.q0;
+                        r.q1 = o.q1;
+                        r.s0 = o.s0;
+                        r.s1 = o.s1;
+                        raw_round[todo[i]] = round_id;
+                        raw_off[todo[i]] = ooff[i];
+                        raw_n[todo[i]] = o.n_ops;
+                    }
+                    rounds_ops.push_back(std::move(ops));
+                    if (again.size() == todo.size()) {  // nothing finished: grow the caps
+                        trace_cap *= 4;
+                        ops_cap *= 4;
+                    } else if (!again.empty()) {
+                        trace_cap *= 4;
+                        ops_cap *= 4;
+                    }
+                    ctr.tb_cells += cells;
+                    todo.swap(again);
                 }
             }
-            return ms_since(t2);
-        };
-        ctr.ms_host_2b += phase2b();
+            ctr.tb_dp += tin.size();
+            tb_lock.unlock();  // the results are on the host
+            ctr.ms_traceback += ms_since(t0);
+            // item k's script from its round's packed ops (op << 30 | count)
+            auto unpack = [](const std::vector<std::vector<uint32_t>>& rops, uint32_t rd, uint64_t off, uint32_t n,
+                             Script& out) {
+                out.clear();
+                if (!n) return;
+                const uint32_t* v = rops[rd].data() + off;
+                for (uint32_t j = 0; j < n; ++j) out.push_back(RunOp{(uint8_t)(v[j] >> 30), v[j] & 0x3fffffffu});
+            };
+            if (taps && taps->tracebacks) {
+                for (size_t k = 0; k < tin.size(); ++k) unpack(rounds_ops, raw_round[k], raw_off[k], raw_n[k], tres[k].script);
+                for (size_t k = 0; k < tin.size(); ++k) {
+                    const TbResult& r = tres[k];
+                    uint32_t h = 2166136261u;  // FNV-1a over the run-length ops
+                    for (const RunOp& o : r.script) {
+                        const uint32_t v = ((uint32_t)o.op << 30) | o.n;
+                        for (int b = 0; b < 4; ++b) h = (h ^ ((v >> (8 * b)) & 0xffu)) * 16777619u;
+                    }
+                    const bool ok = r.status == 0;
+                    taps->tracebacks->insert(taps->tracebacks->end(),
+                                             {tin[k].strand, ok ? 0u : 1u, ok ? (uint32_t)r.score : 0u, ok ? r.q0 : 0u,
+                                              ok ? r.q1 : 0u, ok ? r.s0 : 0u, ok ? r.s1 : 0u,
+                                              ok ? (uint32_t)r.script.size() : 0u, ok ? h : 2166136261u});
+                }
+                return true;
+            }
+
+            // ---- host Phase 2b per pair, then per query
+            // everything it reads is owned by it or outlives the caller's sub-batch (it may still run
+            // after the sub-batch body has returned, held by the sub-batch's host tail)
+            auto phase2b = [&C, ns, np, out, hqlen = std::vector<uint32_t>(hqlen, hqlen + nb), qhost, pair_ids,
+                            prelims = std::move(prelims),
+                            tres = std::move(tres), pre_off = std::move(pre_off), rounds_ops = std::move(rounds_ops),
+                            raw_round = std::move(raw_round), raw_off = std::move(raw_off), raw_n = std::move(raw_n),
+                            unpack]() mutable {
+                const auto t2 = std::chrono::steady_clock::now();
+                std::vector<std::vector<Hit>> pair_hits(np);
+                // the reverse complement of each query with prelims, once
+                std::vector<uint32_t> uq;
+                for (size_t k = 0; k < np; ++k) uq.push_back(pair_ids[k] / ns);
+                std::sort(uq.begin(), uq.end());
+                uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
+                std::vector<std::vector<uint8_t>> qrcs(uq.size());
+                parallel_for(uq.size(), [&](size_t j) { qrcs[j] = revcomp_full(qhost(uq[j]), hqlen[uq[j]] + 2); });
+                parallel_for(np, [&](size_t k) {
+                    const uint32_t qi = pair_ids[k] / ns, si = pair_ids[k] % ns;
+                    const uint8_t* qs = qhost(qi);
+                    const std::vector<uint8_t>& qrc = qrcs[std::lower_bound(uq.begin(), uq.end(), qi) - uq.begin()];
+                    SubjectView v;
+                    v.align = C.h_align.data() + C.plus_off[si];
+                    v.align_rc = C.h_align_rc.data() + C.plus_off[si];
+                    v.n_mask = C.mask_off[si] >= 0 ? C.h_mask.data() + C.mask_off[si] : nullptr;
+                    v.n_mask_rc = C.mask_off[si] >= 0 ? C.h_mask_rc.data() + C.mask_off[si] : nullptr;
+                    v.len = C.slen[si];
+                    std::vector<TbResult> tr(tres.begin() + pre_off[k], tres.begin() + pre_off[k + 1]);
+                    for (uint64_t j = pre_off[k]; j < pre_off[k + 1]; ++j)
+                        unpack(rounds_ops, raw_round[j], raw_off[j], raw_n[j], tr[j - pre_off[k]].script);
+                    pair_hits[k] = phase2b_filter(prelims[k], tr, qs, qrc.data(), hqlen[qi], v, si, C.gp);
+                });
+                for (size_t k = 0; k < np; ++k) {
+                    const uint32_t qi = pair_ids[k] / ns;
+                    auto& dst = out[qi];
+                    for (auto& h : pair_hits[k]) {
+                        h.q_len = hqlen[qi];
+                        dst.push_back(std::move(h));
+                    }
+                }
+                return ms_since(t2);
+            };
+            ctr.ms_host_2b += phase2b();
+        }
+        return false;
+    };
+    if (defer) {
+        const int dev = C.p.device;
+        cudaStream_t st2 = W.st2;
+        *defer = std::async(std::launch::async, [job = std::move(job), dev, st2]() mutable {
+            CK(cudaSetDevice(dev));
+            rmb_counters c{};
+            job(c, st2);
+            return c;
+        });
+        return false;
     }
-    return false;
-  };
-  if (defer) {
-      const int dev = C.p.device;
-      cudaStream_t st2 = W.st2;
-      *defer = std::async(std::launch::async, [job = std::move(job), dev, st2]() mutable {
-          CK(cudaSetDevice(dev));
-          rmb_counters c{};
-          job(c, st2);
-          return c;
-      });
-      return false;
-  }
-  return job(ctr_in, W.st);
+    return job(ctr_in, W.st);
 }
 
 int fail_out(const std::exception& e, char* err, size_t errlen, int code) {
