@@ -114,7 +114,6 @@ __device__ __forceinline__ bool exact_extend(const PairView& v, uint32_t q0c, ui
 //               from warp * stage_cap), the pair's first entry in stage_start; if a stretch runs
 //               out, *stage_over is set and the batch takes the SCAN_WRITE pass instead.
 enum { SCAN_COUNT = 0, SCAN_WRITE = 1, SCAN_STAGE = 2 };
-constexpr uint32_t SCAN_QUEUE_RUN = 8;
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws, uint64_t pair0, uint64_t n_pairs,
@@ -130,18 +129,14 @@ __global__ void __launch_bounds__(256) k_scan(DevLib L, DevQueries Q, int32_t ws
     const uint32_t stage0 = MODE == SCAN_STAGE ? (uint32_t)warp * stage_cap : 0u;  // this warp's stretch
     uint32_t cursor = 0;                                                            // entries of it used
     bool fits = true;
-    // pairs by warp stride, or, with pair_queue, the next run of SCAN_QUEUE_RUN consecutive pairs
-    // off a grid-wide counter as a warp finishes one (subject lengths vary 100-fold, so fixed
-    // strides leave warps idle at the end; a run's pairs share their query's tables in L1)
-    uint64_t w_next = warp, run_end = 0;
+    // pairs by warp stride, or, with pair_queue, the next pair off a grid-wide counter as a warp
+    // finishes one (subject lengths vary 100-fold, so fixed strides leave warps idle at the end)
+    uint64_t w_next = warp;
     auto next_pair = [&]() -> uint64_t {
         if (pair_queue) {
-            if (w_next < run_end) return w_next++;
             unsigned long long x = 0;
-            if (lane == 0) x = atomicAdd(pair_queue, (unsigned long long)SCAN_QUEUE_RUN);
-            w_next = __shfl_sync(0xffffffffu, x, 0);
-            run_end = w_next + SCAN_QUEUE_RUN;
-            return w_next++;
+            if (lane == 0) x = atomicAdd(pair_queue, 1ull);
+            return __shfl_sync(0xffffffffu, x, 0);
         }
         const uint64_t r = w_next;
         w_next += nwarps;
@@ -2199,8 +2194,8 @@ cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, 
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
     // the queue pays where a warp gets few pairs (under 64: its strides' lengths vary the most); with
     // many pairs a warp, fixed strides balance and keep a block's warps on one query's tables in
-    // L1 (measured: sub-batches of ~150 queries of 1-200 kb, 54 -> 41 ms with the queue; 1,000
-    // queries of 60 kb, 2 M pairs, 75 -> 115 ms)
+    // L1 (measured: sub-batches of ~150 queries of 1-200 kb, 54 -> 38 ms with the queue; 1,000
+    // queries of 60 kb, 2 M pairs, 75 -> 109 ms)
     const bool use_queue = queue && n_pairs < (uint64_t)grid * (block / 32) * 64;
     k_scan<SCAN_STAGE><<<grid, block, 0, st>>>(L, Q, ws, 0, n_pairs, counts, nullptr, stage, nullptr, stage_start,
                                                SCAN_STAGE_PER_WARP, stage_over,
