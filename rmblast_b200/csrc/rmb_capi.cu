@@ -728,11 +728,19 @@ void run_core(rmb_ctx& C, rmb_queries& QH, std::vector<std::vector<Hit>>& out_hi
         W.stage_start.ensure(npairs * 4);
         W.stage.ensure(scan_stage_entries(npairs, C.sms) * sizeof(SeedHit));
         W.stage_over.ensure(16);  // the overflow flag and the scan's pair queue
+        // The batched pipeline feeds the scan's warps pairs from a queue where the sub-batch's
+        // query lengths vary (over 2x): a pair's cost then follows its query too, and fixed
+        // strides left warps idle (1,000 chunks of 1-200 kb: 54 -> 38 ms a step).  Over queries
+        // of one length the strides balance and keep a block's warps on one query's tables in L1
+        // (1,000 queries of 60 kb: 75 ms with strides, 109 with the queue).
+        const uint32_t qlo = *std::min_element(hqlen.begin(), hqlen.end());
+        const uint32_t qhi = *std::max_element(hqlen.begin(), hqlen.end());
+        const bool scan_queue = P.pipeline != 1 && (uint64_t)qhi > 2ull * qlo;
         CK(cudaMemsetAsync(W.counts.p, 0, (npairs + 1) * 4, st));
         CK(cudaMemsetAsync(W.stage_over.p, 0, 16, st));
         ev.start(st);
         CK(launch_scan_stage(C.L, Q, P.word_size, npairs, W.counts.as<uint32_t>(), W.stage_start.as<uint32_t>(),
-                             W.stage.as<SeedHit>(), W.stage_over.as<unsigned int>(), C.sms, st, P.pipeline != 1));
+                             W.stage.as<SeedHit>(), W.stage_over.as<unsigned int>(), C.sms, st, scan_queue));
         size_t tb = 0;
         CK(launch_offsets(W.counts.as<uint32_t>(), npairs + 1, W.offs.as<uint64_t>(), nullptr, tb, st));
         W.temp.ensure(tb);

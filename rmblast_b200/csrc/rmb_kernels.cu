@@ -2189,17 +2189,12 @@ cudaError_t launch_scan_stage(const DevLib& L, const DevQueries& Q, int32_t ws, 
                               uint32_t* stage_start, SeedHit* stage, unsigned int* stage_over, int sms,
                               cudaStream_t st, bool queue) {
     // stage_over: [0] the overflow flag, [2..3] the pair queue (both zeroed by the caller); without
-    // `queue` the warps take pairs by stride (the plain pipeline)
+    // `queue` the warps take pairs by stride
     const int block = 256;
     const int grid = grid_for(n_pairs * 32, block, 8, sms);
-    // the queue pays where a warp gets few pairs (under 64: its strides' lengths vary the most); with
-    // many pairs a warp, fixed strides balance and keep a block's warps on one query's tables in
-    // L1 (measured: sub-batches of ~150 queries of 1-200 kb, 54 -> 38 ms with the queue; 1,000
-    // queries of 60 kb, 2 M pairs, 75 -> 109 ms)
-    const bool use_queue = queue && n_pairs < (uint64_t)grid * (block / 32) * 64;
     k_scan<SCAN_STAGE><<<grid, block, 0, st>>>(L, Q, ws, 0, n_pairs, counts, nullptr, stage, nullptr, stage_start,
                                                SCAN_STAGE_PER_WARP, stage_over,
-                                               use_queue ? reinterpret_cast<unsigned long long*>(stage_over + 2) : nullptr);
+                                               queue ? reinterpret_cast<unsigned long long*>(stage_over + 2) : nullptr);
     return cudaGetLastError();
 }
 
