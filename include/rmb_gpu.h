@@ -202,7 +202,9 @@ typedef struct rmb_results {
  * queries of 1,999,800 bp or more the multi-chunk path (main.rs:1236-1400: 1 Mb chunks with a
  * 100 bp overlap, whole-query DUST, cross-chunk merge, full-query traceback); both in one call.
  * query[i]: sentinel-wrapped BLASTNA (qlen[i] + 2 bytes), not CRandom-resolved (queries keep
- * N).  Stage taps (rmb_debug_stage) take single-chunk queries only. */
+ * N).  Stage taps (rmb_debug_stage) take single-chunk queries only.  The batched pipeline runs
+ * some host steps on threads of its own beside its kernels and joins them before returning;
+ * calls on one context must not overlap. */
 int rmb_search_batch(rmb_ctx* ctx, uint32_t n_queries, const uint8_t* const* query, const uint32_t* qlen,
                      rmb_results** out, char* err, size_t errlen);
 
